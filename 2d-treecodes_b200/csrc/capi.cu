@@ -1,0 +1,514 @@
+// capi.cu -- the C ABI: contexts, host and device entry points, statistics, inspection.
+//
+// treecode_potential / treecode_force_mrag keep the reference's prototypes
+// (drivers/treecode-potential.h:21-29, drivers/treecode-force.h:21-31).  Each calling thread
+// gets its own context (stream + grow-only device buffers), so the functions are reentrant,
+// unlike the reference whose Tree:: globals are shared (drivers/upward.cpp:51-59).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "treecodes_b200.h"
+#include "tc_internal.h"
+
+namespace tc {
+
+int direct_potential(Context &c, const double *xs, const double *ys, const double *vs, int n,
+                     const double *xt, const double *yt, int m, double *out);
+int direct_force(Context &c, const double *xs, const double *ys, const double *vs, int n,
+                 const double *xt, const double *yt, int m, double *xo, double *yo);
+int measure_fma_peak(int fp64, double *tflops);
+
+static thread_local int tls_status = TC_OK;
+static thread_local char tls_msg[512] = "";
+
+void set_error(int status, const char *fmt, ...) {
+    tls_status = status;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(tls_msg, sizeof(tls_msg), fmt, ap);
+    va_end(ap);
+}
+
+static void clear_error() {
+    tls_status = TC_OK;
+    tls_msg[0] = 0;
+}
+
+void phase_mark(Context &c, int idx) {
+    if (c.timing) cudaEventRecord(c.ev[idx], c.stream);
+}
+
+int check_device_errors(Context &c, const char *where) {
+    unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 8, err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    const unsigned e = c.h_pinned[8];
+    if (e & DEVERR_SPIN_LIMIT) {
+        set_error(TC_ERR_TIMEOUT, "%s: a bounded device wait gave up (flags 0x%x)", where, e);
+        return TC_ERR_TIMEOUT;
+    }
+    if (e & DEVERR_STACK) {
+        set_error(TC_ERR_CAPACITY, "%s: traversal stack capacity exceeded (flags 0x%x)", where, e);
+        return TC_ERR_CAPACITY;
+    }
+    if (e) {
+        set_error(TC_ERR_CUDA, "%s: inconsistent tree bookkeeping (flags 0x%x)", where, e);
+        return TC_ERR_CUDA;
+    }
+    return TC_OK;
+}
+
+static int context_init(Context &c, int device, cudaStream_t stream) {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        set_error(TC_ERR_NO_DEVICE, "no CUDA device available (%s)",
+                  e == cudaSuccess ? "device count 0" : cudaGetErrorString(e));
+        return TC_ERR_NO_DEVICE;
+    }
+    if (device < 0) TC_CUDA_TRY(cudaGetDevice(&device));
+    TC_CUDA_TRY(cudaSetDevice(device));
+    c.device = device;
+    if (stream) {
+        c.stream = stream;
+        c.own_stream = false;
+    } else {
+        TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        c.own_stream = true;
+    }
+    TC_CUDA_TRY(cudaMallocHost(&c.h_pinned, 4096));
+    for (auto &ev : c.ev) TC_CUDA_TRY(cudaEventCreate(&ev));
+    unsigned *err;
+    int rc;
+    if ((rc = ensure(c, S_ERR, 64, &err))) return rc;
+    TC_CUDA_TRY(cudaMemsetAsync(err, 0, 64 * sizeof(unsigned), c.stream));
+    return TC_OK;
+}
+
+static void context_free(Context &c) {
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    for (auto &b : c.buf)
+        if (b.p) cudaFree(b.p);
+    for (auto &ev : c.ev)
+        if (ev) cudaEventDestroy(ev);
+    if (c.h_pinned) cudaFreeHost(c.h_pinned);
+    if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+}
+
+static void finish_timing(Context &c) {
+    if (!c.timing) return;
+    cudaEventSynchronize(c.ev[5]);
+    float t[6] = {};
+    for (int i = 1; i <= 5; ++i) cudaEventElapsedTime(&t[i], c.ev[i - 1], c.ev[i]);
+    c.times.sort_ms = t[1];
+    c.times.tree_ms = t[2];
+    c.times.upward_ms = t[3];
+    c.times.lists_ms = t[4];
+    c.times.eval_ms = t[5];
+    float tot = 0;
+    cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
+    c.times.total_ms = tot;
+}
+
+// Sort, topology and upward pass for `kind` (0 potential, 1 force).
+static int build_tree(Context &c, int kind, const double *x, const double *y, const double *v,
+                      int n) {
+    int rc;
+    TC_CUDA_TRY(cudaMemsetAsync(slot_ptr<unsigned>(c, S_ERR), 0, sizeof(unsigned), c.stream));
+    if ((rc = sort_sources(c, x, y, v, n))) return rc;
+    phase_mark(c, 1);
+    if ((rc = build_topology(c, kind ? LEAF_FORCE : LEAF_POTENTIAL))) return rc;
+    phase_mark(c, 2);
+    if ((rc = upward_pass(c, kind ? ORDER_FORCE : ORDER_POTENTIAL))) return rc;
+    phase_mark(c, 3);
+    return TC_OK;
+}
+
+static int potential_device(Context &c, double theta, const double *xs, const double *ys,
+                            const double *vs, int n, const double *xt, const double *yt, int m,
+                            double *out) {
+    if (n < 0 || m < 0) {
+        set_error(TC_ERR_INVALID, "negative size (nsources %d, ntargets %d)", n, m);
+        return TC_ERR_INVALID;
+    }
+    if (m == 0) return TC_OK;
+    if (n == 0) {
+        TC_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * m, c.stream));
+        TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        return TC_OK;
+    }
+    if (c.precision != 0) {
+        set_error(TC_ERR_INVALID, "precision mode %d is not available for the potential", c.precision);
+        return TC_ERR_INVALID;
+    }
+    int rc;
+    phase_mark(c, 0);
+    if ((rc = build_tree(c, 0, xs, ys, vs, n))) return rc;
+    if ((rc = potential(c, theta, xt, yt, m, out))) return rc;
+    phase_mark(c, 5);
+    if ((rc = check_device_errors(c, "treecode_potential"))) return rc;
+    finish_timing(c);
+    return TC_OK;
+}
+
+static int force_device(Context &c, double theta, const double *xs, const double *ys,
+                        const double *vs, int n, const double *x0s, const double *y0s,
+                        const double *hs, int nb, double *xo, double *yo) {
+    if (n < 0 || nb < 0) {
+        set_error(TC_ERR_INVALID, "negative size (nsources %d, nblocks %d)", n, nb);
+        return TC_ERR_INVALID;
+    }
+    if (nb == 0) return TC_OK;
+    if (nb > (1 << 30) / (BLOCKSIZE * BLOCKSIZE)) {
+        set_error(TC_ERR_INVALID, "too many blocks (%d)", nb);
+        return TC_ERR_INVALID;
+    }
+    const size_t nt = (size_t)nb * BLOCKSIZE * BLOCKSIZE;
+    if (n == 0) {
+        TC_CUDA_TRY(cudaMemsetAsync(xo, 0, sizeof(double) * nt, c.stream));
+        TC_CUDA_TRY(cudaMemsetAsync(yo, 0, sizeof(double) * nt, c.stream));
+        TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        return TC_OK;
+    }
+    if (c.precision != 0) {
+        set_error(TC_ERR_INVALID, "precision mode %d is not available yet", c.precision);
+        return TC_ERR_INVALID;
+    }
+    int rc;
+    phase_mark(c, 0);
+    if ((rc = build_tree(c, 1, xs, ys, vs, n))) return rc;
+    if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo))) return rc;
+    phase_mark(c, 5);
+    if ((rc = check_device_errors(c, "treecode_force_mrag"))) return rc;
+    finish_timing(c);
+    return TC_OK;
+}
+
+template <class T>
+static int stage(Context &c, Slot s, const T *host, size_t n, T **dev) {
+    int rc;
+    if ((rc = ensure(c, s, n, dev))) return rc;
+    if (n) TC_CUDA_TRY(cudaMemcpyAsync(*dev, host, sizeof(T) * n, cudaMemcpyHostToDevice, c.stream));
+    return TC_OK;
+}
+
+static int potential_host(Context &c, double theta, const double *xs, const double *ys,
+                          const double *vs, int n, const double *xt, const double *yt, int m,
+                          double *out) {
+    if (n < 0 || m < 0 || (m > 0 && (!xt || !yt || !out)) || (n > 0 && (!xs || !ys || !vs))) {
+        set_error(TC_ERR_INVALID, "invalid arguments (nsources %d, ntargets %d)", n, m);
+        return TC_ERR_INVALID;
+    }
+    if (m == 0) return TC_OK;
+    int rc;
+    double *dx, *dy, *dv, *dxt, *dyt, *dout;
+    if ((rc = stage(c, S_XIN, xs, n, &dx)) || (rc = stage(c, S_YIN, ys, n, &dy)) ||
+        (rc = stage(c, S_VIN, vs, n, &dv)) || (rc = stage(c, S_XT, xt, m, &dxt)) ||
+        (rc = stage(c, S_YT, yt, m, &dyt)) || (rc = ensure(c, S_OUTX, m, &dout)))
+        return rc;
+    if ((rc = potential_device(c, theta, dx, dy, dv, n, dxt, dyt, m, dout))) return rc;
+    TC_CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return TC_OK;
+}
+
+static int force_host(Context &c, double theta, const double *xs, const double *ys,
+                      const double *vs, int n, const double *x0s, const double *y0s,
+                      const double *hs, int nb, double *xo, double *yo) {
+    if (n < 0 || nb < 0 || (nb > 0 && (!x0s || !y0s || !hs || !xo || !yo)) ||
+        (n > 0 && (!xs || !ys || !vs))) {
+        set_error(TC_ERR_INVALID, "invalid arguments (nsources %d, nblocks %d)", n, nb);
+        return TC_ERR_INVALID;
+    }
+    if (nb == 0) return TC_OK;
+    int rc;
+    const size_t nt = (size_t)nb * BLOCKSIZE * BLOCKSIZE;
+    double *dx, *dy, *dv, *d0x, *d0y, *dh, *dox, *doy;
+    if ((rc = stage(c, S_XIN, xs, n, &dx)) || (rc = stage(c, S_YIN, ys, n, &dy)) ||
+        (rc = stage(c, S_VIN, vs, n, &dv)) || (rc = stage(c, S_X0, x0s, nb, &d0x)) ||
+        (rc = stage(c, S_Y0, y0s, nb, &d0y)) || (rc = stage(c, S_H, hs, nb, &dh)) ||
+        (rc = ensure(c, S_OUTX, nt, &dox)) || (rc = ensure(c, S_OUTY, nt, &doy)))
+        return rc;
+    if ((rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy))) return rc;
+    TC_CUDA_TRY(cudaMemcpyAsync(xo, dox, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(yo, doy, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return TC_OK;
+}
+
+// Per-thread default context of the reference-compatible entry points.
+struct TlsContext {
+    Context *c = nullptr;
+    ~TlsContext() {
+        if (c) {
+            context_free(*c);
+            delete c;
+        }
+    }
+};
+static thread_local TlsContext tls_ctx;
+
+static Context *default_context() {
+    if (!tls_ctx.c) {
+        Context *c = new Context();
+        if (context_init(*c, -1, nullptr) != TC_OK) {
+            delete c;
+            return nullptr;
+        }
+        tls_ctx.c = c;
+    }
+    return tls_ctx.c;
+}
+
+static void report_failure(const char *fn) {
+    // The reference signatures return void; a failed solve is reported on stderr as well as
+    // through treecode_last_status(), so it cannot pass unnoticed.
+    fprintf(stderr, "%s failed (status %d): %s\n", fn, tls_status, tls_msg);
+}
+
+}  // namespace tc
+
+struct tc_context {
+    tc::Context c;
+};
+
+using namespace tc;
+
+extern "C" {
+
+TC_API void treecode_potential(const double theta, const double *const xsources,
+                               const double *const ysources, const double *const sourcevalues,
+                               const int nsources, const double *const xtargets,
+                               const double *const ytargets, const int ntargets,
+                               double *const targetvalues) {
+    clear_error();
+    Context *c = default_context();
+    if (!c || potential_host(*c, theta, xsources, ysources, sourcevalues, nsources, xtargets,
+                             ytargets, ntargets, targetvalues) != TC_OK)
+        report_failure("treecode_potential");
+}
+
+TC_API void treecode_force_mrag(const double theta, const double *const xsources,
+                                const double *const ysources, const double *const sourcevalues,
+                                const int nsources, const double *const x0s,
+                                const double *const y0s, const double *const hs,
+                                const int nblocks, double *const xresults,
+                                double *const yresults) {
+    clear_error();
+    Context *c = default_context();
+    if (!c || force_host(*c, theta, xsources, ysources, sourcevalues, nsources, x0s, y0s, hs,
+                         nblocks, xresults, yresults) != TC_OK)
+        report_failure("treecode_force_mrag");
+}
+
+TC_API int treecode_last_status(void) { return tls_status; }
+TC_API const char *treecode_last_error(void) { return tls_msg; }
+
+TC_API int tc_context_create(tc_context **ctx, int device, void *cuda_stream) {
+    clear_error();
+    if (!ctx) {
+        set_error(TC_ERR_INVALID, "ctx is NULL");
+        return TC_ERR_INVALID;
+    }
+    tc_context *t = new tc_context();
+    int rc = context_init(t->c, device, (cudaStream_t)cuda_stream);
+    if (rc) {
+        context_free(t->c);
+        delete t;
+        *ctx = nullptr;
+        return rc;
+    }
+    *ctx = t;
+    return TC_OK;
+}
+
+TC_API void tc_context_destroy(tc_context *ctx) {
+    if (!ctx) return;
+    context_free(ctx->c);
+    delete ctx;
+}
+
+TC_API int tc_set_precision(tc_context *ctx, int precision) {
+    clear_error();
+    if (!ctx || precision < 0 || precision > 1) {
+        set_error(TC_ERR_INVALID, "invalid precision mode %d", precision);
+        return TC_ERR_INVALID;
+    }
+    ctx->c.precision = precision;
+    return TC_OK;
+}
+
+TC_API int tc_set_timing(tc_context *ctx, int enabled) {
+    if (!ctx) return TC_ERR_INVALID;
+    ctx->c.timing = enabled != 0;
+    return TC_OK;
+}
+
+TC_API void *tc_get_stream(tc_context *ctx) { return ctx ? (void *)ctx->c.stream : nullptr; }
+
+TC_API int tc_get_stats(tc_context *ctx, tc_stats *out) {
+    if (!ctx || !out) return TC_ERR_INVALID;
+    const Context &c = ctx->c;
+    out->sort_ms = c.times.sort_ms;
+    out->tree_ms = c.times.tree_ms;
+    out->upward_ms = c.times.upward_ms;
+    out->lists_ms = c.times.lists_ms;
+    out->eval_ms = c.times.eval_ms;
+    out->total_ms = c.times.total_ms;
+    out->nnodes = c.counts.nnodes;
+    out->nleaves = c.counts.nleaves;
+    out->ninner = c.counts.ninner;
+    out->nlevels = c.counts.nlevels;
+    out->n_e2l = c.counts.n_e2l;
+    out->n_e2p = c.counts.n_e2p;
+    out->n_p2p = c.counts.n_p2p;
+    return TC_OK;
+}
+
+#define CTX_GUARD()                                             \
+    clear_error();                                              \
+    if (!ctx) {                                                 \
+        set_error(TC_ERR_INVALID, "context is NULL");           \
+        return TC_ERR_INVALID;                                  \
+    }                                                           \
+    cudaSetDevice(ctx->c.device)
+
+TC_API int tc_potential_host(tc_context *ctx, double theta, const double *xs, const double *ys,
+                             const double *vs, int n, const double *xt, const double *yt, int m,
+                             double *out) {
+    CTX_GUARD();
+    return potential_host(ctx->c, theta, xs, ys, vs, n, xt, yt, m, out);
+}
+
+TC_API int tc_force_mrag_host(tc_context *ctx, double theta, const double *xs, const double *ys,
+                              const double *vs, int n, const double *x0s, const double *y0s,
+                              const double *hs, int nb, double *xo, double *yo) {
+    CTX_GUARD();
+    return force_host(ctx->c, theta, xs, ys, vs, n, x0s, y0s, hs, nb, xo, yo);
+}
+
+TC_API int tc_potential_device(tc_context *ctx, double theta, const double *xs, const double *ys,
+                               const double *vs, int n, const double *xt, const double *yt,
+                               int m, double *out) {
+    CTX_GUARD();
+    return potential_device(ctx->c, theta, xs, ys, vs, n, xt, yt, m, out);
+}
+
+TC_API int tc_force_mrag_device(tc_context *ctx, double theta, const double *xs,
+                                const double *ys, const double *vs, int n, const double *x0s,
+                                const double *y0s, const double *hs, int nb, double *xo,
+                                double *yo) {
+    CTX_GUARD();
+    return force_device(ctx->c, theta, xs, ys, vs, n, x0s, y0s, hs, nb, xo, yo);
+}
+
+TC_API int tc_tree_build_device(tc_context *ctx, int kind, const double *xs, const double *ys,
+                                const double *vs, int n) {
+    CTX_GUARD();
+    if (n <= 0 || (kind != 0 && kind != 1)) {
+        set_error(TC_ERR_INVALID, "invalid tree request (kind %d, n %d)", kind, n);
+        return TC_ERR_INVALID;
+    }
+    int rc = build_tree(ctx->c, kind, xs, ys, vs, n);
+    if (rc) return rc;
+    return check_device_errors(ctx->c, "tc_tree_build_device");
+}
+
+TC_API int tc_tree_size(tc_context *ctx, int *nnodes, int *order, int *nsources) {
+    CTX_GUARD();
+    if (nnodes) *nnodes = ctx->c.nnodes;
+    if (order) *order = ctx->c.order;
+    if (nsources) *nsources = ctx->c.nsrc;
+    return TC_OK;
+}
+
+TC_API int tc_tree_copy(tc_context *ctx, int *keys, int *perm, double *xs, double *ys,
+                        double *vs, double *frame, int *s, int *e, int *child, int *count,
+                        int *level, int *cx, int *cy, int *parent, double *mass, double *xcom,
+                        double *ycom, double *r, double *exps) {
+    CTX_GUARD();
+    Context &c = ctx->c;
+    const int n = c.nsrc, nn = c.nnodes;
+    auto d2h = [&](void *dst, const void *src, size_t bytes) {
+        return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    };
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    if (keys) TC_CUDA_TRY(d2h(keys, c.buf[S_KEYS].p, sizeof(int) * n));
+    if (perm) TC_CUDA_TRY(d2h(perm, c.buf[S_PERM].p, sizeof(int) * n));
+    if (xs) TC_CUDA_TRY(d2h(xs, c.buf[S_XS].p, sizeof(double) * n));
+    if (ys) TC_CUDA_TRY(d2h(ys, c.buf[S_YS].p, sizeof(double) * n));
+    if (vs) TC_CUDA_TRY(d2h(vs, c.buf[S_VS].p, sizeof(double) * n));
+    if (frame) {
+        Frame f;
+        TC_CUDA_TRY(d2h(&f, c.buf[S_FRAME].p, sizeof(Frame)));
+        frame[0] = f.xmin;
+        frame[1] = f.ymin;
+        frame[2] = f.ext;
+    }
+    if (s || e || child || count || level || cx || cy || parent || xcom || ycom || r) {
+        TNode *tn = new TNode[nn];
+        int2 *rg = new int2[nn];
+        int4 *cl = new int4[nn];
+        cudaError_t err = d2h(tn, c.buf[S_TNODE].p, sizeof(TNode) * nn);
+        if (err == cudaSuccess) err = d2h(rg, c.buf[S_RANGE].p, sizeof(int2) * nn);
+        if (err == cudaSuccess) err = d2h(cl, c.buf[S_CELL].p, sizeof(int4) * nn);
+        if (err == cudaSuccess)
+            for (int i = 0; i < nn; ++i) {
+                // a leaf emptied by the all-negligible rule keeps its range for the upward
+                // pass; report it as the reference does, s = e = 0 (upward.cpp:179)
+                const bool emptied = tn[i].child < 0 && tn[i].count == 0 && rg[i].y > rg[i].x;
+                if (s) s[i] = emptied ? 0 : rg[i].x;
+                if (e) e[i] = emptied ? 0 : rg[i].y;
+                if (child) child[i] = tn[i].child;
+                if (count) count[i] = tn[i].count;
+                if (level) level[i] = cl[i].x;
+                if (cx) cx[i] = cl[i].y;
+                if (cy) cy[i] = cl[i].z;
+                if (parent) parent[i] = cl[i].w;
+                if (xcom) xcom[i] = tn[i].xcom;
+                if (ycom) ycom[i] = tn[i].ycom;
+                if (r) r[i] = tn[i].r;
+            }
+        delete[] tn;
+        delete[] rg;
+        delete[] cl;
+        TC_CUDA_TRY(err);
+    }
+    if (mass) TC_CUDA_TRY(d2h(mass, c.buf[S_MASS].p, sizeof(double) * nn));
+    if (exps) TC_CUDA_TRY(d2h(exps, c.buf[S_EXPS].p, sizeof(double) * nn * 2 * c.order));
+    return TC_OK;
+}
+
+TC_API int tc_direct_potential_device(tc_context *ctx, const double *xs, const double *ys,
+                                      const double *vs, int n, const double *xt,
+                                      const double *yt, int m, double *out) {
+    CTX_GUARD();
+    int rc = direct_potential(ctx->c, xs, ys, vs, n, xt, yt, m, out);
+    if (rc) return rc;
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+    return TC_OK;
+}
+
+TC_API int tc_direct_force_device(tc_context *ctx, const double *xs, const double *ys,
+                                  const double *vs, int n, const double *xt, const double *yt,
+                                  int m, double *xo, double *yo) {
+    CTX_GUARD();
+    int rc = direct_force(ctx->c, xs, ys, vs, n, xt, yt, m, xo, yo);
+    if (rc) return rc;
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+    return TC_OK;
+}
+
+TC_API int tc_measure_fma_peak(int fp64, double *tflops) {
+    clear_error();
+    if (!tflops) return TC_ERR_INVALID;
+    return measure_fma_peak(fp64, tflops);
+}
+
+TC_API const char *tc_version(void) { return "2d-treecodes-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

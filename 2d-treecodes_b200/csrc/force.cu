@@ -1,0 +1,401 @@
+// force.cu -- treecode_force_mrag on the GPU: per-brick interaction lists, then one fused
+// far-field + near-field evaluation per 8 x 8 brick.
+//
+// Restates drivers/treecode-force.cpp:94-199 (traversal) and kernels/force-kernels.m4
+// (P2P, E2P, E2L, L2P).  An MRAG block of 32 x 32 targets is 16 bricks of 8 x 8
+// (treecode-force.cpp:110-111), brick q = (by/8)*4 + bx/8.
+//
+// 1. k_force_lists<false>: one warp per brick walks the tree 32 nodes at a time and classifies
+//    every node with the reference's two criteria (treecode-force.cpp:136-151):
+//      E2L  iff  dist(brick centre, com)/r - 1 > 1/theta  and  r_brick <= r
+//      E2P  iff  r^2 < theta^2 |clamp(com to brick) - com|^2
+//      else P2P for a leaf, descend for an inner node.
+//    Counts per brick and kind are compacted with warp ballots.  The arithmetic is the one
+//    the compiled reference executes (fma(dx, dx, dy*dy), brick centre fma(bx + 3.5, h, x0),
+//    r_brick = 4.949747468305833 h), so every decision is the reference's.
+// 2. exclusive scan of the 3 x nbricks counts -> list offsets (E2L | E2P | P2P lists).
+// 3. k_force_lists<true>: same walk, writes node ids into the lists.
+// 4. k_force_eval: one warp per brick, 2 targets per lane; local expansion from the E2L list
+//    (lane l owns coefficient l), L2P, E2P from the E2P list, P2P over the leaves of the P2P
+//    list with source tiles staged in shared memory; results written straight into the
+//    ix + 32*(iy + 32*ib) layout (treecode-force.cpp:191-197).
+#include <cfloat>
+
+#include "tc_internal.h"
+#include "tc_math.cuh"
+
+namespace tc {
+
+__constant__ BinomTable c_binom_f = make_binom_table();
+
+struct Brick {
+    double x0b, y0b;        // brick centre
+    double rbrick;          // sqrt(2) * h * 3.5
+    double xlo, xhi, ylo, yhi;
+    double h;
+};
+
+__device__ __forceinline__ Brick brick_geometry(double x0, double y0, double h, int q) {
+    const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
+    Brick b;
+    b.h = h;
+    b.x0b = __fma_rn((double)bx + 3.5, h, x0);
+    b.y0b = __fma_rn((double)by + 3.5, h, y0);
+    b.rbrick = __dmul_rn(4.949747468305833, h);
+    b.xlo = __fma_rn((double)bx, h, x0);
+    b.xhi = __fma_rn((double)(bx + TILE - 1), h, x0);
+    b.ylo = __fma_rn((double)by, h, y0);
+    b.yhi = __fma_rn((double)(by + TILE - 1), h, y0);
+    return b;
+}
+
+enum { K_E2L = 0, K_E2P = 1, K_P2P = 2, K_DESCEND = 3, K_SKIP = 4 };
+
+__device__ __forceinline__ int classify(const TNode &nd, const Brick &b, double inv_theta,
+                                        double theta2) {
+    const double dx = __dsub_rn(b.x0b, nd.xcom), dy = __dsub_rn(b.y0b, nd.ycom);
+    const double dist = __dsqrt_rn(__fma_rn(dx, dx, __dmul_rn(dy, dy)));
+    if (__dsub_rn(__ddiv_rn(dist, nd.r), 1.0) > inv_theta && b.rbrick <= nd.r) return K_E2L;
+    const double xt = fmax(b.xlo, fmin(b.xhi, nd.xcom));
+    const double yt = fmax(b.ylo, fmin(b.yhi, nd.ycom));
+    const double ex = __dsub_rn(xt, nd.xcom), ey = __dsub_rn(yt, nd.ycom);
+    const double r2 = __fma_rn(ex, ex, __dmul_rn(ey, ey));
+    if (__dmul_rn(nd.r, nd.r) < __dmul_rn(theta2, r2)) return K_E2P;
+    if (nd.child < 0) return nd.count > 0 ? K_P2P : K_SKIP;
+    return K_DESCEND;
+}
+
+constexpr int TR_WARPS = 4;
+constexpr int TR_STACK = 2048;
+
+template <bool FILL>
+__global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
+    int nbricks, const double *__restrict__ x0s, const double *__restrict__ y0s,
+    const double *__restrict__ hs, double theta, const TNode *__restrict__ tnode, int nnodes,
+    int *__restrict__ counts, const int *__restrict__ offs, int *__restrict__ lists,
+    unsigned *err) {
+    __shared__ int stack_all[TR_WARPS][TR_STACK];
+    const int lane = lane_id(), warp = threadIdx.x >> 5;
+    int *stack = stack_all[warp];
+    const double inv_theta = 1.0 / theta, theta2 = theta * theta;
+    const unsigned lt = lanemask_lt();
+
+    for (int brick = blockIdx.x * TR_WARPS + warp; brick < nbricks;
+         brick += gridDim.x * TR_WARPS) {
+        const int blk = brick >> 4;
+        const Brick b = brick_geometry(x0s[blk], y0s[blk], hs[blk], brick & 15);
+        int o[3] = {0, 0, 0}, lim[3] = {0, 0, 0};
+        if (FILL) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                o[k] = offs[k * nbricks + brick];
+                lim[k] = offs[k * nbricks + brick + 1];
+            }
+        }
+        int n[3] = {0, 0, 0};
+        if (lane == 0) stack[0] = 0;
+        int top = 1;
+        __syncwarp();
+        while (top > 0) {
+            const int take = min(top, 32);
+            top -= take;
+            int node = -1, kind = K_SKIP, child = -1;
+            if (lane < take) {
+                node = stack[top + lane];
+                if ((unsigned)node < (unsigned)nnodes) {
+                    const TNode nd = tnode[node];
+                    kind = classify(nd, b, inv_theta, theta2);
+                    child = nd.child;
+                    if (kind == K_DESCEND && (child <= node || child + 4 > nnodes)) {
+                        atomicOr(err, DEVERR_BOUNDS);
+                        kind = K_SKIP;
+                    }
+                } else {
+                    atomicOr(err, DEVERR_BOUNDS);
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const unsigned bal = __ballot_sync(FULL_MASK, kind == k);
+                if (FILL && kind == k) {
+                    const int at = o[k] + n[k] + __popc(bal & lt);
+                    if (at < lim[k]) lists[at] = node;
+                    else atomicOr(err, DEVERR_BOUNDS);
+                }
+                n[k] += __popc(bal);
+            }
+            const unsigned bd = __ballot_sync(FULL_MASK, kind == K_DESCEND);
+            const int nd4 = 4 * __popc(bd);
+            if (top + nd4 > TR_STACK) {
+                if (lane == 0) atomicOr(err, DEVERR_STACK);
+                break;
+            }
+            if (kind == K_DESCEND) {
+                const int pos = top + 4 * __popc(bd & lt);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) stack[pos + c] = child + c;
+            }
+            top += nd4;
+            __syncwarp();
+        }
+        if (!FILL && lane == 0) {
+            counts[brick] = n[0];
+            counts[nbricks + brick] = n[1];
+            counts[2 * nbricks + brick] = n[2];
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------------------ evaluation
+constexpr int EV_WARPS = 4;
+constexpr int EV_CHUNK = 32;
+
+template <int P>
+struct EvalShared {
+    cplx coef[P];                 // E2L: a_k z^-(k+1); E2P: (k+1) a_k
+    cplx local[P + 1];            // local expansion L_1..L_P
+    double2 sxy[EV_CHUNK];        // P2P source tile
+    double sv[EV_CHUNK];
+};
+
+// z^e for e = 1..31 by binary powering
+__device__ __forceinline__ cplx cpow_int(cplx z, int e) {
+    cplx r = {1.0, 0.0};
+    cplx b = z;
+#pragma unroll
+    for (int bit = 0; bit < 5; ++bit) {
+        if (e & (1 << bit)) r = cmul(r, b);
+        b = cmul(b, b);
+    }
+    return r;
+}
+
+template <int P>
+__global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
+    int nbricks, const double *__restrict__ x0s, const double *__restrict__ y0s,
+    const double *__restrict__ hs, const TNode *__restrict__ tnode,
+    const double *__restrict__ mass, const double *__restrict__ exps,
+    const int2 *__restrict__ range, const double *__restrict__ xs,
+    const double *__restrict__ ys, const double *__restrict__ vs,
+    const int *__restrict__ offs, const int *__restrict__ lists, double *__restrict__ xout,
+    double *__restrict__ yout) {
+    __shared__ EvalShared<P> shared[EV_WARPS];
+    const int lane = lane_id(), warp = threadIdx.x >> 5;
+    EvalShared<P> &sh = shared[warp];
+    const int tx = lane & 7, ty = lane >> 3;   // targets (tx, ty) and (tx, ty + 4)
+    const double eps = 10 * DBL_EPSILON;
+
+    // signed binomials of lane l = lane + 1: (-1)^k C(l+k-1, k-1), k = 1..P
+    double bsg[P];
+    {
+        const int l = lane < P ? lane + 1 : 1;
+#pragma unroll
+        for (int k = 1; k <= P; ++k)
+            bsg[k - 1] = (k & 1 ? -1.0 : 1.0) * c_binom_f.c[l + k - 1][k - 1];
+    }
+
+    for (int brick = blockIdx.x * EV_WARPS + warp; brick < nbricks;
+         brick += gridDim.x * EV_WARPS) {
+        const int blk = brick >> 4, q = brick & 15;
+        const double h = hs[blk];
+        const Brick b = brick_geometry(x0s[blk], y0s[blk], h, q);
+        double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
+
+        // ---------------- E2L: local expansion about the brick centre (force-kernels.m4:102-155)
+        {
+            const int beg = offs[brick], end = offs[brick + 1];
+            cplx L = {0.0, 0.0};
+            const int l = lane + 1;
+            const double minv = -1.0 / l;
+            for (int it = beg; it < end; ++it) {
+                const int node = lists[it];
+                const TNode nd = tnode[node];
+                const double m = mass[node];
+                const double zx = nd.xcom - b.x0b, zy = nd.ycom - b.y0b;
+                const double r2z0 = zx * zx + zy * zy;
+                const cplx zinv = {zx / r2z0, -zy / r2z0};
+                cplx zl = {0.0, 0.0};
+                if (lane < P) {
+                    zl = cpow_int(zinv, l);   // z0^-l
+                    const double *ex = exps + (size_t)node * 2 * P;
+                    const cplx a = {ex[lane], ex[P + lane]};
+                    sh.coef[lane] = cmul(a, zl);   // C_l = a_{l-1} z0^-l
+                }
+                __syncwarp();
+                if (lane < P) {
+                    double tr = l == 1 ? -m : m * minv, ti = 0.0;
+#pragma unroll
+                    for (int k = 0; k < P; ++k) {
+                        const cplx ck = sh.coef[k];
+                        tr = fma(bsg[k], ck.re, tr);
+                        ti = fma(bsg[k], ck.im, ti);
+                    }
+                    L = cfma({tr, ti}, zl, L);
+                }
+                __syncwarp();
+            }
+            if (lane < P) sh.local[lane + 1] = L;
+            __syncwarp();
+        }
+
+        // ---------------- L2P (force-kernels.m4:157-191): sum_l l L_l z^(l-1), z about the centre
+        {
+            const double xr = -3.5 * h + tx * h;
+            const double yr0 = -3.5 * h + ty * h, yr1 = -3.5 * h + (ty + 4) * h;
+            cplx acc0 = {P * sh.local[P].re, P * sh.local[P].im}, acc1 = acc0;
+            const cplx z0 = {xr, yr0}, z1 = {xr, yr1};
+#pragma unroll
+            for (int l = P - 1; l >= 1; --l) {
+                const cplx cl = {l * sh.local[l].re, l * sh.local[l].im};
+                acc0 = cfma(acc0, z0, cl);
+                acc1 = cfma(acc1, z1, cl);
+            }
+            ax0 += acc0.re;
+            ay0 -= acc0.im;
+            ax1 += acc1.re;
+            ay1 -= acc1.im;
+        }
+
+        // ---------------- E2P (force-kernels.m4:57-98): w = m/z - sum (j+1) a_j z^-(j+2)
+        {
+            const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
+            for (int it = beg; it < end; ++it) {
+                const int node = lists[it];
+                const TNode nd = tnode[node];
+                const double m = mass[node];
+                __syncwarp();
+                if (lane < P) {
+                    const double *ex = exps + (size_t)node * 2 * P;
+                    sh.coef[lane] = {(lane + 1) * ex[lane], (lane + 1) * ex[P + lane]};
+                }
+                __syncwarp();
+                const double rx = (b.xlo - nd.xcom) + tx * h;
+                const double ry0 = (b.ylo - nd.ycom) + ty * h;
+                const double ry1 = (b.ylo - nd.ycom) + (ty + 4) * h;
+                const double i0 = rcp_nr(rx * rx + ry0 * ry0);
+                const double i1 = rcp_nr(rx * rx + ry1 * ry1);
+                const cplx u0 = {rx * i0, -ry0 * i0}, u1 = {rx * i1, -ry1 * i1};
+                cplx q0 = sh.coef[P - 1], q1 = q0;
+#pragma unroll
+                for (int j = P - 2; j >= 0; --j) {
+                    const cplx d = sh.coef[j];
+                    q0 = cfma(q0, u0, d);
+                    q1 = cfma(q1, u1, d);
+                }
+                // w = u (m - u q)
+                const cplx t0 = cmul(u0, q0), t1 = cmul(u1, q1);
+                const cplx w0 = cmul(u0, {m - t0.re, -t0.im});
+                const cplx w1 = cmul(u1, {m - t1.re, -t1.im});
+                ax0 += w0.re;
+                ay0 -= w0.im;
+                ax1 += w1.re;
+                ay1 -= w1.im;
+            }
+        }
+
+        // ---------------- P2P (force-kernels.m4:15-55): sum v (xr, yr) / (xr^2 + yr^2 + eps)
+        {
+            const int beg = offs[2 * nbricks + brick], end = offs[2 * nbricks + brick + 1];
+            const double xt = b.xlo + tx * h;
+            const double yt0 = b.ylo + ty * h, yt1 = b.ylo + (ty + 4) * h;
+            for (int it = beg; it < end; ++it) {
+                const int2 rg = range[lists[it]];
+                for (int s0 = rg.x; s0 < rg.y; s0 += EV_CHUNK) {
+                    const int cnt = min(EV_CHUNK, rg.y - s0);
+                    __syncwarp();
+                    if (lane < cnt) {
+                        sh.sxy[lane] = make_double2(xs[s0 + lane], ys[s0 + lane]);
+                        sh.sv[lane] = vs[s0 + lane];
+                    }
+                    __syncwarp();
+                    for (int k = 0; k < cnt; ++k) {
+                        const double2 sp = sh.sxy[k];
+                        const double v = sh.sv[k];
+                        const double xr = xt - sp.x;
+                        const double xr2e = fma(xr, xr, eps);
+                        const double yr0 = yt0 - sp.y, yr1 = yt1 - sp.y;
+                        const double f0 = v * rcp_nr(fma(yr0, yr0, xr2e));
+                        const double f1 = v * rcp_nr(fma(yr1, yr1, xr2e));
+                        ax0 = fma(xr, f0, ax0);
+                        ay0 = fma(yr0, f0, ay0);
+                        ax1 = fma(xr, f1, ax1);
+                        ay1 = fma(yr1, f1, ay1);
+                    }
+                }
+            }
+        }
+
+        const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
+        const size_t o0 = (size_t)blk * BLOCKSIZE * BLOCKSIZE + (by + ty) * BLOCKSIZE + bx + tx;
+        const size_t o1 = o0 + 4 * BLOCKSIZE;
+        xout[o0] = ax0;
+        yout[o0] = ay0;
+        xout[o1] = ax1;
+        yout[o1] = ay1;
+        __syncwarp();
+    }
+}
+
+static int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
+               int nblocks, double *xout, double *yout) {
+    if (c.order != ORDER_FORCE) {
+        set_error(TC_ERR_INVALID, "force evaluation needs an order-%d tree", ORDER_FORCE);
+        return TC_ERR_INVALID;
+    }
+    const int nbricks = nblocks * 16;
+    if (nbricks == 0) return TC_OK;
+    int rc;
+    int *counts, *offs;
+    if ((rc = ensure(c, S_FCOUNT, (size_t)3 * nbricks, &counts)) ||
+        (rc = ensure(c, S_FOFF, (size_t)3 * nbricks + 1, &offs)))
+        return rc;
+    const TNode *tnode = slot_ptr<TNode>(c, S_TNODE);
+    unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    const int trgrid = (int)std::min<long long>((nbricks + TR_WARPS - 1) / TR_WARPS,
+                                                (long long)sm_count() * 16);
+    k_force_lists<false><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(nbricks, x0s, y0s, hs, theta,
+                                                                 tnode, c.nnodes, counts, nullptr, nullptr,
+                                                                 err);
+    TC_KERNEL_CHECK();
+    if ((rc = exclusive_scan(c, counts, offs, 3 * nbricks))) return rc;
+    int tot[4];
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, offs + nbricks, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 1, offs + 2 * nbricks, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 2, offs + 3 * nbricks, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    tot[0] = (int)c.h_pinned[0];
+    tot[1] = (int)c.h_pinned[1];
+    tot[2] = (int)c.h_pinned[2];
+    c.counts.n_e2l = tot[0];
+    c.counts.n_e2p = tot[1] - tot[0];
+    c.counts.n_p2p = tot[2] - tot[1];
+    int *lists;
+    if ((rc = ensure(c, S_E2L, (size_t)tot[2] + 1, &lists))) return rc;
+    k_force_lists<true><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(nbricks, x0s, y0s, hs, theta,
+                                                                tnode, c.nnodes, nullptr, offs, lists, err);
+    TC_KERNEL_CHECK();
+    phase_mark(c, 4);
+    const int evgrid = (int)std::min<long long>((nbricks + EV_WARPS - 1) / EV_WARPS,
+                                                (long long)sm_count() * 8);
+    k_force_eval<ORDER_FORCE><<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
+        nbricks, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
+        slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
+        slot_ptr<double>(c, S_VS), offs, lists, xout, yout);
+    TC_KERNEL_CHECK();
+    return TC_OK;
+}
+
+}  // namespace tc

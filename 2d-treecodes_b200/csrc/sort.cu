@@ -1,0 +1,508 @@
+// sort.cu -- bounding square, Morton keys, LSD radix sort with a stable permutation, and the
+// source gather.  Restates drivers/sort-sources.cpp:23-132 of the reference.
+//
+// Data flow per solve (N sources, all FP64 SoA in HBM):
+//   k_bbox          x, y           -> Frame (xmin, ymin, ext, scale)       2 x 8 B/src read
+//   k_keys          x, y, Frame    -> keys (30-bit Morton)                 16 B read, 4 B write
+//   radix sort      keys (+ index) -> sorted keys, permutation             4 onesweep passes
+//   k_gather        x, y, v, perm  -> sorted x, y, v                       24 B gathered, 24 B written
+//
+// The radix sort is a one-pass-per-digit ("onesweep") LSD sort: every CTA ranks a tile of
+// 4096 keys in shared memory with warp-level match_any, publishes its per-digit counts, and
+// finds its global offsets by a decoupled look-back over the tiles before it.  Tiles take
+// their ids from an atomic counter, so each waits only on tiles that already run; the waits
+// are bounded and raise DEVERR_SPIN_LIMIT instead of hanging.
+#include <cfloat>
+#include <cmath>
+
+#include "tc_internal.h"
+
+namespace tc {
+
+// ---------------------------------------------------------------------------- bbox
+constexpr int BBOX_THREADS = 256;
+
+__device__ __forceinline__ void warp_minmax(double &a, double &b, double &c, double &d) {
+    for (int m = 16; m; m >>= 1) {
+        a = fmin(a, shfl_xor_d(a, m));
+        b = fmax(b, shfl_xor_d(b, m));
+        c = fmin(c, shfl_xor_d(c, m));
+        d = fmax(d, shfl_xor_d(d, m));
+    }
+}
+
+// Per-CTA min/max, then the last CTA to finish reduces the partials and derives the frame.
+// Initial extrema follow upward-common.ispc:132 (min 1e13, max 0) and sort-sources.cpp:48.
+__global__ __launch_bounds__(BBOX_THREADS) void k_bbox(const double *__restrict__ x,
+                                                       const double *__restrict__ y, int n,
+                                                       double4 *partials, unsigned *done,
+                                                       Frame *frame) {
+    double xmi = 1e13, xma = 0, ymi = 1e13, yma = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double xv = x[i], yv = y[i];
+        xmi = fmin(xmi, xv);
+        xma = fmax(xma, xv);
+        ymi = fmin(ymi, yv);
+        yma = fmax(yma, yv);
+    }
+    warp_minmax(xmi, xma, ymi, yma);
+    __shared__ double4 s[BBOX_THREADS / 32];
+    __shared__ bool last;
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 0) s[w] = make_double4(xmi, xma, ymi, yma);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double4 r = s[0];
+        for (int i = 1; i < BBOX_THREADS / 32; ++i) {
+            r.x = fmin(r.x, s[i].x); r.y = fmax(r.y, s[i].y);
+            r.z = fmin(r.z, s[i].z); r.w = fmax(r.w, s[i].w);
+        }
+        partials[blockIdx.x] = r;
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    xmi = 1e13; xma = 0; ymi = 1e13; yma = 0;
+    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+        const double2 ra = __ldcg(reinterpret_cast<const double2 *>(&partials[i]));
+        const double2 rb = __ldcg(reinterpret_cast<const double2 *>(&partials[i]) + 1);
+        xmi = fmin(xmi, ra.x); xma = fmax(xma, ra.y);
+        ymi = fmin(ymi, rb.x); yma = fmax(yma, rb.y);
+    }
+    warp_minmax(xmi, xma, ymi, yma);
+    __syncthreads();
+    if (lane_id() == 0) s[w] = make_double4(xmi, xma, ymi, yma);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double4 r = s[0];
+        for (int i = 1; i < BBOX_THREADS / 32; ++i) {
+            r.x = fmin(r.x, s[i].x); r.y = fmax(r.y, s[i].y);
+            r.z = fmin(r.z, s[i].z); r.w = fmax(r.w, s[i].w);
+        }
+        // sort-sources.cpp:98-110, with the arithmetic the compiled reference executes:
+        // ext = max(ex, ey) * (1 + 2 eps); xmin -= eps * ext; keys use (1/ext) * 2^15.
+        const double eps = 10000.0 * DBL_EPSILON;
+        const double ext0 = __dsub_rn(r.y, r.x);
+        const double ext1 = __dsub_rn(r.w, r.z);
+        const double ext = __dmul_rn(ext0 < ext1 ? ext1 : ext0, 1.0 + 2.0 * eps);
+        Frame f;
+        f.xmin = __dsub_rn(r.x, __dmul_rn(eps, ext));
+        f.ymin = __dsub_rn(r.z, __dmul_rn(eps, ext));
+        f.ext = ext;
+        f.scale = __dmul_rn(__ddiv_rn(1.0, ext), (double)(1 << LMAX));
+        *frame = f;
+        *done = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------- keys
+// sort-sources.cpp:114-137: x = floor((x - xmin) * scale), bits interleaved, x on even bits.
+__device__ __forceinline__ int quantize(double v, double vmin, double scale) {
+    return (int)floor(__dmul_rn(__dsub_rn(v, vmin), scale));
+}
+
+__global__ void k_keys(const double *__restrict__ x, const double *__restrict__ y, int n,
+                       const Frame *__restrict__ frame, int *__restrict__ keys) {
+    const Frame f = *frame;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int kx = quantize(x[i], f.xmin, f.scale);
+        const int ky = quantize(y[i], f.ymin, f.scale);
+        keys[i] = spread_bits(kx) | (spread_bits(ky) << 1);
+    }
+}
+
+// Target keys in the source frame, clamped to the quantisation range (targets may lie outside
+// the sources' square).  Used only to group nearby targets; it does not affect results.
+__global__ void k_target_keys(const double *__restrict__ x, const double *__restrict__ y, int n,
+                              const Frame *__restrict__ frame, int *__restrict__ keys) {
+    const Frame f = *frame;
+    const double hi = (double)((1 << LMAX) - 1);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double qx = floor((x[i] - f.xmin) * f.scale);
+        double qy = floor((y[i] - f.ymin) * f.scale);
+        qx = fmin(fmax(qx, 0.0), hi);
+        qy = fmin(fmax(qy, 0.0), hi);
+        if (qx != qx) qx = 0;
+        if (qy != qy) qy = 0;
+        keys[i] = spread_bits((int)qx) | (spread_bits((int)qy) << 1);
+    }
+}
+
+__global__ void k_gather3(const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ v, const int *__restrict__ perm, int n,
+                          double *__restrict__ xs, double *__restrict__ ys,
+                          double *__restrict__ vs, unsigned *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int j = perm[i];
+        if ((unsigned)j >= (unsigned)n) {
+            atomicOr(err, DEVERR_BOUNDS);
+            continue;
+        }
+        xs[i] = x[j];
+        ys[i] = y[j];
+        vs[i] = v[j];
+    }
+}
+
+// ---------------------------------------------------------------------------- radix sort
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_RADIX = 256;
+constexpr unsigned RS_FLAG_AGG = 1u << 30;
+constexpr unsigned RS_FLAG_INC = 2u << 30;
+constexpr unsigned RS_VALMASK = (1u << 30) - 1;
+constexpr int RS_SPIN_LIMIT = 1 << 22;
+constexpr int RS_MAX_PASSES = 4;
+
+// Histograms of every 8-bit digit of the keys, in one read.
+__global__ __launch_bounds__(256) void k_hist(const int *__restrict__ keys, int n, int npasses,
+                                              int *__restrict__ hist) {
+    __shared__ int s[RS_MAX_PASSES][RS_RADIX];
+    for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned k = (unsigned)keys[i];
+        for (int p = 0; p < npasses; ++p) atomicAdd(&s[p][(k >> (8 * p)) & 0xFF], 1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npasses * RS_RADIX; i += blockDim.x) {
+        const int c = (&s[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x a multiple of 32, <= 1024).
+__device__ int block_exclusive_scan(int v, int *total) {
+    __shared__ int warp_sums[32];
+    const int lane = lane_id(), w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL_MASK, inc, o);
+        if (lane >= o) inc += t;
+    }
+    __syncthreads();
+    if (lane == 31) warp_sums[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < nw ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(FULL_MASK, s, o);
+            if (lane >= o) s += t;
+        }
+        if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    const int base = w ? warp_sums[w - 1] : 0;
+    if (total) *total = warp_sums[nw - 1];
+    return base + inc - v;
+}
+
+__global__ __launch_bounds__(RS_RADIX) void k_hist_scan(const int *__restrict__ hist,
+                                                        int *__restrict__ offsets) {
+    const int p = blockIdx.x;
+    const int v = hist[p * RS_RADIX + threadIdx.x];
+    offsets[p * RS_RADIX + threadIdx.x] = block_exclusive_scan(v, nullptr);
+}
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) {
+    return *(const volatile unsigned *)p;
+}
+
+__global__ __launch_bounds__(RS_THREADS) void k_onesweep(
+    const int *__restrict__ keys_in, const int *__restrict__ vals_in, int *__restrict__ keys_out,
+    int *__restrict__ vals_out, int n, int shift, const int *__restrict__ digit_offsets,
+    unsigned *status, int *tile_counter, unsigned *err) {
+    __shared__ int s_keys[RS_TILE];
+    __shared__ int s_vals[RS_TILE];
+    __shared__ int s_whist[RS_WARPS][RS_RADIX];
+    __shared__ int s_tile_start[RS_RADIX];
+    __shared__ int s_global[RS_RADIX];
+    __shared__ int s_tile;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1);
+    for (int i = tid; i < RS_WARPS * RS_RADIX; i += RS_THREADS) (&s_whist[0][0])[i] = 0;
+    __syncthreads();
+    const int tile = s_tile;
+    const int tile_base = tile * RS_TILE;
+    const int warp_base = tile_base + warp * (RS_ITEMS * 32);
+
+    int key[RS_ITEMS], val[RS_ITEMS], rank[RS_ITEMS];
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        const bool valid = idx < n;
+        key[k] = valid ? keys_in[idx] : 0;
+        val[k] = valid ? (vals_in ? vals_in[idx] : idx) : 0;
+    }
+
+    // Stable rank within the warp: items are visited in their original order (k, lane).
+    const unsigned lt = lanemask_lt();
+    int *hist = s_whist[warp];
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        const bool valid = idx < n;
+        const unsigned vmask = __ballot_sync(FULL_MASK, valid);
+        const int d = (key[k] >> shift) & 0xFF;
+        unsigned peers = 0;
+        if (valid) peers = __match_any_sync(vmask, d);
+        const int old = valid ? hist[d] : 0;
+        __syncwarp();
+        if (valid && (peers & lt) == 0) hist[d] = old + __popc(peers);
+        __syncwarp();
+        rank[k] = old + __popc(peers & lt);
+    }
+    __syncthreads();
+
+    // Thread `tid` owns digit `tid`: exclusive prefix over warps and the tile's count.
+    const int d = tid;
+    int total = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) {
+        const int c = s_whist[w][d];
+        s_whist[w][d] = total;
+        total += c;
+    }
+
+    // Decoupled look-back for this digit.
+    unsigned *mine = status + (size_t)tile * RS_RADIX + d;
+    int excl = 0;
+    if (tile == 0) {
+        atomicExch(mine, RS_FLAG_INC | (unsigned)total);
+    } else {
+        atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
+        int j = tile - 1;
+        int spins = 0;
+        while (j >= 0) {
+            const unsigned s = ld_volatile(status + (size_t)j * RS_RADIX + d);
+            const unsigned flag = s & ~RS_VALMASK;
+            if (flag == 0) {
+                if (++spins > RS_SPIN_LIMIT) {
+                    atomicOr(err, DEVERR_SPIN_LIMIT);
+                    break;
+                }
+                continue;
+            }
+            excl += (int)(s & RS_VALMASK);
+            if (flag == RS_FLAG_INC) break;
+            --j;
+        }
+        atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
+    }
+
+    const int start = block_exclusive_scan(total, nullptr);
+    s_tile_start[d] = start;
+    s_global[d] = digit_offsets[d] + excl - start;
+    __syncthreads();
+
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        if (idx < n) {
+            const int dk = (key[k] >> shift) & 0xFF;
+            const int pos = s_tile_start[dk] + s_whist[warp][dk] + rank[k];
+            if ((unsigned)pos >= (unsigned)RS_TILE) {
+                atomicOr(err, DEVERR_BOUNDS);
+                continue;
+            }
+            s_keys[pos] = key[k];
+            s_vals[pos] = val[k];
+        }
+    }
+    __syncthreads();
+
+    const int tile_n = min(RS_TILE, n - tile_base);
+    for (int j = tid; j < tile_n; j += RS_THREADS) {
+        const int kk = s_keys[j];
+        const int g = s_global[(kk >> shift) & 0xFF] + j;
+        if ((unsigned)g >= (unsigned)n) {
+            atomicOr(err, DEVERR_BOUNDS);
+            continue;
+        }
+        keys_out[g] = kk;
+        vals_out[g] = s_vals[j];
+    }
+}
+
+static int grid_for(int n, int threads, int per_sm = 8) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long g = ((long long)n + threads - 1) / threads;
+    long long cap = (long long)sms * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, int nbits,
+                     int *keys_a, int *vals_a, int *keys_b, int *vals_b, int **keys_out,
+                     int **vals_out) {
+    if (n >= (1 << 30)) {
+        set_error(TC_ERR_INVALID, "radix sort supports fewer than 2^30 keys (got %d)", n);
+        return TC_ERR_INVALID;
+    }
+    const int npasses = (nbits + 7) / 8;
+    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    int *hist, *counter;
+    unsigned *status;
+    int rc;
+    if ((rc = ensure(c, S_RS_HIST, 2 * RS_MAX_PASSES * RS_RADIX, &hist))) return rc;
+    if ((rc = ensure(c, S_RS_COUNTER, RS_MAX_PASSES, &counter))) return rc;
+    if ((rc = ensure(c, S_RS_STATUS, (size_t)RS_MAX_PASSES * ntiles * RS_RADIX, &status))) return rc;
+    int *offsets = hist + RS_MAX_PASSES * RS_RADIX;
+    TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * RS_MAX_PASSES * RS_RADIX, c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
+                                c.stream));
+    k_hist<<<grid_for(n, 256, 4), 256, 0, c.stream>>>(keys_in, n, npasses, hist);
+    TC_KERNEL_CHECK();
+    k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
+    TC_KERNEL_CHECK();
+    unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+
+    const int *ki = keys_in, *vi = vals_in;
+    int *ko = keys_a, *vo = vals_a;
+    for (int p = 0; p < npasses; ++p) {
+        k_onesweep<<<ntiles, RS_THREADS, 0, c.stream>>>(ki, vi, ko, vo, n, 8 * p,
+                                                         offsets + p * RS_RADIX,
+                                                         status + (size_t)p * ntiles * RS_RADIX,
+                                                         counter + p, err);
+        TC_KERNEL_CHECK();
+        ki = ko;
+        vi = vo;
+        if (ko == keys_a) { ko = keys_b; vo = vals_b; }
+        else { ko = keys_a; vo = vals_a; }
+    }
+    *keys_out = const_cast<int *>(ki);
+    *vals_out = const_cast<int *>(vi);
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------- scan
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(const int *__restrict__ in, int n,
+                                                             int *__restrict__ block_sums) {
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i)
+        if (base + i < n) s += in[base + i];
+    int total;
+    block_exclusive_scan(s, &total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_blocks(int *block_sums, int nb,
+                                                             int *out_total) {
+    // one CTA: each thread scans a contiguous chunk of the block sums
+    const int per = (nb + SCAN_THREADS - 1) / SCAN_THREADS;
+    const int b0 = threadIdx.x * per;
+    int s = 0;
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < nb) s += block_sums[b0 + i];
+    int total;
+    int run = block_exclusive_scan(s, &total);
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < nb) {
+            const int v = block_sums[b0 + i];
+            block_sums[b0 + i] = run;
+            run += v;
+        }
+    if (threadIdx.x == 0) *out_total = total;
+}
+
+__global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(const int *__restrict__ in, int n,
+                                                            const int *__restrict__ block_offs,
+                                                            int *__restrict__ out) {
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        v[i] = base + i < n ? in[base + i] : 0;
+        s += v[i];
+    }
+    int run = block_exclusive_scan(s, nullptr) + block_offs[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i)
+        if (base + i < n) {
+            out[base + i] = run;
+            run += v[i];
+        }
+}
+
+int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
+    const int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    int *bs;
+    int rc;
+    if ((rc = ensure(c, S_SCAN_BLOCKS, (size_t)nb + 1, &bs))) return rc;
+    if (n == 0) {
+        TC_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(int), c.stream));
+        return TC_OK;
+    }
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, c.stream>>>(d_in, n, bs);
+    TC_KERNEL_CHECK();
+    k_scan_blocks<<<1, SCAN_THREADS, 0, c.stream>>>(bs, nb, d_out + n);
+    TC_KERNEL_CHECK();
+    k_scan_apply<<<nb, SCAN_THREADS, 0, c.stream>>>(d_in, n, bs, d_out);
+    TC_KERNEL_CHECK();
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------- drivers
+int sort_sources(Context &c, const double *x, const double *y, const double *v, int n) {
+    int rc;
+    double *xs, *ys, *vs;
+    int *keys, *perm, *keys2, *perm2;
+    Frame *frame;
+    double4 *partials;
+    if ((rc = ensure(c, S_XS, n, &xs)) || (rc = ensure(c, S_YS, n, &ys)) ||
+        (rc = ensure(c, S_VS, n, &vs)) || (rc = ensure(c, S_KEYS, n, &keys)) ||
+        (rc = ensure(c, S_PERM, n, &perm)) || (rc = ensure(c, S_KEYS2, n, &keys2)) ||
+        (rc = ensure(c, S_PERM2, n, &perm2)))
+        return rc;
+    // frame + bbox partials + completion counter share one small buffer
+    const int gb = grid_for(n, BBOX_THREADS, 4);
+    if ((rc = ensure(c, S_FRAME, sizeof(Frame) + sizeof(double4) * (gb + 1) + 64, (char **)&frame)))
+        return rc;
+    partials = reinterpret_cast<double4 *>(reinterpret_cast<char *>(frame) + 64);
+    unsigned *done = reinterpret_cast<unsigned *>(partials + gb);
+    TC_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned), c.stream));
+    k_bbox<<<gb, BBOX_THREADS, 0, c.stream>>>(x, y, n, partials, done, frame);
+    TC_KERNEL_CHECK();
+    k_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(x, y, n, frame, keys);
+    TC_KERNEL_CHECK();
+    int *ko, *vo;
+    // ping-pong keys -> keys2/perm2 -> keys/perm -> ...: an even number of passes (4 for
+    // 30-bit keys) ends in keys/perm.
+    if ((rc = radix_sort_pairs(c, keys, nullptr, n, 2 * LMAX, keys2, perm2, keys, perm, &ko, &vo)))
+        return rc;
+    if (ko != keys) {
+        TC_CUDA_TRY(cudaMemcpyAsync(keys, ko, sizeof(int) * n, cudaMemcpyDeviceToDevice, c.stream));
+        TC_CUDA_TRY(cudaMemcpyAsync(perm, vo, sizeof(int) * n, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    k_gather3<<<grid_for(n, 256), 256, 0, c.stream>>>(x, y, v, perm, n, xs, ys, vs,
+                                                       slot_ptr<unsigned>(c, S_ERR));
+    TC_KERNEL_CHECK();
+    c.nsrc = n;
+    return TC_OK;
+}
+
+int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys, int *idx) {
+    (void)idx;
+    Frame *frame = slot_ptr<Frame>(c, S_FRAME);
+    k_target_keys<<<grid_for(m, 256), 256, 0, c.stream>>>(xt, yt, m, frame, keys);
+    TC_KERNEL_CHECK();
+    return TC_OK;
+}
+
+}  // namespace tc

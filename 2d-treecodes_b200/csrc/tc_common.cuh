@@ -1,0 +1,111 @@
+// tc_common.cuh -- shared constants, error plumbing and device helpers of the B200 treecode.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "treecodes_b200.h"
+
+namespace tc {
+
+// Compile-time parameters of the reference build (Makefile:13-15 of the reference,
+// drivers/Makefile:20): expansion order 12 for the potential, 24 for the force, MRAG block
+// of 32 x 32 targets, deepest level 15, leaf capacities 512 / 192
+// (drivers/treecode-potential.cpp:99, drivers/treecode-force.cpp:216), bricks of 8 x 8
+// (drivers/treecode-force.cpp:91).
+constexpr int LMAX = 15;
+constexpr int BLOCKSIZE = 32;
+constexpr int TILE = 8;
+constexpr int ORDER_POTENTIAL = 12;
+constexpr int ORDER_FORCE = 24;
+constexpr int LEAF_POTENTIAL = 32 * 16;
+constexpr int LEAF_FORCE = 192;
+constexpr int MAX_ORDER = 32;
+
+// Status codes: tc_status of the C ABI (treecodes_b200.h).
+
+// Device-side error word bits (set by kernels, read by the host after the call).
+enum DeviceError : unsigned {
+    DEVERR_SPIN_LIMIT = 1u << 0,   // a bounded wait gave up
+    DEVERR_STACK = 1u << 1,        // traversal stack overflow
+    DEVERR_TREE = 1u << 2,         // inconsistent tree bookkeeping
+    DEVERR_BOUNDS = 1u << 3,       // an index failed its bounds check (access skipped)
+};
+
+// Coordinate frame of a source set: sort-sources.cpp:78-82 of the reference.
+struct Frame {
+    double xmin, ymin, ext;   // padded bounding square
+    double scale;             // (1 / ext) * 2^LMAX, the factor the compiled reference uses
+};
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Approximate FP64 reciprocal from the SFU (PTX rcp.approx.ftz.f64), refined by two
+// Newton-Raphson steps y <- y + y (1 - d y); each step doubles the number of correct bits.
+__device__ __forceinline__ double rcp_nr(double d) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    return y;
+}
+
+__device__ __forceinline__ double shfl_xor_d(double v, int m) {
+    return __shfl_xor_sync(FULL_MASK, v, m);
+}
+
+// Morton interleave of a 15-bit coordinate: sort-sources.cpp:96-104 of the reference.
+__host__ __device__ __forceinline__ int spread_bits(int x) {
+    x = (x | (x << 8)) & 0x00FF00FF;
+    x = (x | (x << 4)) & 0x0F0F0F0F;
+    x = (x | (x << 2)) & 0x33333333;
+    x = (x | (x << 1)) & 0x55555555;
+    return x;
+}
+
+__host__ __device__ __forceinline__ int compact_bits(int x) {
+    x &= 0x55555555;
+    x = (x | (x >> 1)) & 0x33333333;
+    x = (x | (x >> 2)) & 0x0F0F0F0F;
+    x = (x | (x >> 4)) & 0x00FF00FF;
+    x = (x | (x >> 8)) & 0x0000FFFF;
+    return x;
+}
+
+// Node record read by the traversals: centre of mass, radius, first child (-1: leaf) and the
+// number of sources the node hands to P2P (0 for empty leaves).
+struct __align__(32) TNode {
+    double xcom, ycom, r;
+    int child;
+    int count;
+};
+
+}  // namespace tc
+
+#define TC_CUDA_TRY(expr)                                                            \
+    do {                                                                             \
+        cudaError_t err__ = (expr);                                                  \
+        if (err__ != cudaSuccess) {                                                  \
+            ::tc::set_error(::TC_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__,       \
+                            #expr, cudaGetErrorString(err__));                       \
+            return ::TC_ERR_CUDA;                                                    \
+        }                                                                            \
+    } while (0)
+
+#define TC_KERNEL_CHECK()  TC_CUDA_TRY(cudaGetLastError())
+
+namespace tc {
+// Records status and message for treecode_last_status / treecode_last_error (thread-local).
+void set_error(int status, const char *fmt, ...);
+}

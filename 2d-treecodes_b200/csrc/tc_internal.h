@@ -1,0 +1,126 @@
+// tc_internal.h -- host-side state of one treecode context and the entry points shared
+// between the translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "tc_common.cuh"
+
+namespace tc {
+
+// Grow-only device allocation.  A context keeps its buffers between calls, so repeated
+// solves of similar size allocate nothing.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+enum Slot {
+    // inputs staged from host memory
+    S_XIN, S_YIN, S_VIN, S_XT, S_YT, S_X0, S_Y0, S_H, S_OUTX, S_OUTY,
+    // sorted sources
+    S_XS, S_YS, S_VS, S_KEYS, S_PERM, S_KEYS2, S_PERM2, S_FRAME,
+    // radix sort scratch
+    S_RS_STATUS, S_RS_HIST, S_RS_COUNTER,
+    // scan scratch
+    S_SCAN_BLOCKS,
+    // tree build
+    S_TMASK, S_TFLAG, S_TOFF, S_LPOS, S_LMASK, S_LRANK, S_LBLK, S_LEVEL_TOTALS,
+    // nodes
+    S_TNODE, S_RANGE, S_CELL, S_MASS, S_W, S_WX, S_WY, S_EXPS, S_UPCNT,
+    // force traversal / lists
+    S_FCOUNT, S_FOFF, S_E2L, S_E2P, S_P2P, S_BRICK_CTR,
+    // potential targets / lists
+    S_TKEYS, S_TPERM, S_TKEYS2, S_TPERM2, S_PCOUNT, S_POFF, S_PE2P, S_PP2P,
+    // misc
+    S_ERR, S_STATS,
+    S_NUM_SLOTS
+};
+
+struct PhaseTimes {
+    float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms;
+};
+
+struct Counts {
+    long long nnodes, nleaves, ninner, nlevels;
+    long long n_e2l, n_e2p, n_p2p;        // interaction-list entries
+    long long p2p_pairs;                  // source-target pairs evaluated directly
+    long long e2p_pairs;                  // (target, cell) pairs of far-field evaluation
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DevBuf buf[S_NUM_SLOTS];
+    unsigned *h_pinned = nullptr;         // small pinned staging area for readbacks
+    int precision = 0;                    // 0 = plain FP64, 1 = mixed
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    PhaseTimes times = {};
+    Counts counts = {};
+
+    // current tree
+    int nsrc = 0, order = 0, leafcap = 0;
+    int nnodes = 0, ninner = 0;
+    int level_off[LMAX + 3] = {};         // node id of the first node of each level
+    Frame frame_h = {};
+};
+
+template <class T>
+int ensure(Context &c, Slot s, size_t count, T **out) {
+    size_t need = count * sizeof(T);
+    if (need == 0) need = sizeof(T);
+    DevBuf &b = c.buf[s];
+    if (b.bytes < need) {
+        if (b.p) {
+            cudaError_t e = cudaStreamSynchronize(c.stream);
+            if (e != cudaSuccess) { set_error(TC_ERR_CUDA, "sync before realloc: %s", cudaGetErrorString(e)); return TC_ERR_CUDA; }
+            cudaFree(b.p);
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        size_t alloc = need + need / 8;   // headroom for the next call
+        cudaError_t e = cudaMalloc(&b.p, alloc);
+        if (e != cudaSuccess) {
+            set_error(TC_ERR_ALLOC, "cudaMalloc(%zu bytes) failed: %s", alloc, cudaGetErrorString(e));
+            return TC_ERR_ALLOC;
+        }
+        b.bytes = alloc;
+    }
+    *out = static_cast<T *>(b.p);
+    return TC_OK;
+}
+
+template <class T>
+T *slot_ptr(Context &c, Slot s) { return static_cast<T *>(c.buf[s].p); }
+
+// ---- sort.cu
+int exclusive_scan(Context &c, const int *d_in, int *d_out, int n);   // d_out has n+1 entries
+int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, int nbits,
+                     int *keys_a, int *vals_a, int *keys_b, int *vals_b, int **keys_out,
+                     int **vals_out);
+int sort_sources(Context &c, const double *x, const double *y, const double *v, int n);
+int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys, int *idx);
+
+// ---- tree.cu
+int build_topology(Context &c, int leafcap);
+
+// ---- upward.cu
+int upward_pass(Context &c, int order);
+
+// ---- force.cu
+int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
+               int nblocks, double *xout, double *yout);
+
+// ---- potential.cu
+int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out);
+
+// ---- capi.cu
+int check_device_errors(Context &c, const char *where);
+void phase_mark(Context &c, int idx);
+
+}  // namespace tc

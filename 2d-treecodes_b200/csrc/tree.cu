@@ -1,0 +1,322 @@
+// tree.cu -- quadtree topology from the sorted Morton keys.
+//
+// Restates the top-down split of drivers/upward.cpp:223-277 without recursion.  A cell at
+// level l with key prefix P exists iff its parent is split; it is split ("inner") iff it holds
+// more than L sources and l < LMAX (upward.cpp:245).  Both facts can be read off the sorted
+// keys at O(1) cost per source:
+//   * source i starts the level-l run of its prefix iff keys[i-1] and keys[i] differ at level l;
+//   * that run holds more than L sources iff keys[i+L] has the same level-l prefix.
+// So each source yields a bit mask of the levels at which it starts an inner cell.  The cells
+// are numbered breadth first (level by level, Morton order inside a level, children c = 0..3
+// contiguous), the same canonical order in which the tests walk the reference's tree; the
+// reference's own numbering depends on OpenMP task timing.  Child ranges come from exact
+// binary searches for the child key boundaries, the bounds lower_bound_vec/upper_bound_vec
+// (kernels/upward-common.ispc:59-124) compute.
+//
+// Node arrays (HBM, one entry per node, breadth-first order):
+//   TNode tnode    {xcom, ycom, r, child, count}  32 B   (traversal record)
+//   int2  range    {s, e}                           8 B
+//   int4  cell     {level, cx, cy, parent}         16 B
+#include "tc_internal.h"
+
+namespace tc {
+
+// Largest level at which the prefixes of two keys agree (0..LMAX).
+__device__ __forceinline__ int common_level(int a, int b) {
+    const unsigned x = (unsigned)(a ^ b);
+    if (!x) return LMAX;
+    const int hb = 31 - __clz(x);
+    return LMAX - 1 - hb / 2;
+}
+
+__device__ __forceinline__ int lower_bound_dev(const int *__restrict__ keys, int lo, int hi,
+                                               int val) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < val) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_tree_mask(const int *__restrict__ keys, int n, int leafcap,
+                            unsigned short *__restrict__ mask, int *__restrict__ flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int k = keys[i];
+        const int cprev = i == 0 ? -1 : common_level(keys[i - 1], k);
+        const int cnext = i + leafcap < n ? common_level(k, keys[i + leafcap]) : -1;
+        const int hi = min(cnext, LMAX - 1);
+        unsigned m = 0;
+        for (int l = cprev + 1; l <= hi; ++l) m |= 1u << l;
+        mask[i] = (unsigned short)m;
+        flag[i] = m != 0;
+    }
+}
+
+__global__ void k_tree_compact(const unsigned short *__restrict__ mask,
+                               const int *__restrict__ off, int n, int cap,
+                               int *__restrict__ lpos, unsigned short *__restrict__ lmask,
+                               unsigned *err) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned m = mask[i];
+        if (m) {
+            const int j = off[i];
+            if (j >= cap) {
+                atomicOr(err, DEVERR_TREE);
+                continue;
+            }
+            lpos[j] = i;
+            lmask[j] = (unsigned short)m;
+        }
+    }
+}
+
+constexpr int RANK_THREADS = 1024;
+
+// Per block of 1024 list entries: how many have bit l, for every level l.
+__global__ __launch_bounds__(RANK_THREADS) void k_rank_count(const unsigned short *__restrict__ lmask,
+                                                             int nlist, int *__restrict__ blk,
+                                                             int nblk) {
+    __shared__ int s_cnt[LMAX];
+    if (threadIdx.x < LMAX) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int j = blockIdx.x * RANK_THREADS + threadIdx.x;
+    const unsigned m = j < nlist ? lmask[j] : 0u;
+    for (int l = 0; l < LMAX; ++l) {
+        const unsigned b = __ballot_sync(FULL_MASK, (m >> l) & 1u);
+        if (lane_id() == 0 && b) atomicAdd(&s_cnt[l], __popc(b));
+    }
+    __syncthreads();
+    if (threadIdx.x < LMAX) blk[threadIdx.x * nblk + blockIdx.x] = s_cnt[threadIdx.x];
+}
+
+// One CTA per level: exclusive scan over the blocks' counts; level total -> totals[l].
+__global__ __launch_bounds__(1024) void k_rank_scan(int *__restrict__ blk, int nblk,
+                                                    int *__restrict__ totals) {
+    __shared__ int s_part[1024];
+    const int l = blockIdx.x;
+    int *row = blk + (size_t)l * nblk;
+    const int per = (nblk + 1023) / 1024;
+    const int b0 = threadIdx.x * per;
+    int s = 0;
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < nblk) s += row[b0 + i];
+    s_part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int t = 0; t < 1024; ++t) {
+            const int v = s_part[t];
+            s_part[t] = run;
+            run += v;
+        }
+        totals[l] = run;
+    }
+    __syncthreads();
+    int run = s_part[threadIdx.x];
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < nblk) {
+            const int v = row[b0 + i];
+            row[b0 + i] = run;
+            run += v;
+        }
+}
+
+// rank[l * nlist + j] = number of list entries before j that have bit l.
+__global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned short *__restrict__ lmask,
+                                                             int nlist,
+                                                             const int *__restrict__ blk, int nblk,
+                                                             int *__restrict__ rank) {
+    __shared__ int s_w[LMAX][RANK_THREADS / 32];
+    const int j = blockIdx.x * RANK_THREADS + threadIdx.x;
+    const int w = threadIdx.x >> 5;
+    const unsigned m = j < nlist ? lmask[j] : 0u;
+    unsigned bal[LMAX];
+#pragma unroll
+    for (int l = 0; l < LMAX; ++l) {
+        bal[l] = __ballot_sync(FULL_MASK, (m >> l) & 1u);
+        if (lane_id() == 0) s_w[l][w] = __popc(bal[l]);
+    }
+    __syncthreads();
+    if (threadIdx.x < LMAX) {
+        int run = 0;
+        for (int t = 0; t < RANK_THREADS / 32; ++t) {
+            const int v = s_w[threadIdx.x][t];
+            s_w[threadIdx.x][t] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    if (j < nlist) {
+        const unsigned lt = lanemask_lt();
+#pragma unroll
+        for (int l = 0; l < LMAX; ++l)
+            if ((m >> l) & 1u)
+                rank[(size_t)l * nlist + j] =
+                    blk[(size_t)l * nblk + blockIdx.x] + s_w[l][w] + __popc(bal[l] & lt);
+    }
+}
+
+struct LevelOffsets {
+    int off[LMAX + 2];
+};
+
+__global__ void k_tree_root(int n, int leafcap, TNode *tnode, int2 *range, int4 *cell) {
+    range[0] = make_int2(0, n);
+    cell[0] = make_int4(0, 0, 0, -1);
+    tnode[0].count = n;
+    if (n <= leafcap) tnode[0].child = -1;
+}
+
+__global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap,
+                                const int *__restrict__ lpos,
+                                const unsigned short *__restrict__ lmask, int nlist,
+                                const int *__restrict__ rank, LevelOffsets lo, int nnodes,
+                                TNode *__restrict__ tnode, int2 *__restrict__ range,
+                                int4 *__restrict__ cell, unsigned *err) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nlist; j += gridDim.x * blockDim.x) {
+        const int s = lpos[j];
+        unsigned m = lmask[j];
+        const int key = keys[s];
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int shift = 2 * (LMAX - l);
+            const int P = l == 0 ? 0 : (key >> shift);
+            const int e = l == 0 ? n : lower_bound_dev(keys, s, n, (P + 1) << shift);
+            int id = 0;
+            if (l > 0) {
+                // the parent run starts at the first key with the level-(l-1) prefix P >> 2
+                const int pshift = shift + 2;
+                const int sp = lower_bound_dev(keys, 0, s + 1, (P >> 2) << pshift);
+                const int jp = lower_bound_dev(lpos, 0, nlist, sp);
+                if (jp >= nlist || lpos[jp] != sp || !((lmask[jp] >> (l - 1)) & 1u)) {
+                    atomicOr(err, DEVERR_TREE);
+                    continue;
+                }
+                id = lo.off[l] + 4 * rank[(size_t)(l - 1) * nlist + jp] + (P & 3);
+            }
+            const int base = lo.off[l + 1] + 4 * rank[(size_t)l * nlist + j];
+            if (id < 0 || id >= nnodes || base < 0 || base + 4 > nnodes) {
+                atomicOr(err, DEVERR_BOUNDS);
+                continue;
+            }
+            tnode[id].child = base;
+            const int cshift = shift - 2;
+            int b[5];
+            b[0] = s;
+            b[4] = e;
+            for (int c = 1; c < 4; ++c) b[c] = lower_bound_dev(keys, b[c - 1], e, ((P << 2) | c) << cshift);
+            const int cx = compact_bits(P), cy = compact_bits(P >> 1);
+            for (int c = 0; c < 4; ++c) {
+                const int cid = base + c;
+                const int cnt = b[c + 1] - b[c];
+                range[cid] = make_int2(b[c], b[c + 1]);
+                cell[cid] = make_int4(l + 1, 2 * cx + (c & 1), 2 * cy + (c >> 1), id);
+                tnode[cid].count = cnt;
+                const bool inner = cnt > leafcap && l + 1 < LMAX;
+                if (!inner) tnode[cid].child = -1;
+            }
+        }
+    }
+}
+
+static int grid_for_tree(int n, int threads) {
+    long long g = ((long long)n + threads - 1) / threads;
+    if (g > 148 * 8) g = 148 * 8;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+int build_topology(Context &c, int leafcap) {
+    const int n = c.nsrc;
+    int rc;
+    const int *keys = slot_ptr<int>(c, S_KEYS);
+    unsigned short *mask;
+    int *flag, *off;
+    if ((rc = ensure(c, S_TMASK, n, &mask)) || (rc = ensure(c, S_TFLAG, n, &flag)) ||
+        (rc = ensure(c, S_TOFF, (size_t)n + 1, &off)))
+        return rc;
+    k_tree_mask<<<grid_for_tree(n, 256), 256, 0, c.stream>>>(keys, n, leafcap, mask, flag);
+    TC_KERNEL_CHECK();
+    if ((rc = exclusive_scan(c, flag, off, n))) return rc;
+    // The list length is needed to size the rank pass: read it back with the level totals.
+    // Upper bound first (every inner cell has > leafcap sources in one level): n/(L+1) per level.
+    const long long bound = (long long)LMAX * (n / (leafcap + 1) + 1);
+    const int cap = (int)(bound < n ? bound : n);
+    int *lpos, *rank, *blkc, *totals;
+    unsigned short *lmask;
+    if ((rc = ensure(c, S_LPOS, (size_t)cap + 1, &lpos)) ||
+        (rc = ensure(c, S_LMASK, (size_t)cap + 1, &lmask)))
+        return rc;
+    k_tree_compact<<<grid_for_tree(n, 256), 256, 0, c.stream>>>(mask, off, n, cap, lpos, lmask,
+                                                                slot_ptr<unsigned>(c, S_ERR));
+    TC_KERNEL_CHECK();
+    // read back the list length
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, off + n, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    const int nlist = (int)c.h_pinned[0];
+    if (nlist > cap) {
+        set_error(TC_ERR_INVALID, "tree list length %d exceeds its bound %d", nlist, cap);
+        return TC_ERR_INVALID;
+    }
+    const int nblk = (nlist + RANK_THREADS - 1) / RANK_THREADS;
+    if ((rc = ensure(c, S_LRANK, (size_t)LMAX * (nlist + 1), &rank)) ||
+        (rc = ensure(c, S_LBLK, (size_t)LMAX * (nblk + 1), &blkc)) ||
+        (rc = ensure(c, S_LEVEL_TOTALS, LMAX + 1, &totals)))
+        return rc;
+    TC_CUDA_TRY(cudaMemsetAsync(totals, 0, sizeof(int) * (LMAX + 1), c.stream));
+    if (nlist > 0) {
+        k_rank_count<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, nlist, blkc, nblk);
+        TC_KERNEL_CHECK();
+        k_rank_scan<<<LMAX, 1024, 0, c.stream>>>(blkc, nblk, totals);
+        TC_KERNEL_CHECK();
+        k_rank_apply<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, nlist, blkc, nblk, rank);
+        TC_KERNEL_CHECK();
+    }
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, totals, sizeof(int) * LMAX, cudaMemcpyDeviceToHost,
+                                c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    LevelOffsets lo;
+    lo.off[0] = 0;
+    lo.off[1] = 1;
+    long long ninner = 0;
+    int nlevels = 1;
+    for (int l = 0; l < LMAX; ++l) {
+        const int inner = (int)c.h_pinned[l];
+        ninner += inner;
+        lo.off[l + 2] = lo.off[l + 1] + 4 * inner;
+        if (inner) nlevels = l + 2;
+    }
+    const long long nnodes = 1 + 4 * ninner;
+    if (nnodes >= (1LL << 31)) {
+        set_error(TC_ERR_INVALID, "too many tree nodes (%lld)", nnodes);
+        return TC_ERR_INVALID;
+    }
+    c.nnodes = (int)nnodes;
+    c.ninner = (int)ninner;
+    c.leafcap = leafcap;
+    for (int l = 0; l < LMAX + 2; ++l) c.level_off[l] = lo.off[l];
+    c.counts.nnodes = nnodes;
+    c.counts.ninner = ninner;
+    c.counts.nleaves = nnodes - ninner;
+    c.counts.nlevels = nlevels;
+
+    TNode *tnode;
+    int2 *range;
+    int4 *cell;
+    if ((rc = ensure(c, S_TNODE, nnodes, &tnode)) || (rc = ensure(c, S_RANGE, nnodes, &range)) ||
+        (rc = ensure(c, S_CELL, nnodes, &cell)))
+        return rc;
+    k_tree_root<<<1, 1, 0, c.stream>>>(n, leafcap, tnode, range, cell);
+    TC_KERNEL_CHECK();
+    if (nlist > 0) {
+        k_tree_children<<<grid_for_tree(nlist, 128), 128, 0, c.stream>>>(
+            keys, n, leafcap, lpos, lmask, nlist, rank, lo, c.nnodes, tnode, range, cell,
+            slot_ptr<unsigned>(c, S_ERR));
+        TC_KERNEL_CHECK();
+    }
+    return TC_OK;
+}
+
+}  // namespace tc

@@ -1,0 +1,259 @@
+"""Python host binding of the B200 treecode library (ctypes over the C ABI).
+
+Mirrors the reference's public interface (drivers/treecode-potential.h:21-29,
+drivers/treecode-force.h:21-31): ``treecode_potential`` and ``treecode_force_mrag`` take the
+same arguments with the same meaning (theta opening criterion, source coordinates and values,
+targets / MRAG blocks) and return what the reference writes into its output arrays.  The
+``Context`` class exposes the extended device-pointer API (inputs resident in GPU memory,
+e.g. torch CUDA tensors), statistics, tree inspection and GPU direct sums.
+
+There is no CPU fallback: if the shared library is missing or no GPU is visible, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "lib2d-treecodes-b200.so")
+
+ORDER = {"potential": 12, "force": 24}
+LEAF = {"potential": 512, "force": 192}
+BLOCKSIZE = 32
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+# Every symbol the header include/treecodes_b200.h declares, with its ctypes signature.
+SIGNATURES = {
+    "treecode_potential": (None, [_d, _dp, _dp, _dp, _i, _dp, _dp, _i, _dp]),
+    "treecode_force_mrag": (None, [_d, _dp, _dp, _dp, _i, _dp, _dp, _dp, _i, _dp, _dp]),
+    "treecode_last_status": (_i, []),
+    "treecode_last_error": (ctypes.c_char_p, []),
+    "tc_context_create": (_i, [ctypes.POINTER(_vp), _i, _vp]),
+    "tc_context_destroy": (None, [_vp]),
+    "tc_set_precision": (_i, [_vp, _i]),
+    "tc_set_timing": (_i, [_vp, _i]),
+    "tc_get_stats": (_i, [_vp, _vp]),
+    "tc_get_stream": (_vp, [_vp]),
+    "tc_potential_host": (_i, [_vp, _d, _dp, _dp, _dp, _i, _dp, _dp, _i, _dp]),
+    "tc_force_mrag_host": (_i, [_vp, _d, _dp, _dp, _dp, _i, _dp, _dp, _dp, _i, _dp, _dp]),
+    "tc_potential_device": (_i, [_vp, _d, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp]),
+    "tc_force_mrag_device": (_i, [_vp, _d, _vp, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp, _vp]),
+    "tc_tree_build_device": (_i, [_vp, _i, _vp, _vp, _vp, _i]),
+    "tc_tree_size": (_i, [_vp, _ip, _ip, _ip]),
+    "tc_tree_copy": (_i, [_vp] + [_vp] * 19),
+    "tc_direct_potential_device": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp]),
+    "tc_direct_force_device": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "tc_measure_fma_peak": (_i, [_i, _dp]),
+    "tc_version": (ctypes.c_char_p, []),
+}
+
+
+class TreecodeError(RuntimeError):
+    pass
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("sort_ms", ctypes.c_float), ("tree_ms", ctypes.c_float),
+                ("upward_ms", ctypes.c_float), ("lists_ms", ctypes.c_float),
+                ("eval_ms", ctypes.c_float), ("total_ms", ctypes.c_float),
+                ("nnodes", ctypes.c_longlong), ("nleaves", ctypes.c_longlong),
+                ("ninner", ctypes.c_longlong), ("nlevels", ctypes.c_longlong),
+                ("n_e2l", ctypes.c_longlong), ("n_e2p", ctypes.c_longlong),
+                ("n_p2p", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise TreecodeError(f"{path} is missing: build it with `make -C 2d-treecodes_b200`")
+        L = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def last_status():
+    return load().treecode_last_status()
+
+
+def last_error():
+    return load().treecode_last_error().decode()
+
+
+def _check(rc):
+    if rc != 0:
+        raise TreecodeError(f"status {rc}: {last_error()}")
+
+
+# ----------------------------------------------------------------- reference-compatible API
+def treecode_potential(theta, xsources, ysources, sourcevalues, xtargets, ytargets):
+    """drivers/treecode-potential.cpp:93-106: potential at every target (host arrays)."""
+    xs, ys, vs, xt, yt = map(_f64, (xsources, ysources, sourcevalues, xtargets, ytargets))
+    out = np.empty(len(xt))
+    load().treecode_potential(float(theta), _p(xs), _p(ys), _p(vs), len(xs), _p(xt), _p(yt),
+                              len(xt), _p(out))
+    _check(last_status())
+    return out
+
+
+def treecode_force_mrag(theta, xsources, ysources, sourcevalues, x0s, y0s, hs):
+    """drivers/treecode-force.cpp:203-236: (xresults, yresults), each 1024 * nblocks long,
+    target (ix, iy) of block ib at ix + 32 * (iy + 32 * ib)."""
+    xs, ys, vs, x0, y0, h = map(_f64, (xsources, ysources, sourcevalues, x0s, y0s, hs))
+    nb = len(x0)
+    xo = np.empty(nb * BLOCKSIZE * BLOCKSIZE)
+    yo = np.empty(nb * BLOCKSIZE * BLOCKSIZE)
+    load().treecode_force_mrag(float(theta), _p(xs), _p(ys), _p(vs), len(xs), _p(x0), _p(y0),
+                               _p(h), nb, _p(xo), _p(yo))
+    _check(last_status())
+    return xo, yo
+
+
+def measure_fma_peak(fp64=True):
+    t = ctypes.c_double()
+    _check(load().tc_measure_fma_peak(1 if fp64 else 0, ctypes.byref(t)))
+    return t.value
+
+
+def _ptr(t):
+    """Device address of a torch CUDA tensor (or an int address)."""
+    if isinstance(t, int):
+        return t
+    if not t.is_contiguous():
+        raise TreecodeError("device arrays must be contiguous")
+    return t.data_ptr()
+
+
+class Context:
+    """A solver context: a CUDA stream plus device buffers reused across calls."""
+
+    def __init__(self, device=-1, stream=None, precision=0, timing=False):
+        self.lib = load()
+        h = _vp()
+        _check(self.lib.tc_context_create(ctypes.byref(h), int(device), stream))
+        self.h = h
+        if precision:
+            _check(self.lib.tc_set_precision(self.h, int(precision)))
+        if timing:
+            self.lib.tc_set_timing(self.h, 1)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tc_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return self.lib.tc_get_stream(self.h)
+
+    def set_precision(self, mode):
+        _check(self.lib.tc_set_precision(self.h, int(mode)))
+
+    def set_timing(self, on=True):
+        self.lib.tc_set_timing(self.h, 1 if on else 0)
+
+    def stats(self):
+        s = Stats()
+        _check(self.lib.tc_get_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    # ---- host pointers
+    def potential_host(self, theta, xs, ys, vs, xt, yt, out=None):
+        xs, ys, vs, xt, yt = map(_f64, (xs, ys, vs, xt, yt))
+        out = np.empty(len(xt)) if out is None else out
+        _check(self.lib.tc_potential_host(self.h, float(theta), _p(xs), _p(ys), _p(vs), len(xs),
+                                          _p(xt), _p(yt), len(xt), _p(out)))
+        return out
+
+    def force_mrag_host(self, theta, xs, ys, vs, x0s, y0s, hs, xo=None, yo=None):
+        xs, ys, vs, x0, y0, h = map(_f64, (xs, ys, vs, x0s, y0s, hs))
+        nt = len(x0) * BLOCKSIZE * BLOCKSIZE
+        xo = np.empty(nt) if xo is None else xo
+        yo = np.empty(nt) if yo is None else yo
+        _check(self.lib.tc_force_mrag_host(self.h, float(theta), _p(xs), _p(ys), _p(vs), len(xs),
+                                           _p(x0), _p(y0), _p(h), len(x0), _p(xo), _p(yo)))
+        return xo, yo
+
+    # ---- device pointers (torch CUDA tensors of dtype float64)
+    def potential_device(self, theta, xs, ys, vs, xt, yt, out):
+        _check(self.lib.tc_potential_device(self.h, float(theta), _ptr(xs), _ptr(ys), _ptr(vs),
+                                            int(xs.numel()), _ptr(xt), _ptr(yt), int(xt.numel()),
+                                            _ptr(out)))
+        return out
+
+    def force_mrag_device(self, theta, xs, ys, vs, x0s, y0s, hs, xo, yo):
+        _check(self.lib.tc_force_mrag_device(self.h, float(theta), _ptr(xs), _ptr(ys), _ptr(vs),
+                                             int(xs.numel()), _ptr(x0s), _ptr(y0s), _ptr(hs),
+                                             int(x0s.numel()), _ptr(xo), _ptr(yo)))
+        return xo, yo
+
+    def direct_potential_device(self, xs, ys, vs, xt, yt, out):
+        _check(self.lib.tc_direct_potential_device(self.h, _ptr(xs), _ptr(ys), _ptr(vs),
+                                                   int(xs.numel()), _ptr(xt), _ptr(yt),
+                                                   int(xt.numel()), _ptr(out)))
+        return out
+
+    def direct_force_device(self, xs, ys, vs, xt, yt, xo, yo):
+        _check(self.lib.tc_direct_force_device(self.h, _ptr(xs), _ptr(ys), _ptr(vs),
+                                               int(xs.numel()), _ptr(xt), _ptr(yt),
+                                               int(xt.numel()), _ptr(xo), _ptr(yo)))
+        return xo, yo
+
+    # ---- tree inspection
+    def tree(self, kind, xs, ys, vs):
+        """Build the tree of `kind` ('potential' | 'force') and copy it to the host."""
+        k = 0 if kind == "potential" else 1
+        _check(self.lib.tc_tree_build_device(self.h, k, _ptr(xs), _ptr(ys), _ptr(vs),
+                                             int(xs.numel())))
+        nn, order, n = _i(), _i(), _i()
+        _check(self.lib.tc_tree_size(self.h, ctypes.byref(nn), ctypes.byref(order),
+                                     ctypes.byref(n)))
+        nn, order, n = nn.value, order.value, n.value
+        out = dict(keys=np.empty(n, np.int32), perm=np.empty(n, np.int32), xs=np.empty(n),
+                   ys=np.empty(n), vs=np.empty(n), frame=np.empty(3))
+        for name in ("s", "e", "child", "count", "level", "cx", "cy", "parent"):
+            out[name] = np.empty(nn, np.int32)
+        for name in ("mass", "xcom", "ycom", "r"):
+            out[name] = np.empty(nn)
+        out["exps"] = np.empty(nn * 2 * order)
+        order_names = ("keys", "perm", "xs", "ys", "vs", "frame", "s", "e", "child", "count",
+                       "level", "cx", "cy", "parent", "mass", "xcom", "ycom", "r", "exps")
+        args = [out[k].ctypes.data_as(_vp) for k in order_names]
+        _check(self.lib.tc_tree_copy(self.h, *args))
+        out["exps"] = out["exps"].reshape(nn, 2, order)
+        out["inner"] = out["child"] >= 0
+        out["n"] = nn
+        out["order"] = order
+        return out

@@ -1,0 +1,153 @@
+/*
+ * treecodes_b200.h -- C ABI of the B200 (sm_100a) 2-D treecode library
+ * (lib2d-treecodes-b200.so).
+ *
+ * The first two functions are drop-in replacements for the reference's public entry points,
+ * with identical prototypes (realtype = double) and semantics:
+ *   treecode_potential   replaces drivers/treecode-potential.h:21-29
+ *                        (definition drivers/treecode-potential.cpp:91-106)
+ *   treecode_force_mrag  replaces drivers/treecode-force.h:21-31
+ *                        (definition drivers/treecode-force.cpp:201-236)
+ * Both take host pointers, copy them to the GPU, solve there and copy the results back.
+ * Expansion orders (12 potential, 24 force), leaf capacities (512, 192), the MRAG block size
+ * (32 x 32) and LMAX = 15 are those of the reference build (Makefile:13-15).
+ * The force output of block ib, target (ix, iy), is at ix + 32 * (iy + 32 * ib).
+ *
+ * Differences from the reference, all additive: the functions are reentrant (state lives in
+ * a per-thread context), print nothing, and report failures through treecode_last_status() /
+ * treecode_last_error() instead of undefined behaviour.  nsources == 0 yields zero outputs.
+ *
+ * The tc_* functions are an extended API (no counterpart in the reference): explicit contexts
+ * on a CUDA stream, device-pointer entry points, statistics, tree inspection for tests, GPU
+ * direct sums for accuracy checks.  They return a tc_status code.
+ */
+#ifndef TREECODES_B200_H
+#define TREECODES_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TC_API __attribute__((visibility("default")))
+
+/* ---- reference-compatible entry points ---------------------------------------------- */
+
+/* drivers/treecode-potential.h:21-29 */
+TC_API void treecode_potential(const double theta,
+                               const double * const xsources,
+                               const double * const ysources,
+                               const double * const sourcevalues,
+                               const int nsources,
+                               const double * const xtargets,
+                               const double * const ytargets,
+                               const int ntargets,
+                               double * const targetvalues);
+
+/* drivers/treecode-force.h:21-31 */
+TC_API void treecode_force_mrag(const double theta,
+                                const double * const xsources,
+                                const double * const ysources,
+                                const double * const sourcevalues,
+                                const int nsources,
+                                const double * const x0s,
+                                const double * const y0s,
+                                const double * const hs,
+                                const int nblocks,
+                                double * const xresults,
+                                double * const yresults);
+
+/* ---- status ----------------------------------------------------------------------- */
+
+typedef enum {
+    TC_OK = 0,
+    TC_ERR_INVALID = 1,    /* bad argument (negative size, NULL pointer, unsupported mode) */
+    TC_ERR_CUDA = 2,       /* a CUDA call failed */
+    TC_ERR_CAPACITY = 3,   /* a device-side capacity (traversal stack) was exceeded */
+    TC_ERR_TIMEOUT = 4,    /* a bounded device-side wait gave up */
+    TC_ERR_NO_DEVICE = 5,  /* no CUDA device is visible */
+    TC_ERR_ALLOC = 6       /* device memory could not be allocated */
+} tc_status;
+
+/* Status and message of the last call made by this thread (any entry point). */
+TC_API int treecode_last_status(void);
+TC_API const char *treecode_last_error(void);
+
+/* ---- extended API ------------------------------------------------------------------ */
+
+typedef struct tc_context tc_context;
+
+typedef enum { TC_PRECISION_FP64 = 0, TC_PRECISION_MIXED = 1 } tc_precision;
+
+typedef struct {
+    /* phase times in ms (filled when timing is enabled) */
+    float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms;
+    /* sizes of the last solve */
+    long long nnodes, nleaves, ninner, nlevels;
+    long long n_e2l, n_e2p, n_p2p;   /* interaction-list entries */
+} tc_stats;
+
+/* device < 0 selects the current device; stream may be NULL (the context creates one). */
+TC_API int tc_context_create(tc_context **ctx, int device, void *cuda_stream);
+TC_API void tc_context_destroy(tc_context *ctx);
+TC_API int tc_set_precision(tc_context *ctx, int precision);
+TC_API int tc_set_timing(tc_context *ctx, int enabled);
+TC_API int tc_get_stats(tc_context *ctx, tc_stats *out);
+TC_API void *tc_get_stream(tc_context *ctx);
+
+/* Same as the reference entry points, host pointers, explicit context and status. */
+TC_API int tc_potential_host(tc_context *ctx, double theta, const double *xsources,
+                             const double *ysources, const double *sourcevalues, int nsources,
+                             const double *xtargets, const double *ytargets, int ntargets,
+                             double *targetvalues);
+TC_API int tc_force_mrag_host(tc_context *ctx, double theta, const double *xsources,
+                              const double *ysources, const double *sourcevalues, int nsources,
+                              const double *x0s, const double *y0s, const double *hs,
+                              int nblocks, double *xresults, double *yresults);
+
+/* Device pointers (all arrays resident in GPU memory); work is ordered on the context's
+ * stream and complete when the call returns. */
+TC_API int tc_potential_device(tc_context *ctx, double theta, const double *xsources,
+                               const double *ysources, const double *sourcevalues, int nsources,
+                               const double *xtargets, const double *ytargets, int ntargets,
+                               double *targetvalues);
+TC_API int tc_force_mrag_device(tc_context *ctx, double theta, const double *xsources,
+                                const double *ysources, const double *sourcevalues,
+                                int nsources, const double *x0s, const double *y0s,
+                                const double *hs, int nblocks, double *xresults,
+                                double *yresults);
+
+/* Tree inspection (tests).  kind: 0 = potential tree (order 12, leaf 512),
+ * 1 = force tree (order 24, leaf 192).  Sources are device pointers. */
+TC_API int tc_tree_build_device(tc_context *ctx, int kind, const double *xsources,
+                                const double *ysources, const double *sourcevalues,
+                                int nsources);
+TC_API int tc_tree_size(tc_context *ctx, int *nnodes, int *order, int *nsources);
+/* Host arrays: keys/perm/xs/ys/vs (nsources each), frame (xmin, ymin, ext), per node
+ * s, e, child (-1 = leaf), count, level, cx, cy, parent, mass, xcom, ycom, r,
+ * exps (nnodes * 2 * order: real parts then imaginary parts).  Any pointer may be NULL. */
+TC_API int tc_tree_copy(tc_context *ctx, int *keys, int *perm, double *xs, double *ys,
+                        double *vs, double *frame, int *s, int *e, int *child, int *count,
+                        int *level, int *cx, int *cy, int *parent, double *mass, double *xcom,
+                        double *ycom, double *r, double *exps);
+
+/* FP64 direct sums (main.cpp:201-245 of the reference) on device pointers. */
+TC_API int tc_direct_potential_device(tc_context *ctx, const double *xsources,
+                                      const double *ysources, const double *sourcevalues,
+                                      int nsources, const double *xtargets,
+                                      const double *ytargets, int ntargets, double *out);
+TC_API int tc_direct_force_device(tc_context *ctx, const double *xsources,
+                                  const double *ysources, const double *sourcevalues,
+                                  int nsources, const double *xtargets, const double *ytargets,
+                                  int ntargets, double *xout, double *yout);
+
+/* Measured FMA throughput of the current device in TFLOP/s (fp64 != 0: FP64, else FP32). */
+TC_API int tc_measure_fma_peak(int fp64, double *tflops);
+
+/* Library version string. */
+TC_API const char *tc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TREECODES_B200_H */
