@@ -22,6 +22,7 @@ int measure_fma_peak(int fp64, double *tflops);
 
 static thread_local int tls_status = TC_OK;
 static thread_local char tls_msg[512] = "";
+thread_local long long g_launches = 0;
 
 void set_error(int status, const char *fmt, ...) {
     tls_status = status;
@@ -40,11 +41,17 @@ void phase_mark(Context &c, int idx) {
     if (c.timing) cudaEventRecord(c.ev[idx], c.stream);
 }
 
+// Reads back the device error word and the work counters (one sync).  The counters land in
+// h_pinned[16 ...] as unsigned long long.
 int check_device_errors(Context &c, const char *where) {
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 8, err, sizeof(unsigned), cudaMemcpyDeviceToHost,
                                 c.stream));
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 16, c.buf[S_STATS].p,
+                                sizeof(unsigned long long) * STAT_SLOTS, cudaMemcpyDeviceToHost,
+                                c.stream));
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    c.counts.launches = g_launches;
     const unsigned e = c.h_pinned[8];
     if (e & DEVERR_SPIN_LIMIT) {
         set_error(TC_ERR_TIMEOUT, "%s: a bounded device wait gave up (flags 0x%x)", where, e);
@@ -55,10 +62,15 @@ int check_device_errors(Context &c, const char *where) {
         return TC_ERR_CAPACITY;
     }
     if (e) {
-        set_error(TC_ERR_CUDA, "%s: inconsistent tree bookkeeping (flags 0x%x)", where, e);
+        set_error(TC_ERR_CUDA, "%s: inconsistent tree bookkeeping or index out of bounds (flags 0x%x)",
+                  where, e);
         return TC_ERR_CUDA;
     }
     return TC_OK;
+}
+
+static unsigned long long stat_counter(Context &c, int slot) {
+    return reinterpret_cast<unsigned long long *>(c.h_pinned + 16)[slot];
 }
 
 static int context_init(Context &c, int device, cudaStream_t stream) {
@@ -82,9 +94,12 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     TC_CUDA_TRY(cudaMallocHost(&c.h_pinned, 4096));
     for (auto &ev : c.ev) TC_CUDA_TRY(cudaEventCreate(&ev));
     unsigned *err;
+    unsigned long long *stats;
     int rc;
     if ((rc = ensure(c, S_ERR, 64, &err))) return rc;
+    if ((rc = ensure(c, S_STATS, STAT_SLOTS, &stats))) return rc;
     TC_CUDA_TRY(cudaMemsetAsync(err, 0, 64 * sizeof(unsigned), c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(stats, 0, STAT_SLOTS * sizeof(unsigned long long), c.stream));
     return TC_OK;
 }
 
@@ -118,7 +133,10 @@ static void finish_timing(Context &c) {
 static int build_tree(Context &c, int kind, const double *x, const double *y, const double *v,
                       int n) {
     int rc;
+    g_launches = 0;
     TC_CUDA_TRY(cudaMemsetAsync(slot_ptr<unsigned>(c, S_ERR), 0, sizeof(unsigned), c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(c.buf[S_STATS].p, 0, STAT_SLOTS * sizeof(unsigned long long),
+                                c.stream));
     if ((rc = sort_sources(c, x, y, v, n))) return rc;
     phase_mark(c, 1);
     if ((rc = build_topology(c, kind ? LEAF_FORCE : LEAF_POTENTIAL))) return rc;
@@ -151,6 +169,8 @@ static int potential_device(Context &c, double theta, const double *xs, const do
     if ((rc = potential(c, theta, xt, yt, m, out))) return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_potential"))) return rc;
+    c.counts.e2p_pairs = (long long)stat_counter(c, STAT_E2P_PAIRS);
+    c.counts.p2p_pairs = (long long)stat_counter(c, STAT_P2P_PAIRS);
     finish_timing(c);
     return TC_OK;
 }
@@ -184,6 +204,7 @@ static int force_device(Context &c, double theta, const double *xs, const double
     if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo))) return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_force_mrag"))) return rc;
+    c.counts.p2p_pairs = (long long)stat_counter(c, STAT_P2P_SOURCES) * TILE * TILE;
     finish_timing(c);
     return TC_OK;
 }
@@ -366,6 +387,11 @@ TC_API int tc_get_stats(tc_context *ctx, tc_stats *out) {
     out->n_e2l = c.counts.n_e2l;
     out->n_e2p = c.counts.n_e2p;
     out->n_p2p = c.counts.n_p2p;
+    out->p2p_pairs = c.counts.p2p_pairs;
+    out->e2p_pairs = c.counts.e2p_pairs;
+    out->e2l_pairs = c.counts.e2l_pairs;
+    out->l2p_targets = c.counts.l2p_targets;
+    out->launches = c.counts.launches;
     return TC_OK;
 }
 

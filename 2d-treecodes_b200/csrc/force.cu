@@ -73,12 +73,13 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
     int nbricks, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int *__restrict__ lists,
-    unsigned *err) {
+    unsigned *err, unsigned long long *stats) {
     __shared__ int stack_all[TR_WARPS][TR_STACK];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     int *stack = stack_all[warp];
     const double inv_theta = 1.0 / theta, theta2 = theta * theta;
     const unsigned lt = lanemask_lt();
+    unsigned long long p2p_sources = 0;   // per lane: sources of the P2P leaves it listed
 
     for (int brick = blockIdx.x * TR_WARPS + warp; brick < nbricks;
          brick += gridDim.x * TR_WARPS) {
@@ -106,6 +107,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                     const TNode nd = tnode[node];
                     kind = classify(nd, b, inv_theta, theta2);
                     child = nd.child;
+                    if (FILL && kind == K_P2P) p2p_sources += (unsigned)nd.count;
                     if (kind == K_DESCEND && (child <= node || child + 4 > nnodes)) {
                         atomicOr(err, DEVERR_BOUNDS);
                         kind = K_SKIP;
@@ -145,6 +147,10 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
             counts[2 * nbricks + brick] = n[2];
         }
         __syncwarp();
+    }
+    if (FILL) {
+        for (int m = 16; m; m >>= 1) p2p_sources += __shfl_xor_sync(FULL_MASK, p2p_sources, m);
+        if (lane == 0 && p2p_sources) atomicAdd(&stats[STAT_P2P_SOURCES], p2p_sources);
     }
 }
 
@@ -368,7 +374,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                                 (long long)sm_count() * 16);
     k_force_lists<false><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(nbricks, x0s, y0s, hs, theta,
                                                                  tnode, c.nnodes, counts, nullptr, nullptr,
-                                                                 err);
+                                                                 err, nullptr);
     TC_KERNEL_CHECK();
     if ((rc = exclusive_scan(c, counts, offs, 3 * nbricks))) return rc;
     int tot[4];
@@ -382,10 +388,14 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     c.counts.n_e2l = tot[0];
     c.counts.n_e2p = tot[1] - tot[0];
     c.counts.n_p2p = tot[2] - tot[1];
+    c.counts.e2l_pairs = c.counts.n_e2l;
+    c.counts.e2p_pairs = c.counts.n_e2p * TILE * TILE;
+    c.counts.l2p_targets = (long long)nbricks * TILE * TILE;
     int *lists;
     if ((rc = ensure(c, S_E2L, (size_t)tot[2] + 1, &lists))) return rc;
     k_force_lists<true><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(nbricks, x0s, y0s, hs, theta,
-                                                                tnode, c.nnodes, nullptr, offs, lists, err);
+                                                                tnode, c.nnodes, nullptr, offs, lists, err,
+                                                                slot_ptr<unsigned long long>(c, S_STATS));
     TC_KERNEL_CHECK();
     phase_mark(c, 4);
     const int evgrid = (int)std::min<long long>((nbricks + EV_WARPS - 1) / EV_WARPS,

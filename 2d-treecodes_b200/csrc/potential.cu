@@ -27,11 +27,12 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
     int ngroups, int m, const double *__restrict__ xt, const double *__restrict__ yt,
     const int *__restrict__ tperm, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int2 *__restrict__ lists,
-    unsigned *err) {
+    unsigned *err, unsigned long long *stats) {
     __shared__ int2 stack_all[PT_WARPS][PT_STACK];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     int2 *stack = stack_all[warp];
     const double theta2 = theta * theta;
+    unsigned long long e2p_pairs = 0, p2p_pairs = 0;   // warp-uniform work counters
 
     for (int g = blockIdx.x * PT_WARPS + warp; g < ngroups; g += gridDim.x * PT_WARPS) {
         const int t = g * 32 + lane;
@@ -72,6 +73,7 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             const unsigned far = __ballot_sync(FULL_MASK, accept);
             const unsigned rest = mask & ~far;
             if (far) {
+                e2p_pairs += __popc(far);
                 if (FILL && lane == 0) {
                     if (o0 + n0 < l0) lists[o0 + n0] = make_int2(ent.x, (int)far);
                     else atomicOr(err, DEVERR_BOUNDS);
@@ -81,6 +83,7 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             if (rest) {
                 if (nd.child < 0) {
                     if (nd.count > 0) {
+                        p2p_pairs += (unsigned long long)__popc(rest) * (unsigned)nd.count;
                         if (FILL && lane == 0) {
                             if (o1 + n1 < l1) lists[o1 + n1] = make_int2(ent.x, (int)rest);
                             else atomicOr(err, DEVERR_BOUNDS);
@@ -107,6 +110,10 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             counts[ngroups + g] = n1;
         }
         __syncwarp();
+    }
+    if (FILL && lane == 0) {
+        if (e2p_pairs) atomicAdd(&stats[STAT_E2P_PAIRS], e2p_pairs);
+        if (p2p_pairs) atomicAdd(&stats[STAT_P2P_PAIRS], p2p_pairs);
     }
 }
 
@@ -228,7 +235,7 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
                                               (long long)sm_count_p() * 16);
     k_potential_lists<false><<<grid, PT_WARPS * 32, 0, c.stream>>>(ngroups, m, xt, yt, vo, theta,
                                                                   tnode, c.nnodes, counts, nullptr, nullptr,
-                                                                  err);
+                                                                  err, nullptr);
     TC_KERNEL_CHECK();
     if ((rc = exclusive_scan(c, counts, offs, 2 * ngroups))) return rc;
     TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, offs + ngroups, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
@@ -238,10 +245,13 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     c.counts.n_e2p = n_e2p;
     c.counts.n_p2p = total - n_e2p;
     c.counts.n_e2l = 0;
+    c.counts.e2l_pairs = 0;
+    c.counts.l2p_targets = 0;
     int2 *lists;
     if ((rc = ensure(c, S_PE2P, (size_t)total + 1, &lists))) return rc;
     k_potential_lists<true><<<grid, PT_WARPS * 32, 0, c.stream>>>(ngroups, m, xt, yt, vo, theta,
-                                                                 tnode, c.nnodes, nullptr, offs, lists, err);
+                                                                 tnode, c.nnodes, nullptr, offs, lists, err,
+                                                                 slot_ptr<unsigned long long>(c, S_STATS));
     TC_KERNEL_CHECK();
     phase_mark(c, 4);
     const int egrid = (int)std::min<long long>((ngroups + PE_WARPS - 1) / PE_WARPS,

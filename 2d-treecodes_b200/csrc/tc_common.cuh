@@ -103,9 +103,16 @@ struct __align__(32) TNode {
         }                                                                            \
     } while (0)
 
-#define TC_KERNEL_CHECK()  TC_CUDA_TRY(cudaGetLastError())
+// Every kernel launch site is followed by TC_KERNEL_CHECK(), which also counts the launch.
+#define TC_KERNEL_CHECK()          \
+    do {                           \
+        ++::tc::g_launches;        \
+        TC_CUDA_TRY(cudaGetLastError()); \
+    } while (0)
 
 namespace tc {
+// Kernel launches issued by this thread since the counter was last reset (per solve).
+extern thread_local long long g_launches;
 // Records status and message for treecode_last_status / treecode_last_error (thread-local).
 void set_error(int status, const char *fmt, ...);
 }

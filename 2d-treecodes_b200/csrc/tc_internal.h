@@ -49,7 +49,13 @@ struct Counts {
     long long n_e2l, n_e2p, n_p2p;        // interaction-list entries
     long long p2p_pairs;                  // source-target pairs evaluated directly
     long long e2p_pairs;                  // (target, cell) pairs of far-field evaluation
+    long long e2l_pairs;                  // (brick, cell) pairs of local-expansion builds
+    long long l2p_targets;                // targets evaluated from a local expansion
+    long long launches;                   // kernels launched by the last solve
 };
+
+// Device-side work counters (unsigned long long each) in the S_STATS slot.
+enum { STAT_P2P_SOURCES = 0, STAT_E2P_PAIRS = 1, STAT_P2P_PAIRS = 2, STAT_SLOTS = 8 };
 
 struct Context {
     int device = 0;

@@ -29,11 +29,13 @@ namespace tc {
 __constant__ BinomTable c_binom_up = make_binom_table();
 
 constexpr int UP_WARPS = 4;
+constexpr int UP_CHUNK = 256;   // leaf sources staged in shared memory per pass (multiple of 4)
 
 template <int P>
 struct UpShared {
     double zr[4][P + 1], zi[4][P + 1];   // z0^-k per child
     double cr[4][P + 1], ci[4][P + 1];   // a_{k-1} z0^-k per child
+    double sx[UP_CHUNK], sy[UP_CHUNK], sv[UP_CHUNK];   // staged leaf sources
 };
 
 template <int P>
@@ -115,17 +117,35 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_upward(
     const Frame f = *frame;
     const int s = rg.x, e = rg.y;
 
-    // ---- upward_setup: four strided lane accumulators (upward-common.ispc:24-42)
-    double ms = 0, ws = 0, wxs_l = 0, wys_l = 0;
-    if (lane < 4)
-        for (int i = s + lane; i < e; i += 4) {
-            const double x = xs[i], y = ys[i], m = vs[i];
-            const double w = fabs(m);
-            ms = __dadd_rn(ms, m);
-            ws = __dadd_rn(ws, w);
-            wxs_l = __dadd_rn(wxs_l, __dmul_rn(x, w));
-            wys_l = __dadd_rn(wys_l, __dmul_rn(y, w));
+    // Leaf sources pass through shared memory in chunks of UP_CHUNK (coalesced loads by all
+    // lanes); a leaf that fits one chunk is loaded once for all three passes below.
+    const int nch = (e - s + UP_CHUNK - 1) / UP_CHUNK;
+    auto stage = [&](int c0, int cnt) {
+        __syncwarp();
+        for (int j = lane; j < cnt; j += 32) {
+            sh.sx[j] = xs[c0 + j];
+            sh.sy[j] = ys[c0 + j];
+            sh.sv[j] = vs[c0 + j];
         }
+        __syncwarp();
+    };
+
+    // ---- upward_setup: four strided lane accumulators (upward-common.ispc:24-42); chunks
+    // start at multiples of 4 from s, so element i still goes to lane (i - s) % 4.
+    double ms = 0, ws = 0, wxs_l = 0, wys_l = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int c0 = s + ch * UP_CHUNK, cnt = min(UP_CHUNK, e - c0);
+        stage(c0, cnt);
+        if (lane < 4)
+            for (int j = lane; j < cnt; j += 4) {
+                const double x = sh.sx[j], y = sh.sy[j], m = sh.sv[j];
+                const double w = fabs(m);
+                ms = __dadd_rn(ms, m);
+                ws = __dadd_rn(ws, w);
+                wxs_l = __dadd_rn(wxs_l, __dmul_rn(x, w));
+                wys_l = __dadd_rn(wys_l, __dmul_rn(y, w));
+            }
+    }
     auto reduce4 = [&](double v) {
         const double a = __dadd_rn(v, __shfl_down_sync(FULL_MASK, v, 1));   // lane0: l0+l1, lane2: l2+l3
         return __shfl_sync(FULL_MASK, __dadd_rn(a, __shfl_down_sync(FULL_MASK, a, 2)), 0);
@@ -137,12 +157,17 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_upward(
 
     // radius about the per-lane centre (upward-common.ispc:44-56)
     double r2 = 0;
-    if (lane < 4) {
+    {
         const double lx = ws != 0 ? __ddiv_rn(xsum, wsum) : 0.0;
         const double ly = ws != 0 ? __ddiv_rn(ysum, wsum) : 0.0;
-        for (int i = s + lane; i < e; i += 4) {
-            const double xr = __dsub_rn(xs[i], lx), yr = __dsub_rn(ys[i], ly);
-            r2 = fmax(r2, __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(yr, yr)));
+        for (int ch = 0; ch < nch; ++ch) {
+            const int c0 = s + ch * UP_CHUNK, cnt = min(UP_CHUNK, e - c0);
+            if (nch > 1) stage(c0, cnt);
+            if (lane < 4)
+                for (int j = lane; j < cnt; j += 4) {
+                    const double xr = __dsub_rn(sh.sx[j], lx), yr = __dsub_rn(sh.sy[j], ly);
+                    r2 = fmax(r2, __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(yr, yr)));
+                }
         }
     }
     r2 = fmax(r2, __shfl_down_sync(FULL_MASK, r2, 1));
@@ -164,20 +189,24 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_upward(
     double ar[P], ai[P];
 #pragma unroll
     for (int n = 0; n < P; ++n) ar[n] = ai[n] = 0;
-    for (int i = s + lane; i < e; i += 32) {
-        const double r0 = xs[i] - xcom, i0 = ys[i] - ycom, src = vs[i];
-        double pr = r0, pim = i0;
-        ar[0] -= r0 * src;
-        ai[0] -= i0 * src;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int c0 = s + ch * UP_CHUNK, cnt = min(UP_CHUNK, e - c0);
+        if (nch > 1) stage(c0, cnt);
+        for (int j = lane; j < cnt; j += 32) {
+            const double r0 = sh.sx[j] - xcom, i0 = sh.sy[j] - ycom, src = sh.sv[j];
+            double pr = r0, pim = i0;
+            ar[0] -= r0 * src;
+            ai[0] -= i0 * src;
 #pragma unroll
-        for (int n = 1; n < P; ++n) {
-            const double tr = pr * r0 - pim * i0;
-            const double ti = pr * i0 + pim * r0;
-            pr = tr;
-            pim = ti;
-            const double term = src * (1.0 / (n + 1));
-            ar[n] -= pr * term;
-            ai[n] -= pim * term;
+            for (int n = 1; n < P; ++n) {
+                const double tr = pr * r0 - pim * i0;
+                const double ti = pr * i0 + pim * r0;
+                pr = tr;
+                pim = ti;
+                const double term = src * (1.0 / (n + 1));
+                ar[n] -= pr * term;
+                ai[n] -= pim * term;
+            }
         }
     }
 #pragma unroll

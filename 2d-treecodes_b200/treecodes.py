@@ -66,7 +66,9 @@ class Stats(ctypes.Structure):
                 ("nnodes", ctypes.c_longlong), ("nleaves", ctypes.c_longlong),
                 ("ninner", ctypes.c_longlong), ("nlevels", ctypes.c_longlong),
                 ("n_e2l", ctypes.c_longlong), ("n_e2p", ctypes.c_longlong),
-                ("n_p2p", ctypes.c_longlong)]
+                ("n_p2p", ctypes.c_longlong), ("p2p_pairs", ctypes.c_longlong),
+                ("e2p_pairs", ctypes.c_longlong), ("e2l_pairs", ctypes.c_longlong),
+                ("l2p_targets", ctypes.c_longlong), ("launches", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -84,6 +84,11 @@ typedef struct {
     /* sizes of the last solve */
     long long nnodes, nleaves, ninner, nlevels;
     long long n_e2l, n_e2p, n_p2p;   /* interaction-list entries */
+    long long p2p_pairs;             /* source-target pairs evaluated directly */
+    long long e2p_pairs;             /* (target, cell) pairs evaluated from multipoles */
+    long long e2l_pairs;             /* (brick, cell) multipole-to-local translations */
+    long long l2p_targets;           /* targets evaluated from local expansions */
+    long long launches;              /* kernels launched by the last solve */
 } tc_stats;
 
 /* device < 0 selects the current device; stream may be NULL (the context creates one). */
