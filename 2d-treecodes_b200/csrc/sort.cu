@@ -12,8 +12,10 @@
 // finds its global offsets by a decoupled look-back over the tiles before it.  Tiles take
 // their ids from an atomic counter, so each waits only on tiles that already run; the waits
 // are bounded and raise DEVERR_SPIN_LIMIT instead of hanging.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <mutex>
 
 #include "tc_internal.h"
 
@@ -505,4 +507,133 @@ int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys
     return TC_OK;
 }
 
+// ---------------------------------------------------------------------------- allocation-free
+// Source sort for callers that cannot allocate device memory.  Everything the sort needs
+// besides the caller's inputs and outputs -- the second key/permutation buffer of the
+// ping-pong passes, the per-tile look-back words, the digit histograms, the tile counters,
+// the bounding-box partials and the error word -- lives in one static device array of fixed
+// size, so a call makes no cudaMalloc/cudaFree and no other allocating call.
+constexpr int NOALLOC_MAX_SOURCES = 1 << 20;
+constexpr int NA_MAX_TILES = (NOALLOC_MAX_SOURCES + RS_TILE - 1) / RS_TILE;
+constexpr int NA_MAX_BBOX_BLOCKS = 4096;
+constexpr size_t NA_OFF_KEYS = 0;
+constexpr size_t NA_OFF_PERM = NA_OFF_KEYS + sizeof(int) * NOALLOC_MAX_SOURCES;
+constexpr size_t NA_OFF_STATUS = NA_OFF_PERM + sizeof(int) * NOALLOC_MAX_SOURCES;
+constexpr size_t NA_OFF_HIST =
+    NA_OFF_STATUS + sizeof(unsigned) * RS_MAX_PASSES * NA_MAX_TILES * RS_RADIX;
+constexpr size_t NA_OFF_CTR = NA_OFF_HIST + sizeof(int) * 2 * RS_MAX_PASSES * RS_RADIX;
+constexpr size_t NA_OFF_ERR = NA_OFF_CTR + 256;
+constexpr size_t NA_OFF_DONE = NA_OFF_ERR + 256;
+constexpr size_t NA_OFF_PARTIALS = NA_OFF_DONE + 256;
+constexpr size_t NA_BYTES = NA_OFF_PARTIALS + sizeof(double4) * NA_MAX_BBOX_BLOCKS;  // ~9.2 MB
+
+// One copy per device that loads the library, held until the process exits.  In host code
+// the name is only a host-side handle: kernels get the device address from
+// cudaGetSymbolAddress (noalloc_scratch_base), never the symbol itself.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+static unsigned char *noalloc_scratch_base(int device) {
+    constexpr int MAX_DEVICES = 64;
+    static std::mutex mu;
+    static void *addr[MAX_DEVICES] = {};
+    if (device < 0 || device >= MAX_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            set_error(TC_ERR_CUDA, "tc_sort_sources_noalloc: cudaGetSymbolAddress failed: %s",
+                      cudaGetErrorString(e));
+            return nullptr;
+        }
+        addr[device] = p;
+    }
+    return static_cast<unsigned char *>(addr[device]);
+}
+
 }  // namespace tc
+
+extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const double *ysources,
+                                              const double *sourcevalues, int nsources,
+                                              int *keys, int *perm, double *xsorted,
+                                              double *ysorted, double *vsorted, double *frame,
+                                              void *cuda_stream) {
+    using namespace tc;
+    set_error(TC_OK, "");
+    const int n = nsources;
+    if (n < 0 || n > NOALLOC_MAX_SOURCES) {
+        set_error(TC_ERR_INVALID,
+                  "tc_sort_sources_noalloc: nsources = %d is outside [0, %d], the size of its "
+                  "fixed scratch array", n, NOALLOC_MAX_SOURCES);
+        return TC_ERR_INVALID;
+    }
+    if (n == 0) return TC_OK;
+    if (!xsources || !ysources || !sourcevalues || !keys || !perm || !xsorted || !ysorted ||
+        !vsorted || !frame) {
+        set_error(TC_ERR_INVALID, "tc_sort_sources_noalloc: NULL array argument");
+        return TC_ERR_INVALID;
+    }
+    int dev = 0;
+    TC_CUDA_TRY(cudaGetDevice(&dev));
+    unsigned char *base = noalloc_scratch_base(dev);
+    if (!base) {
+        if (treecode_last_status() == TC_OK)
+            set_error(TC_ERR_INVALID, "tc_sort_sources_noalloc: device %d not supported", dev);
+        return treecode_last_status();
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    int *keys_tmp = reinterpret_cast<int *>(base + NA_OFF_KEYS);
+    int *perm_tmp = reinterpret_cast<int *>(base + NA_OFF_PERM);
+    unsigned *status = reinterpret_cast<unsigned *>(base + NA_OFF_STATUS);
+    int *hist = reinterpret_cast<int *>(base + NA_OFF_HIST);
+    int *offsets = hist + RS_MAX_PASSES * RS_RADIX;
+    int *counter = reinterpret_cast<int *>(base + NA_OFF_CTR);
+    unsigned *err = reinterpret_cast<unsigned *>(base + NA_OFF_ERR);
+    unsigned *done = reinterpret_cast<unsigned *>(base + NA_OFF_DONE);
+    double4 *partials = reinterpret_cast<double4 *>(base + NA_OFF_PARTIALS);
+    Frame *fr = reinterpret_cast<Frame *>(frame);
+
+    // The array keeps the previous call's contents: clear what has to start at zero.
+    const int npasses = (2 * LMAX + 7) / 8;
+    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    TC_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned), s));
+    TC_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned), s));
+    TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * RS_MAX_PASSES * RS_RADIX, s));
+    TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, s));
+    TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX, s));
+
+    const int gb = std::min(grid_for(n, BBOX_THREADS, 4), NA_MAX_BBOX_BLOCKS);
+    k_bbox<<<gb, BBOX_THREADS, 0, s>>>(xsources, ysources, n, partials, done, fr);
+    TC_KERNEL_CHECK();
+    k_keys<<<grid_for(n, 256), 256, 0, s>>>(xsources, ysources, n, fr, keys);
+    TC_KERNEL_CHECK();
+    k_hist<<<grid_for(n, 256, 4), 256, 0, s>>>(keys, n, npasses, hist);
+    TC_KERNEL_CHECK();
+    k_hist_scan<<<npasses, RS_RADIX, 0, s>>>(hist, offsets);
+    TC_KERNEL_CHECK();
+    // keys -> tmp -> keys -> tmp -> keys: four passes end in the caller's arrays
+    const int *ki = keys, *vi = nullptr;
+    for (int p = 0; p < npasses; ++p) {
+        int *ko = (p & 1) ? keys : keys_tmp;
+        int *vo = (p & 1) ? perm : perm_tmp;
+        k_onesweep<<<ntiles, RS_THREADS, 0, s>>>(ki, vi, ko, vo, n, 8 * p, offsets + p * RS_RADIX,
+                                                  status + (size_t)p * ntiles * RS_RADIX,
+                                                  counter + p, err);
+        TC_KERNEL_CHECK();
+        ki = ko;
+        vi = vo;
+    }
+    static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in keys/perm");
+    k_gather3<<<grid_for(n, 256), 256, 0, s>>>(xsources, ysources, sourcevalues, perm, n,
+                                                xsorted, ysorted, vsorted, err);
+    TC_KERNEL_CHECK();
+    unsigned h_err = 0;
+    TC_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    TC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h_err) {
+        set_error(h_err & DEVERR_SPIN_LIMIT ? TC_ERR_TIMEOUT : TC_ERR_CUDA,
+                  "tc_sort_sources_noalloc: device error flags 0x%x", h_err);
+        return treecode_last_status();
+    }
+    return TC_OK;
+}

@@ -50,6 +50,7 @@ SIGNATURES = {
     "tc_tree_copy": (_i, [_vp] + [_vp] * 19),
     "tc_direct_potential_device": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp]),
     "tc_direct_force_device": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "tc_sort_sources_noalloc": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "tc_measure_fma_peak": (_i, [_i, _dp]),
     "tc_version": (ctypes.c_char_p, []),
 }

@@ -145,6 +145,38 @@ TC_API int tc_direct_force_device(tc_context *ctx, const double *xsources,
                                   int nsources, const double *xtargets, const double *ytargets,
                                   int ntargets, double *xout, double *yout);
 
+/* Allocation-free source sort.  No counterpart in the reference.
+ *
+ * Some callers cannot call cudaMalloc at the moment they need the tree: code that owns all of
+ * device memory through its own pool (a flow solver or a framework allocator that hands out
+ * every byte and must not be bypassed), code on a latency-critical path where an allocation's
+ * implicit device synchronisation and unbounded cost are not acceptable, and long-running
+ * services that must not grow or fragment device memory after start-up.  For them this entry
+ * point runs the first stage
+ * of the solve -- padded bounding square, 30-bit Morton keys, stable radix sort, gather of
+ * x/y/value into Morton order, as drivers/sort-sources.cpp:23-132 of the reference defines it
+ * -- with all of its scratch memory in one fixed, statically allocated device array.
+ *
+ *   nsources <= TC_NOALLOC_MAX_SOURCES (1,048,576); larger inputs are rejected with
+ *   TC_ERR_INVALID and a message naming the limit.  The scratch array is about 9.2 MB, held by
+ *   every GPU that loads the library until the process exits.
+ *   All arrays are device pointers supplied by the caller: inputs xsources/ysources/
+ *   sourcevalues; outputs keys and perm (nsources ints: sorted keys and, for each sorted
+ *   position, the input index), xsorted/ysorted/vsorted (nsources doubles) and frame
+ *   (4 doubles: xmin, ymin, ext of the padded square, and the key scale 2^15 / ext).
+ *   The work is ordered on cuda_stream (NULL: the legacy default stream) and complete when the
+ *   call returns.  The results equal those of the allocating solve path bit for bit.
+ *   The first call on each device looks up the array's device address (cudaGetSymbolAddress);
+ *   make that first call before any stream capture begins.
+ *   All calls share the one array: calls whose GPU work could overlap (other streams, other
+ *   threads) race on it and must be serialised by the caller.  The call allocates nothing:
+ *   no cudaMalloc, no cudaFree, no allocating library routine. */
+#define TC_NOALLOC_MAX_SOURCES (1 << 20)
+TC_API int tc_sort_sources_noalloc(const double *xsources, const double *ysources,
+                                   const double *sourcevalues, int nsources, int *keys,
+                                   int *perm, double *xsorted, double *ysorted, double *vsorted,
+                                   double *frame, void *cuda_stream);
+
 /* Measured FMA throughput of the current device in TFLOP/s (fp64 != 0: FP64, else FP32). */
 TC_API int tc_measure_fma_peak(int fp64, double *tflops);
 
