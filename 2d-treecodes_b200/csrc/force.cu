@@ -26,7 +26,9 @@
 
 namespace tc {
 
-__constant__ BinomTable c_binom_f = make_binom_table();
+// In global memory (read through L1): every lane reads a different entry, which the constant
+// cache would serialise.
+__device__ const BinomTable c_binom_f = make_binom_table();
 
 struct Brick {
     double x0b, y0b;        // brick centre
@@ -186,7 +188,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     const int2 *__restrict__ range, const double *__restrict__ xs,
     const double *__restrict__ ys, const double *__restrict__ vs,
     const int *__restrict__ offs, const int *__restrict__ lists, double *__restrict__ xout,
-    double *__restrict__ yout) {
+    double *__restrict__ yout, int *brick_ctr) {
     __shared__ EvalShared<P> shared[EV_WARPS];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     EvalShared<P> &sh = shared[warp];
@@ -202,8 +204,13 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             bsg[k - 1] = (k & 1 ? -1.0 : 1.0) * c_binom_f.c[l + k - 1][k - 1];
     }
 
-    for (int brick = blockIdx.x * EV_WARPS + warp; brick < nbricks;
-         brick += gridDim.x * EV_WARPS) {
+    // Bricks differ in cost by orders of magnitude (a brick on a dense sheet versus one in empty
+    // space), so warps take them one at a time from a global counter.
+    for (;;) {
+        int brick = 0;
+        if (lane == 0) brick = atomicAdd(brick_ctr, 1);
+        brick = __shfl_sync(FULL_MASK, brick, 0);
+        if (brick >= nbricks) break;
         const int blk = brick >> 4, q = brick & 15;
         const double h = hs[blk];
         const Brick b = brick_geometry(x0s[blk], y0s[blk], h, q);
@@ -267,16 +274,27 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         // ---------------- E2P (force-kernels.m4:57-98): w = m/z - sum (j+1) a_j z^-(j+2)
         {
             const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
-            for (int it = beg; it < end; ++it) {
-                const int node = lists[it];
-                const TNode nd = tnode[node];
-                const double m = mass[node];
-                __syncwarp();
+            // the next cell's record and coefficients are loaded while the current one is used
+            TNode nd_n = {};
+            double m_n = 0, cr_n = 0, ci_n = 0;
+            auto fetch = [&](int at) {
+                const int node = lists[at];
+                nd_n = tnode[node];
+                m_n = mass[node];
                 if (lane < P) {
                     const double *ex = exps + (size_t)node * 2 * P;
-                    sh.coef[lane] = {(lane + 1) * ex[lane], (lane + 1) * ex[P + lane]};
+                    cr_n = (lane + 1) * ex[lane];
+                    ci_n = (lane + 1) * ex[P + lane];
                 }
+            };
+            if (beg < end) fetch(beg);
+            for (int it = beg; it < end; ++it) {
+                const TNode nd = nd_n;
+                const double m = m_n;
                 __syncwarp();
+                if (lane < P) sh.coef[lane] = {cr_n, ci_n};
+                __syncwarp();
+                if (it + 1 < end) fetch(it + 1);
                 const double rx = (b.xlo - nd.xcom) + tx * h;
                 const double ry0 = (b.ylo - nd.ycom) + ty * h;
                 const double ry1 = (b.ylo - nd.ycom) + (ty + 4) * h;
@@ -306,29 +324,53 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             const int beg = offs[2 * nbricks + brick], end = offs[2 * nbricks + brick + 1];
             const double xt = b.xlo + tx * h;
             const double yt0 = b.ylo + ty * h, yt1 = b.ylo + (ty + 4) * h;
-            for (int it = beg; it < end; ++it) {
-                const int2 rg = range[lists[it]];
-                for (int s0 = rg.x; s0 < rg.y; s0 += EV_CHUNK) {
-                    const int cnt = min(EV_CHUNK, rg.y - s0);
-                    __syncwarp();
-                    if (lane < cnt) {
-                        sh.sxy[lane] = make_double2(xs[s0 + lane], ys[s0 + lane]);
-                        sh.sv[lane] = vs[s0 + lane];
-                    }
-                    __syncwarp();
-                    for (int k = 0; k < cnt; ++k) {
-                        const double2 sp = sh.sxy[k];
-                        const double v = sh.sv[k];
-                        const double xr = xt - sp.x;
-                        const double xr2e = fma(xr, xr, eps);
-                        const double yr0 = yt0 - sp.y, yr1 = yt1 - sp.y;
-                        const double f0 = v * rcp_nr(fma(yr0, yr0, xr2e));
-                        const double f1 = v * rcp_nr(fma(yr1, yr1, xr2e));
-                        ax0 = fma(xr, f0, ax0);
-                        ay0 = fma(yr0, f0, ay0);
-                        ax1 = fma(xr, f1, ax1);
-                        ay1 = fma(yr1, f1, ay1);
-                    }
+            // Tiles of up to EV_CHUNK consecutive sources walk the listed leaves in order; the
+            // next tile is loaded into registers while the current one is evaluated.
+            int it = beg, s_next = 0, e_next = 0;
+            auto next_tile = [&](int &t0, int &tn) {
+                while (s_next >= e_next && it < end) {
+                    const int2 rg = range[lists[it++]];
+                    s_next = rg.x;
+                    e_next = rg.y;
+                }
+                t0 = s_next;
+                tn = min(EV_CHUNK, e_next - s_next);
+                if (tn < 0) tn = 0;
+                s_next += tn;
+            };
+            int t0, tn;
+            next_tile(t0, tn);
+            double px = 0, py = 0, pv = 0;
+            if (lane < tn) {
+                px = xs[t0 + lane];
+                py = ys[t0 + lane];
+                pv = vs[t0 + lane];
+            }
+            while (tn > 0) {
+                const int cnt = tn;
+                __syncwarp();
+                sh.sxy[lane] = make_double2(px, py);
+                sh.sv[lane] = pv;
+                __syncwarp();
+                next_tile(t0, tn);
+                if (lane < tn) {
+                    px = xs[t0 + lane];
+                    py = ys[t0 + lane];
+                    pv = vs[t0 + lane];
+                }
+#pragma unroll 4
+                for (int k = 0; k < cnt; ++k) {
+                    const double2 sp = sh.sxy[k];
+                    const double v = sh.sv[k];
+                    const double xr = xt - sp.x;
+                    const double xr2e = fma(xr, xr, eps);
+                    const double yr0 = yt0 - sp.y, yr1 = yt1 - sp.y;
+                    const double f0 = v * rcp_nr(fma(yr0, yr0, xr2e));
+                    const double f1 = v * rcp_nr(fma(yr1, yr1, xr2e));
+                    ax0 = fma(xr, f0, ax0);
+                    ay0 = fma(yr0, f0, ay0);
+                    ax1 = fma(xr, f1, ax1);
+                    ay1 = fma(yr1, f1, ay1);
                 }
             }
         }
@@ -398,12 +440,21 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                                                 slot_ptr<unsigned long long>(c, S_STATS));
     TC_KERNEL_CHECK();
     phase_mark(c, 4);
+    int *brick_ctr;
+    if ((rc = ensure(c, S_BRICK_CTR, 4, &brick_ctr))) return rc;
+    TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, sizeof(int), c.stream));
+    static int occ = 0;
+    if (!occ) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_force_eval<ORDER_FORCE>,
+                                                      EV_WARPS * 32, 0);
+        if (occ <= 0) occ = 1;
+    }
     const int evgrid = (int)std::min<long long>((nbricks + EV_WARPS - 1) / EV_WARPS,
-                                                (long long)sm_count() * 8);
+                                                (long long)sm_count() * occ);
     k_force_eval<ORDER_FORCE><<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
         nbricks, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
         slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-        slot_ptr<double>(c, S_VS), offs, lists, xout, yout);
+        slot_ptr<double>(c, S_VS), offs, lists, xout, yout, brick_ctr);
     TC_KERNEL_CHECK();
     return TC_OK;
 }
