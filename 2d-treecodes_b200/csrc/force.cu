@@ -69,6 +69,9 @@ __device__ __forceinline__ int classify(const TNode &nd, const Brick &b, double 
 
 constexpr int TR_WARPS = 4;
 constexpr int TR_STACK = 2048;
+// A brick's evaluation is split into tasks of at most P2P_SEG near-field sources (task 0 also
+// does the far field), so that the few bricks on a dense region do not serialise the kernel.
+constexpr int P2P_SEG = 2048;
 
 template <bool FILL>
 __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
@@ -96,6 +99,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
             }
         }
         int n[3] = {0, 0, 0};
+        int bsrc = 0;   // per lane: sources of the P2P leaves it classified for this brick
         if (lane == 0) stack[0] = 0;
         int top = 1;
         __syncwarp();
@@ -109,6 +113,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                     const TNode nd = tnode[node];
                     kind = classify(nd, b, inv_theta, theta2);
                     child = nd.child;
+                    if (kind == K_P2P) bsrc += nd.count;
                     if (FILL && kind == K_P2P) p2p_sources += (unsigned)nd.count;
                     if (kind == K_DESCEND && (child <= node || child + 4 > nnodes)) {
                         atomicOr(err, DEVERR_BOUNDS);
@@ -143,10 +148,15 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
             top += nd4;
             __syncwarp();
         }
-        if (!FILL && lane == 0) {
-            counts[brick] = n[0];
-            counts[nbricks + brick] = n[1];
-            counts[2 * nbricks + brick] = n[2];
+        if (!FILL) {
+            const int total = __reduce_add_sync(FULL_MASK, bsrc);
+            if (lane == 0) {
+                counts[brick] = n[0];
+                counts[nbricks + brick] = n[1];
+                counts[2 * nbricks + brick] = n[2];
+                // evaluation tasks: the brick's P2P sources in segments of at most P2P_SEG
+                counts[3 * nbricks + brick] = max(1, (total + P2P_SEG - 1) / P2P_SEG);
+            }
         }
         __syncwarp();
     }
@@ -188,7 +198,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     const int2 *__restrict__ range, const double *__restrict__ xs,
     const double *__restrict__ ys, const double *__restrict__ vs,
     const int *__restrict__ offs, const int *__restrict__ lists, double *__restrict__ xout,
-    double *__restrict__ yout, int *brick_ctr) {
+    double *__restrict__ yout, double *__restrict__ partial, int *task_ctr) {
     __shared__ EvalShared<P> shared[EV_WARPS];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     EvalShared<P> &sh = shared[warp];
@@ -204,20 +214,34 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             bsg[k - 1] = (k & 1 ? -1.0 : 1.0) * c_binom_f.c[l + k - 1][k - 1];
     }
 
-    // Bricks differ in cost by orders of magnitude (a brick on a dense sheet versus one in empty
-    // space), so warps take them one at a time from a global counter.
+    // Tasks: brick b owns tasks [toff[b], toff[b+1]) (relative to toff[0]); task 0 of a brick
+    // evaluates its far field and the first P2P_SEG near-field sources, task p > 0 the p-th
+    // segment.  Costs vary by orders of magnitude between bricks, so warps take tasks one at a
+    // time from a global counter.
+    const int *toff = offs + 3 * nbricks;
+    const int tbase = toff[0];
+    const int ntasks = toff[nbricks] - tbase;
     for (;;) {
-        int brick = 0;
-        if (lane == 0) brick = atomicAdd(brick_ctr, 1);
-        brick = __shfl_sync(FULL_MASK, brick, 0);
-        if (brick >= nbricks) break;
+        int task = 0;
+        if (lane == 0) task = atomicAdd(task_ctr, 1);
+        task = __shfl_sync(FULL_MASK, task, 0);
+        if (task >= ntasks) break;
+        int blo = 0, bhi = nbricks;   // toff[blo] - tbase <= task < toff[bhi] - tbase
+        while (bhi - blo > 1) {
+            const int mid = (blo + bhi) >> 1;
+            if (toff[mid] - tbase <= task) blo = mid;
+            else bhi = mid;
+        }
+        const int brick = blo;
+        const int part = task - (toff[brick] - tbase);
+        const int nparts = toff[brick + 1] - toff[brick];
         const int blk = brick >> 4, q = brick & 15;
         const double h = hs[blk];
         const Brick b = brick_geometry(x0s[blk], y0s[blk], h, q);
         double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
 
         // ---------------- E2L: local expansion about the brick centre (force-kernels.m4:102-155)
-        {
+        if (part == 0) {
             const int beg = offs[brick], end = offs[brick + 1];
             cplx L = {0.0, 0.0};
             const int l = lane + 1;
@@ -254,7 +278,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         }
 
         // ---------------- L2P (force-kernels.m4:157-191): sum_l l L_l z^(l-1), z about the centre
-        {
+        if (part == 0) {
             const double xr = -3.5 * h + tx * h;
             const double yr0 = -3.5 * h + ty * h, yr1 = -3.5 * h + (ty + 4) * h;
             cplx acc0 = {P * sh.local[P].re, P * sh.local[P].im}, acc1 = acc0;
@@ -272,7 +296,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         }
 
         // ---------------- E2P (force-kernels.m4:57-98): w = m/z - sum (j+1) a_j z^-(j+2)
-        {
+        if (part == 0) {
             const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
             // the next cell's record and coefficients are loaded while the current one is used
             TNode nd_n = {};
@@ -325,8 +349,20 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             const double xt = b.xlo + tx * h;
             const double yt0 = b.ylo + ty * h, yt1 = b.ylo + (ty + 4) * h;
             // Tiles of up to EV_CHUNK consecutive sources walk the listed leaves in order; the
-            // next tile is loaded into registers while the current one is evaluated.
+            // next tile is loaded into registers while the current one is evaluated.  This task
+            // covers sources [part * P2P_SEG, (part + 1) * P2P_SEG) of the brick's sequence.
             int it = beg, s_next = 0, e_next = 0;
+            int skip = part * P2P_SEG, budget = P2P_SEG;
+            while (it < end) {
+                const int2 rg = range[lists[it++]];
+                const int cnt = rg.y - rg.x;
+                if (skip < cnt) {
+                    s_next = rg.x + skip;
+                    e_next = rg.y;
+                    break;
+                }
+                skip -= cnt;
+            }
             auto next_tile = [&](int &t0, int &tn) {
                 while (s_next >= e_next && it < end) {
                     const int2 rg = range[lists[it++]];
@@ -334,9 +370,10 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
                     e_next = rg.y;
                 }
                 t0 = s_next;
-                tn = min(EV_CHUNK, e_next - s_next);
+                tn = min(min(EV_CHUNK, e_next - s_next), budget);
                 if (tn < 0) tn = 0;
                 s_next += tn;
+                budget -= tn;
             };
             int t0, tn;
             next_tile(t0, tn);
@@ -375,6 +412,47 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             }
         }
 
+        if (nparts == 1) {
+            const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
+            const size_t o0 = (size_t)blk * BLOCKSIZE * BLOCKSIZE + (by + ty) * BLOCKSIZE + bx + tx;
+            const size_t o1 = o0 + 4 * BLOCKSIZE;
+            xout[o0] = ax0;
+            yout[o0] = ay0;
+            xout[o1] = ax1;
+            yout[o1] = ay1;
+        } else {
+            // partial result of this task; k_force_gather_parts adds the parts in order
+            double *pp = partial + (size_t)task * 4 * 32;
+            pp[lane] = ax0;
+            pp[32 + lane] = ay0;
+            pp[64 + lane] = ax1;
+            pp[96 + lane] = ay1;
+        }
+        __syncwarp();
+    }
+}
+
+// Sum of the parts of every multi-task brick, in task order (deterministic).
+__global__ void k_force_gather_parts(int nbricks, const int *__restrict__ offs,
+                                     const double *__restrict__ partial, double *__restrict__ xout,
+                                     double *__restrict__ yout) {
+    const int lane = lane_id();
+    const int *toff = offs + 3 * nbricks;
+    const int tbase = toff[0];
+    for (int brick = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; brick < nbricks;
+         brick += (gridDim.x * blockDim.x) >> 5) {
+        const int t0 = toff[brick] - tbase, np = toff[brick + 1] - toff[brick];
+        if (np <= 1) continue;
+        double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
+        for (int p = 0; p < np; ++p) {
+            const double *pp = partial + (size_t)(t0 + p) * 4 * 32;
+            ax0 += pp[lane];
+            ay0 += pp[32 + lane];
+            ax1 += pp[64 + lane];
+            ay1 += pp[96 + lane];
+        }
+        const int tx = lane & 7, ty = lane >> 3;
+        const int blk = brick >> 4, q = brick & 15;
         const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
         const size_t o0 = (size_t)blk * BLOCKSIZE * BLOCKSIZE + (by + ty) * BLOCKSIZE + bx + tx;
         const size_t o1 = o0 + 4 * BLOCKSIZE;
@@ -382,7 +460,6 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         yout[o0] = ay0;
         xout[o1] = ax1;
         yout[o1] = ay1;
-        __syncwarp();
     }
 }
 
@@ -406,9 +483,10 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     const int nbricks = nblocks * 16;
     if (nbricks == 0) return TC_OK;
     int rc;
+    // counts / offsets: E2L | E2P | P2P list lengths and evaluation tasks, nbricks each
     int *counts, *offs;
-    if ((rc = ensure(c, S_FCOUNT, (size_t)3 * nbricks, &counts)) ||
-        (rc = ensure(c, S_FOFF, (size_t)3 * nbricks + 1, &offs)))
+    if ((rc = ensure(c, S_FCOUNT, (size_t)4 * nbricks, &counts)) ||
+        (rc = ensure(c, S_FOFF, (size_t)4 * nbricks + 1, &offs)))
         return rc;
     const TNode *tnode = slot_ptr<TNode>(c, S_TNODE);
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
@@ -418,15 +496,14 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                                                  tnode, c.nnodes, counts, nullptr, nullptr,
                                                                  err, nullptr);
     TC_KERNEL_CHECK();
-    if ((rc = exclusive_scan(c, counts, offs, 3 * nbricks))) return rc;
+    if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
     int tot[4];
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, offs + nbricks, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 1, offs + 2 * nbricks, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 2, offs + 3 * nbricks, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    for (int k = 0; k < 4; ++k)
+        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + k, offs + (k + 1) * nbricks, sizeof(int),
+                                    cudaMemcpyDeviceToHost, c.stream));
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    tot[0] = (int)c.h_pinned[0];
-    tot[1] = (int)c.h_pinned[1];
-    tot[2] = (int)c.h_pinned[2];
+    for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[k];
+    const int ntasks = tot[3] - tot[2];
     c.counts.n_e2l = tot[0];
     c.counts.n_e2p = tot[1] - tot[0];
     c.counts.n_p2p = tot[2] - tot[1];
@@ -441,7 +518,10 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     TC_KERNEL_CHECK();
     phase_mark(c, 4);
     int *brick_ctr;
-    if ((rc = ensure(c, S_BRICK_CTR, 4, &brick_ctr))) return rc;
+    double *partial;
+    if ((rc = ensure(c, S_BRICK_CTR, 4, &brick_ctr)) ||
+        (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)))
+        return rc;
     TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, sizeof(int), c.stream));
     static int occ = 0;
     if (!occ) {
@@ -449,13 +529,18 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                                       EV_WARPS * 32, 0);
         if (occ <= 0) occ = 1;
     }
-    const int evgrid = (int)std::min<long long>((nbricks + EV_WARPS - 1) / EV_WARPS,
+    const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
                                                 (long long)sm_count() * occ);
     k_force_eval<ORDER_FORCE><<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
         nbricks, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
         slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-        slot_ptr<double>(c, S_VS), offs, lists, xout, yout, brick_ctr);
+        slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr);
     TC_KERNEL_CHECK();
+    if (ntasks > nbricks) {
+        k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8, (long long)sm_count() * 16),
+                               256, 0, c.stream>>>(nbricks, offs, partial, xout, yout);
+        TC_KERNEL_CHECK();
+    }
     return TC_OK;
 }
 
