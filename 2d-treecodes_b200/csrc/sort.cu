@@ -331,6 +331,153 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
     }
 }
 
+// The same pass for the sources, carrying their coordinates and values along with the key and
+// the input index, so that the sorted x/y/v come out of the last pass without a random gather
+// (which costs ~300 B of DRAM traffic per source on HBM, against 24 + 24 B here).  The local
+// reordering goes through one shared buffer, one component at a time.
+constexpr size_t XYV_SMEM = (size_t)RS_TILE * sizeof(int) + (size_t)RS_TILE * sizeof(double) +
+                            (size_t)RS_WARPS * RS_RADIX * sizeof(int) + 2 * RS_RADIX * sizeof(int) +
+                            16;
+
+__global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
+    const int *__restrict__ keys_in, const int *__restrict__ idx_in,
+    const double *__restrict__ x_in, const double *__restrict__ y_in,
+    const double *__restrict__ v_in, int *__restrict__ keys_out, int *__restrict__ idx_out,
+    double *__restrict__ x_out, double *__restrict__ y_out, double *__restrict__ v_out, int n,
+    int shift, const int *__restrict__ digit_offsets, unsigned *status, int *tile_counter,
+    unsigned *err) {
+    extern __shared__ __align__(16) unsigned char xyv_smem[];
+    int *s_keys = reinterpret_cast<int *>(xyv_smem);
+    double *s_buf = reinterpret_cast<double *>(xyv_smem + RS_TILE * sizeof(int));
+    int *s_ibuf = reinterpret_cast<int *>(s_buf);
+    int(*s_whist)[RS_RADIX] = reinterpret_cast<int(*)[RS_RADIX]>(
+        xyv_smem + RS_TILE * (sizeof(int) + sizeof(double)));
+    int *s_tile_start = &s_whist[RS_WARPS][0];
+    int *s_global = s_tile_start + RS_RADIX;
+    int *s_tile = s_global + RS_RADIX;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) *s_tile = atomicAdd(tile_counter, 1);
+    for (int i = tid; i < RS_WARPS * RS_RADIX; i += RS_THREADS) (&s_whist[0][0])[i] = 0;
+    __syncthreads();
+    const int tile = *s_tile;
+    const int tile_base = tile * RS_TILE;
+    const int warp_base = tile_base + warp * (RS_ITEMS * 32);
+
+    int key[RS_ITEMS], pos[RS_ITEMS];
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        key[k] = idx < n ? keys_in[idx] : 0;
+    }
+
+    // stable rank within the warp, items visited in their original order (k, lane)
+    const unsigned lt = lanemask_lt();
+    int *hist = s_whist[warp];
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        const bool valid = idx < n;
+        const unsigned vmask = __ballot_sync(FULL_MASK, valid);
+        const int d = (key[k] >> shift) & 0xFF;
+        unsigned peers = 0;
+        if (valid) peers = __match_any_sync(vmask, d);
+        const int old = valid ? hist[d] : 0;
+        __syncwarp();
+        if (valid && (peers & lt) == 0) hist[d] = old + __popc(peers);
+        __syncwarp();
+        pos[k] = old + __popc(peers & lt);
+    }
+    __syncthreads();
+
+    const int d = tid;
+    int total = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) {
+        const int c = s_whist[w][d];
+        s_whist[w][d] = total;
+        total += c;
+    }
+    unsigned *mine = status + (size_t)tile * RS_RADIX + d;
+    int excl = 0;
+    if (tile == 0) {
+        atomicExch(mine, RS_FLAG_INC | (unsigned)total);
+    } else {
+        atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
+        int j = tile - 1;
+        int spins = 0;
+        while (j >= 0) {
+            const unsigned s = ld_volatile(status + (size_t)j * RS_RADIX + d);
+            const unsigned flag = s & ~RS_VALMASK;
+            if (flag == 0) {
+                if (++spins > RS_SPIN_LIMIT) {
+                    atomicOr(err, DEVERR_SPIN_LIMIT);
+                    break;
+                }
+                continue;
+            }
+            excl += (int)(s & RS_VALMASK);
+            if (flag == RS_FLAG_INC) break;
+            --j;
+        }
+        atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
+    }
+    const int start = block_exclusive_scan(total, nullptr);
+    s_tile_start[d] = start;
+    s_global[d] = digit_offsets[d] + excl - start;
+    __syncthreads();
+
+    // local sorted positions (pos held the in-warp rank); keys and input indices first
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        int p = -1;
+        if (idx < n) {
+            const int dk = (key[k] >> shift) & 0xFF;
+            p = s_tile_start[dk] + s_whist[warp][dk] + pos[k];
+            if ((unsigned)p >= (unsigned)RS_TILE) {
+                atomicOr(err, DEVERR_BOUNDS);
+                p = -1;
+            } else {
+                s_keys[p] = key[k];
+                s_ibuf[p] = idx_in ? idx_in[idx] : idx;
+            }
+        }
+        pos[k] = p;
+    }
+    __syncthreads();
+
+    const int tile_n = min(RS_TILE, n - tile_base);
+    // global position of local slot j
+    auto gpos = [&](int j) { return s_global[(s_keys[j] >> shift) & 0xFF] + j; };
+    for (int j = tid; j < tile_n; j += RS_THREADS) {
+        const int g = gpos(j);
+        if ((unsigned)g >= (unsigned)n) {
+            atomicOr(err, DEVERR_BOUNDS);
+            continue;
+        }
+        keys_out[g] = s_keys[j];
+        idx_out[g] = s_ibuf[j];
+    }
+    // then x, y and v, one component at a time through the same buffer
+#pragma unroll 1
+    for (int comp = 0; comp < 3; ++comp) {
+        const double *src = comp == 0 ? x_in : (comp == 1 ? y_in : v_in);
+        double *dst = comp == 0 ? x_out : (comp == 1 ? y_out : v_out);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < RS_ITEMS; ++k) {
+            const int idx = warp_base + k * 32 + lane;
+            if (pos[k] >= 0) s_buf[pos[k]] = src[idx];
+        }
+        __syncthreads();
+        for (int j = tid; j < tile_n; j += RS_THREADS) {
+            const int g = gpos(j);
+            if ((unsigned)g < (unsigned)n) dst[g] = s_buf[j];
+        }
+    }
+}
+
 static int grid_for(int n, int threads, int per_sm = 8) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -483,18 +630,56 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     TC_KERNEL_CHECK();
     k_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(x, y, n, frame, keys);
     TC_KERNEL_CHECK();
-    int *ko, *vo;
-    // ping-pong keys -> keys2/perm2 -> keys/perm -> ...: an even number of passes (4 for
-    // 30-bit keys) ends in keys/perm.
-    if ((rc = radix_sort_pairs(c, keys, nullptr, n, 2 * LMAX, keys2, perm2, keys, perm, &ko, &vo)))
-        return rc;
-    if (ko != keys) {
-        TC_CUDA_TRY(cudaMemcpyAsync(keys, ko, sizeof(int) * n, cudaMemcpyDeviceToDevice, c.stream));
-        TC_CUDA_TRY(cudaMemcpyAsync(perm, vo, sizeof(int) * n, cudaMemcpyDeviceToDevice, c.stream));
+
+    // four 8-bit passes carrying (index, x, y, v); the ping-pong
+    // input -> tmp -> sorted -> tmp -> sorted ends in keys/perm/xs/ys/vs
+    if (n >= (1 << 30)) {
+        set_error(TC_ERR_INVALID, "too many sources for the radix sort (%d)", n);
+        return TC_ERR_INVALID;
     }
-    k_gather3<<<grid_for(n, 256), 256, 0, c.stream>>>(x, y, v, perm, n, xs, ys, vs,
-                                                       slot_ptr<unsigned>(c, S_ERR));
+    double *x2, *y2, *v2;
+    int *hist, *counter;
+    unsigned *status;
+    const int npasses = (2 * LMAX + 7) / 8;
+    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    if ((rc = ensure(c, S_X2, n, &x2)) || (rc = ensure(c, S_Y2, n, &y2)) ||
+        (rc = ensure(c, S_V2, n, &v2)) ||
+        (rc = ensure(c, S_RS_HIST, 2 * RS_MAX_PASSES * RS_RADIX, &hist)) ||
+        (rc = ensure(c, S_RS_COUNTER, RS_MAX_PASSES, &counter)) ||
+        (rc = ensure(c, S_RS_STATUS, (size_t)RS_MAX_PASSES * ntiles * RS_RADIX, &status)))
+        return rc;
+    int *offsets = hist + RS_MAX_PASSES * RS_RADIX;
+    TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * RS_MAX_PASSES * RS_RADIX, c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
+                                c.stream));
+    k_hist<<<grid_for(n, 256, 4), 256, 0, c.stream>>>(keys, n, npasses, hist);
     TC_KERNEL_CHECK();
+    k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
+    TC_KERNEL_CHECK();
+    static bool attr = false;
+    if (!attr) {
+        TC_CUDA_TRY(cudaFuncSetAttribute(k_onesweep_xyv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)XYV_SMEM));
+        attr = true;
+    }
+    unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in the sorted arrays");
+    for (int p = 0; p < npasses; ++p) {
+        const bool odd = p & 1;
+        const int *ki = odd ? keys2 : keys;
+        const int *ii = p == 0 ? nullptr : (odd ? perm2 : perm);
+        const double *xi = p == 0 ? x : (odd ? x2 : xs);
+        const double *yi = p == 0 ? y : (odd ? y2 : ys);
+        const double *vi = p == 0 ? v : (odd ? v2 : vs);
+        int *ko = odd ? keys : keys2, *io = odd ? perm : perm2;
+        double *xo = odd ? xs : x2, *yo = odd ? ys : y2, *vo = odd ? vs : v2;
+        k_onesweep_xyv<<<ntiles, RS_THREADS, XYV_SMEM, c.stream>>>(
+            ki, ii, xi, yi, vi, ko, io, xo, yo, vo, n, 8 * p, offsets + p * RS_RADIX,
+            status + (size_t)p * ntiles * RS_RADIX, counter + p, err);
+        TC_KERNEL_CHECK();
+    }
+    (void)perm2;
     c.nsrc = n;
     return TC_OK;
 }
