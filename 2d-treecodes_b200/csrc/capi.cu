@@ -194,10 +194,6 @@ static int force_device(Context &c, double theta, const double *xs, const double
         TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
         return TC_OK;
     }
-    if (c.precision != 0) {
-        set_error(TC_ERR_INVALID, "precision mode %d is not available yet", c.precision);
-        return TC_ERR_INVALID;
-    }
     int rc;
     phase_mark(c, 0);
     if ((rc = build_tree(c, 1, xs, ys, vs, n))) return rc;

@@ -176,7 +176,32 @@ struct EvalShared {
     cplx local[P + 1];            // local expansion L_1..L_P
     double2 sxy[EV_CHUNK];        // P2P source tile
     double sv[EV_CHUNK];
+    // mixed form: scaled E2P coefficients and the P2P tile as float offsets (hi + lo) from the
+    // brick corner
+    float2 coef32[P];
+    float sxh[EV_CHUNK], sxl[EV_CHUNK], syh[EV_CHUNK], syl[EV_CHUNK], sv32[EV_CHUNK];
 };
+
+__device__ __forceinline__ float rcp_approx_f32(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Compensated accumulation: (hi, lo) += x with an error-free two-sum (Knuth).
+__device__ __forceinline__ void two_sum_acc(float &hi, float &lo, float x) {
+    const float s = hi + x;
+    const float bb = s - hi;
+    const float err = (hi - (s - bb)) + (x - bb);
+    hi = s;
+    lo += err;
+}
+
+// A double split into two floats whose sum is within ~2^-48 relative of it.
+__device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+}
 
 // z^e for e = 1..31 by binary powering
 __device__ __forceinline__ cplx cpow_int(cplx z, int e) {
@@ -190,7 +215,10 @@ __device__ __forceinline__ cplx cpow_int(cplx z, int e) {
     return r;
 }
 
-template <int P>
+// MIXED = false: plain FP64.  MIXED = true: P2P and E2P in FP32 (float offsets from the brick
+// corner split into hi + lo parts, scaled multipole coefficients, compensated per-target
+// sums); the local expansion (E2L, L2P) stays FP64.
+template <int P, bool MIXED>
 __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     int nbricks, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, const TNode *__restrict__ tnode,
@@ -198,7 +226,9 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     const int2 *__restrict__ range, const double *__restrict__ xs,
     const double *__restrict__ ys, const double *__restrict__ vs,
     const int *__restrict__ offs, const int *__restrict__ lists, double *__restrict__ xout,
-    double *__restrict__ yout, double *__restrict__ partial, int *task_ctr) {
+    double *__restrict__ yout, double *__restrict__ partial, int *task_ctr,
+    const float2 *__restrict__ sexp, const float *__restrict__ sscale,
+    const int *__restrict__ task_brick) {
     __shared__ EvalShared<P> shared[EV_WARPS];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     EvalShared<P> &sh = shared[warp];
@@ -226,13 +256,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         if (lane == 0) task = atomicAdd(task_ctr, 1);
         task = __shfl_sync(FULL_MASK, task, 0);
         if (task >= ntasks) break;
-        int blo = 0, bhi = nbricks;   // toff[blo] - tbase <= task < toff[bhi] - tbase
-        while (bhi - blo > 1) {
-            const int mid = (blo + bhi) >> 1;
-            if (toff[mid] - tbase <= task) blo = mid;
-            else bhi = mid;
-        }
-        const int brick = blo;
+        const int brick = task_brick[task];
         const int part = task - (toff[brick] - tbase);
         const int nparts = toff[brick + 1] - toff[brick];
         const int blk = brick >> 4, q = brick & 15;
@@ -246,18 +270,31 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             cplx L = {0.0, 0.0};
             const int l = lane + 1;
             const double minv = -1.0 / l;
+            // the next cell is loaded while the current one is used
+            TNode nd_n = {};
+            double m_n = 0, ar_n = 0, ai_n = 0;
+            auto fetch = [&](int at) {
+                const int node = lists[at];
+                nd_n = tnode[node];
+                m_n = mass[node];
+                if (lane < P) {
+                    const double *ex = exps + (size_t)node * 2 * P;
+                    ar_n = ex[lane];
+                    ai_n = ex[P + lane];
+                }
+            };
+            if (beg < end) fetch(beg);
             for (int it = beg; it < end; ++it) {
-                const int node = lists[it];
-                const TNode nd = tnode[node];
-                const double m = mass[node];
+                const TNode nd = nd_n;
+                const double m = m_n;
+                const cplx a = {ar_n, ai_n};
+                if (it + 1 < end) fetch(it + 1);
                 const double zx = nd.xcom - b.x0b, zy = nd.ycom - b.y0b;
                 const double r2z0 = zx * zx + zy * zy;
                 const cplx zinv = {zx / r2z0, -zy / r2z0};
                 cplx zl = {0.0, 0.0};
                 if (lane < P) {
-                    zl = cpow_int(zinv, l);   // z0^-l
-                    const double *ex = exps + (size_t)node * 2 * P;
-                    const cplx a = {ex[lane], ex[P + lane]};
+                    zl = cpow_int(zinv, l);        // z0^-l
                     sh.coef[lane] = cmul(a, zl);   // C_l = a_{l-1} z0^-l
                 }
                 __syncwarp();
@@ -296,7 +333,59 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         }
 
         // ---------------- E2P (force-kernels.m4:57-98): w = m/z - sum (j+1) a_j z^-(j+2)
-        if (part == 0) {
+        if (MIXED && part == 0) {
+            // FP32: u = 1/z, u' = R u with R the cell's power-of-two radius, scaled coefficients
+            // D_j = (j+1) a_j / R^(j+1), w = u (m - u' Q(u')), Q(u') = sum_j D_j u'^j
+            const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
+            float hx0 = 0, lx0 = 0, hy0 = 0, ly0 = 0, hx1 = 0, lx1 = 0, hy1 = 0, ly1 = 0;
+            TNode nd_n = {};
+            double m_n = 0;
+            float sc_n = 1.f;
+            float2 c_n = make_float2(0.f, 0.f);
+            auto fetch = [&](int at) {
+                const int node = lists[at];
+                nd_n = tnode[node];
+                m_n = mass[node];
+                sc_n = sscale[node];
+                if (lane < P) c_n = sexp[(size_t)node * P + lane];
+            };
+            if (beg < end) fetch(beg);
+            for (int it = beg; it < end; ++it) {
+                const TNode nd = nd_n;
+                const float m = (float)m_n, R = sc_n;
+                __syncwarp();
+                if (lane < P) sh.coef32[lane] = c_n;
+                __syncwarp();
+                if (it + 1 < end) fetch(it + 1);
+                const float rx = (float)((b.xlo - nd.xcom) + tx * h);
+                const float ry0 = (float)((b.ylo - nd.ycom) + ty * h);
+                const float ry1 = (float)((b.ylo - nd.ycom) + (ty + 4) * h);
+                const float i0 = rcp_approx_f32(rx * rx + ry0 * ry0);
+                const float i1 = rcp_approx_f32(rx * rx + ry1 * ry1);
+                const float2 u0 = make_float2(rx * i0, -ry0 * i0), u1 = make_float2(rx * i1, -ry1 * i1);
+                const float2 v0 = make_float2(R * u0.x, R * u0.y), v1 = make_float2(R * u1.x, R * u1.y);
+                float2 q0 = sh.coef32[P - 1], q1 = q0;
+#pragma unroll
+                for (int j = P - 2; j >= 0; --j) {
+                    const float2 dj = sh.coef32[j];
+                    q0 = make_float2(fmaf(q0.x, v0.x, fmaf(-q0.y, v0.y, dj.x)),
+                                     fmaf(q0.x, v0.y, fmaf(q0.y, v0.x, dj.y)));
+                    q1 = make_float2(fmaf(q1.x, v1.x, fmaf(-q1.y, v1.y, dj.x)),
+                                     fmaf(q1.x, v1.y, fmaf(q1.y, v1.x, dj.y)));
+                }
+                const float t0x = m - (v0.x * q0.x - v0.y * q0.y), t0y = -(v0.x * q0.y + v0.y * q0.x);
+                const float t1x = m - (v1.x * q1.x - v1.y * q1.y), t1y = -(v1.x * q1.y + v1.y * q1.x);
+                two_sum_acc(hx0, lx0, u0.x * t0x - u0.y * t0y);
+                two_sum_acc(hy0, ly0, -(u0.x * t0y + u0.y * t0x));
+                two_sum_acc(hx1, lx1, u1.x * t1x - u1.y * t1y);
+                two_sum_acc(hy1, ly1, -(u1.x * t1y + u1.y * t1x));
+            }
+            ax0 += (double)hx0 + (double)lx0;
+            ay0 += (double)hy0 + (double)ly0;
+            ax1 += (double)hx1 + (double)lx1;
+            ay1 += (double)hy1 + (double)ly1;
+        }
+        if (!MIXED && part == 0) {
             const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
             // the next cell's record and coefficients are loaded while the current one is used
             TNode nd_n = {};
@@ -383,7 +472,56 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
                 py = ys[t0 + lane];
                 pv = vs[t0 + lane];
             }
-            while (tn > 0) {
+            if (MIXED) {
+                // FP32 pairs on offsets from the brick corner; differences of (hi, lo) splits
+                // keep the separation accurate to a few float ulps of itself
+                float txh, txl, ty0h, ty0l, ty1h, ty1l;
+                split_f32(tx * h, txh, txl);
+                split_f32(ty * h, ty0h, ty0l);
+                split_f32((ty + 4) * h, ty1h, ty1l);
+                const float epsf = (float)eps;
+                float hx0 = 0, lx0 = 0, hy0 = 0, ly0 = 0, hx1 = 0, lx1 = 0, hy1 = 0, ly1 = 0;
+                while (tn > 0) {
+                    const int cnt = tn;
+                    __syncwarp();
+                    split_f32(px - b.xlo, sh.sxh[lane], sh.sxl[lane]);
+                    split_f32(py - b.ylo, sh.syh[lane], sh.syl[lane]);
+                    sh.sv32[lane] = (float)pv;
+                    __syncwarp();
+                    next_tile(t0, tn);
+                    if (lane < tn) {
+                        px = xs[t0 + lane];
+                        py = ys[t0 + lane];
+                        pv = vs[t0 + lane];
+                    }
+                    float fx0 = 0, fy0 = 0, fx1 = 0, fy1 = 0;
+#pragma unroll 4
+                    for (int k = 0; k < cnt; ++k) {
+                        const float v = sh.sv32[k];
+                        const float sxh = sh.sxh[k], sxl = sh.sxl[k];
+                        const float syh = sh.syh[k], syl = sh.syl[k];
+                        const float dx = (txh - sxh) + (txl - sxl);
+                        const float dy0 = (ty0h - syh) + (ty0l - syl);
+                        const float dy1 = (ty1h - syh) + (ty1l - syl);
+                        const float dx2e = fmaf(dx, dx, epsf);
+                        const float f0 = v * rcp_approx_f32(fmaf(dy0, dy0, dx2e));
+                        const float f1 = v * rcp_approx_f32(fmaf(dy1, dy1, dx2e));
+                        fx0 = fmaf(dx, f0, fx0);
+                        fy0 = fmaf(dy0, f0, fy0);
+                        fx1 = fmaf(dx, f1, fx1);
+                        fy1 = fmaf(dy1, f1, fy1);
+                    }
+                    two_sum_acc(hx0, lx0, fx0);
+                    two_sum_acc(hy0, ly0, fy0);
+                    two_sum_acc(hx1, lx1, fx1);
+                    two_sum_acc(hy1, ly1, fy1);
+                }
+                ax0 += (double)hx0 + (double)lx0;
+                ay0 += (double)hy0 + (double)ly0;
+                ax1 += (double)hx1 + (double)lx1;
+                ay1 += (double)hy1 + (double)ly1;
+            }
+            while (!MIXED && tn > 0) {
                 const int cnt = tn;
                 __syncwarp();
                 sh.sxy[lane] = make_double2(px, py);
@@ -429,6 +567,36 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             pp[96 + lane] = ay1;
         }
         __syncwarp();
+    }
+}
+
+// task -> brick map of the evaluation tasks
+__global__ void k_task_map(int nbricks, const int *__restrict__ offs, int *__restrict__ task_brick) {
+    const int *toff = offs + 3 * nbricks;
+    const int tbase = toff[0];
+    for (int brick = blockIdx.x * blockDim.x + threadIdx.x; brick < nbricks;
+         brick += gridDim.x * blockDim.x)
+        for (int t = toff[brick]; t < toff[brick + 1]; ++t) task_brick[t - tbase] = brick;
+}
+
+// Mixed form: multipole coefficients scaled by the cell's power-of-two radius R >= r,
+// D_k = f_k a_k / R^(k+1) in FP32 (f_k = k + 1 for the force's derivative series, 1 for the
+// potential), so that they stay O(mass) whatever the cell size; sscale = R.
+template <int P, bool DERIV>
+__global__ void k_scale_coeffs(int nnodes, const TNode *__restrict__ tnode,
+                               const double *__restrict__ exps, float2 *__restrict__ sexp,
+                               float *__restrict__ sscale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)nnodes * P;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int node = (int)(i / P), k = (int)(i % P);
+        const double r = tnode[node].r;
+        int e = 0;
+        if (r > 0 && r < 1e300) frexp(r, &e);   // r = f 2^e with f in [0.5, 1): 2^e >= r
+        const double *ex = exps + (size_t)node * 2 * P;
+        const double f = DERIV ? (double)(k + 1) : 1.0;
+        sexp[i] = make_float2((float)(f * ldexp(ex[k], -e * (k + 1))),
+                              (float)(f * ldexp(ex[P + k], -e * (k + 1))));
+        if (k == 0) sscale[node] = (float)ldexp(1.0, e);
     }
 }
 
@@ -517,24 +685,47 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                                                 slot_ptr<unsigned long long>(c, S_STATS));
     TC_KERNEL_CHECK();
     phase_mark(c, 4);
-    int *brick_ctr;
+    int *brick_ctr, *task_brick;
     double *partial;
     if ((rc = ensure(c, S_BRICK_CTR, 4, &brick_ctr)) ||
-        (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)))
+        (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)) ||
+        (rc = ensure(c, S_TASKMAP, (size_t)ntasks, &task_brick)))
         return rc;
     TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, sizeof(int), c.stream));
-    static int occ = 0;
-    if (!occ) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_force_eval<ORDER_FORCE>,
-                                                      EV_WARPS * 32, 0);
-        if (occ <= 0) occ = 1;
+    k_task_map<<<(int)std::min<long long>((nbricks + 255) / 256, (long long)sm_count() * 8), 256, 0,
+                 c.stream>>>(nbricks, offs, task_brick);
+    TC_KERNEL_CHECK();
+    const bool mixed = c.precision == 1;
+    float2 *sexp = nullptr;
+    float *sscale = nullptr;
+    if (mixed) {
+        if ((rc = ensure(c, S_SEXP, (size_t)c.nnodes * ORDER_FORCE, &sexp)) ||
+            (rc = ensure(c, S_SSCALE, (size_t)c.nnodes, &sscale)))
+            return rc;
+        const long long items = (long long)c.nnodes * ORDER_FORCE;
+        k_scale_coeffs<ORDER_FORCE, true>
+            <<<(int)std::min<long long>((items + 255) / 256, (long long)sm_count() * 8), 256, 0,
+               c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
+        TC_KERNEL_CHECK();
+    }
+    static int occ[2] = {0, 0};
+    if (!occ[mixed]) {
+        if (mixed)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_force_eval<ORDER_FORCE, true>,
+                                                          EV_WARPS * 32, 0);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_force_eval<ORDER_FORCE, false>,
+                                                          EV_WARPS * 32, 0);
+        if (occ[mixed] <= 0) occ[mixed] = 1;
     }
     const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
-                                                (long long)sm_count() * occ);
-    k_force_eval<ORDER_FORCE><<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
+                                                (long long)sm_count() * occ[mixed]);
+    auto eval = mixed ? k_force_eval<ORDER_FORCE, true> : k_force_eval<ORDER_FORCE, false>;
+    eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
         nbricks, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
         slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-        slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr);
+        slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr, sexp, sscale,
+        task_brick);
     TC_KERNEL_CHECK();
     if (ntasks > nbricks) {
         k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8, (long long)sm_count() * 16),

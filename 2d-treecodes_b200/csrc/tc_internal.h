@@ -32,7 +32,7 @@ enum Slot {
     // nodes
     S_TNODE, S_RANGE, S_CELL, S_MASS, S_W, S_WX, S_WY, S_EXPS, S_UPCNT,
     // force traversal / lists
-    S_FCOUNT, S_FOFF, S_E2L, S_E2P, S_P2P, S_BRICK_CTR, S_FPART,
+    S_FCOUNT, S_FOFF, S_E2L, S_E2P, S_P2P, S_BRICK_CTR, S_FPART, S_SEXP, S_SSCALE, S_TASKMAP,
     // potential targets / lists
     S_TKEYS, S_TPERM, S_TKEYS2, S_TPERM2, S_PCOUNT, S_POFF, S_PE2P, S_PP2P,
     // misc

@@ -53,6 +53,7 @@ def parse_args():
     p.add_argument("--accuracy-targets", type=int, default=4096)
     p.add_argument("--single", action="store_true",
                    help="only `warmup` + `steps` device solves and a timing line (for profilers)")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     return p.parse_args()
 
 
@@ -258,7 +259,7 @@ def run_b200(args, ws, rank, local):
     dev = torch.device("cuda", local)
     w = make_workload(args.workload, seed_offset=rank)
     kind = w["kind"]
-    ctx = T.Context(device=local)
+    ctx = T.Context(device=local, precision=1 if args.precision == "mixed" else 0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     d = {k: torch.as_tensor(w[k]).to(dev) for k in w if isinstance(w[k], np.ndarray)}
     m = n_targets(w)
