@@ -159,10 +159,6 @@ static int potential_device(Context &c, double theta, const double *xs, const do
         TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
         return TC_OK;
     }
-    if (c.precision != 0) {
-        set_error(TC_ERR_INVALID, "precision mode %d is not available for the potential", c.precision);
-        return TC_ERR_INVALID;
-    }
     int rc;
     phase_mark(c, 0);
     if ((rc = build_tree(c, 0, xs, ys, vs, n))) return rc;

@@ -21,6 +21,9 @@ namespace tc {
 
 constexpr int PT_WARPS = 4;
 constexpr int PT_STACK = 64;   // depth-first, one entry popped per step: <= 3 * LMAX + 4 live entries
+// A group's evaluation is split into tasks of at most PT_SEG near-field sources (task 0 also
+// does the far field), so that groups inside dense clusters do not serialise the kernel.
+constexpr int PT_SEG = 4096;
 
 template <bool FILL>
 __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
@@ -51,7 +54,7 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             o1 = offs[ngroups + g];
             l1 = offs[ngroups + g + 1];
         }
-        int n0 = 0, n1 = 0;
+        int n0 = 0, n1 = 0, gsrc = 0;
         int top = 0;
         if (lane == 0) stack[0] = make_int2(0, (int)vmask);
         top = 1;
@@ -84,6 +87,7 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
                 if (nd.child < 0) {
                     if (nd.count > 0) {
                         p2p_pairs += (unsigned long long)__popc(rest) * (unsigned)nd.count;
+                        gsrc += nd.count;
                         if (FILL && lane == 0) {
                             if (o1 + n1 < l1) lists[o1 + n1] = make_int2(ent.x, (int)rest);
                             else atomicOr(err, DEVERR_BOUNDS);
@@ -108,6 +112,8 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
         if (!FILL && lane == 0) {
             counts[g] = n0;
             counts[ngroups + g] = n1;
+            // evaluation tasks: the group's near-field sources in segments of at most PT_SEG
+            counts[2 * ngroups + g] = max(1, (gsrc + PT_SEG - 1) / PT_SEG);
         }
         __syncwarp();
     }
@@ -120,21 +126,65 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
 constexpr int PE_WARPS = 4;
 constexpr int PE_CHUNK = 32;
 
-template <int P>
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ void two_sum_add(float &hi, float &lo, float x) {
+    const float s = hi + x;
+    const float bb = s - hi;
+    lo += (hi - (s - bb)) + (x - bb);
+    hi = s;
+}
+
+__device__ __forceinline__ void split2(double v, float &hi, float &lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+}
+
+// Tasks: group g owns tasks [toff[g], toff[g+1]); task 0 evaluates the far field and the first
+// PT_SEG near-field sources of the group, task p > 0 the p-th segment.
+// MIXED = false: FP64 throughout (log of FP64).  MIXED = true: the series of E2P and the P2P
+// logs in FP32 (offsets from the group's first target split hi + lo, lg2.approx, compensated
+// sums); the monopole term m log|z| of E2P stays FP64.
+template <int P, bool MIXED>
 __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
     int ngroups, int m, const double *__restrict__ xt, const double *__restrict__ yt,
     const int *__restrict__ tperm, const TNode *__restrict__ tnode,
     const double *__restrict__ mass, const double *__restrict__ exps,
     const int2 *__restrict__ range, const double *__restrict__ xs,
     const double *__restrict__ ys, const double *__restrict__ vs,
-    const int *__restrict__ offs, const int2 *__restrict__ lists, double *__restrict__ out) {
+    const int *__restrict__ offs, const int2 *__restrict__ lists, double *__restrict__ out,
+    double *__restrict__ partial, int *task_ctr, const int *__restrict__ task_group,
+    const float2 *__restrict__ sexp, const float *__restrict__ sscale) {
     __shared__ cplx s_coef[PE_WARPS][P];
+    __shared__ float2 s_coef32[PE_WARPS][P];
     __shared__ double2 s_xy[PE_WARPS][PE_CHUNK];
     __shared__ double s_v[PE_WARPS][PE_CHUNK];
+    __shared__ float4 s_off[PE_WARPS][PE_CHUNK];   // (x hi, x lo, y hi, y lo) from the reference
+    __shared__ float s_v32[PE_WARPS][PE_CHUNK];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     const double eps = 10 * DBL_EPSILON;
+    const int *toff = offs + 2 * ngroups;
+    const int tbase = toff[0];
+    const int ntasks = toff[ngroups] - tbase;
 
-    for (int g = blockIdx.x * PE_WARPS + warp; g < ngroups; g += gridDim.x * PE_WARPS) {
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = atomicAdd(task_ctr, 1);
+        task = __shfl_sync(FULL_MASK, task, 0);
+        if (task >= ntasks) break;
+        const int g = task_group[task];
+        const int part = task - (toff[g] - tbase);
+        const int nparts = toff[g + 1] - toff[g];
         const int t = g * 32 + lane;
         const bool valid = t < m;
         int j = 0;
@@ -144,57 +194,173 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
             x = xt[j];
             y = yt[j];
         }
+        // reference point of the mixed form's offsets: the group's first target
+        const double xref = __shfl_sync(FULL_MASK, x, 0), yref = __shfl_sync(FULL_MASK, y, 0);
         double far = 0, near = 0;
 
         // E2P (potential-kernels.m4:59-89): m log(r2)/2 + Re sum_{j=1..p} a_{j-1} z^-j
-        const int b0 = offs[g], e0 = offs[g + 1];
-        for (int it = b0; it < e0; ++it) {
-            const int2 ent = lists[it];
-            const TNode nd = tnode[ent.x];
-            const double mm = mass[ent.x];
-            __syncwarp();
-            if (lane < P) {
-                const double *ex = exps + (size_t)ent.x * 2 * P;
-                s_coef[warp][lane] = {ex[lane], ex[P + lane]};
-            }
-            __syncwarp();
-            if ((ent.y >> lane) & 1) {
-                const double rz = x - nd.xcom, iz = y - nd.ycom;
-                const double r2 = rz * rz + iz * iz;
-                const double inv = 1.0 / r2;
-                const cplx u = {rz * inv, -iz * inv};
-                cplx q = s_coef[warp][P - 1];
-#pragma unroll
-                for (int k = P - 2; k >= 0; --k) q = cfma(q, u, s_coef[warp][k]);
-                far += mm * log(r2) * 0.5 + (u.re * q.re - u.im * q.im);
-            }
-        }
-
-        // P2P (potential-kernels.m4:19-57): 0.5 sum v log(r2 + eps)
-        const int b1 = offs[ngroups + g], e1 = offs[ngroups + g + 1];
-        for (int it = b1; it < e1; ++it) {
-            const int2 ent = lists[it];
-            const int2 rg = range[ent.x];
-            const bool mine = (ent.y >> lane) & 1;
-            for (int s0 = rg.x; s0 < rg.y; s0 += PE_CHUNK) {
-                const int cnt = min(PE_CHUNK, rg.y - s0);
+        if (part == 0) {
+            const int b0 = offs[g], e0 = offs[g + 1];
+            float sh = 0, sl = 0;
+            for (int it = b0; it < e0; ++it) {
+                const int2 ent = lists[it];
+                const TNode nd = tnode[ent.x];
+                const double mm = mass[ent.x];
                 __syncwarp();
-                if (lane < cnt) {
-                    s_xy[warp][lane] = make_double2(xs[s0 + lane], ys[s0 + lane]);
-                    s_v[warp][lane] = vs[s0 + lane];
+                if (lane < P) {
+                    if (MIXED) {
+                        s_coef32[warp][lane] = sexp[(size_t)ent.x * P + lane];
+                    } else {
+                        const double *ex = exps + (size_t)ent.x * 2 * P;
+                        s_coef[warp][lane] = {ex[lane], ex[P + lane]};
+                    }
                 }
                 __syncwarp();
-                if (mine) {
-                    for (int k = 0; k < cnt; ++k) {
-                        const double2 sp = s_xy[warp][k];
-                        const double xr = x - sp.x, yr = y - sp.y;
-                        near += log(xr * xr + yr * yr + eps) * s_v[warp][k];
+                if ((ent.y >> lane) & 1) {
+                    const double rz = x - nd.xcom, iz = y - nd.ycom;
+                    const double r2 = rz * rz + iz * iz;
+                    if (MIXED) {
+                        // series: Re(u' Q(u')), u' = R / z, Q(u') = sum_j D_j u'^j
+                        const float R = sscale[ent.x];
+                        const float zr = (float)rz, zi = (float)iz;
+                        const float inv = rcp_approx(zr * zr + zi * zi);
+                        const float ur = R * zr * inv, ui = -R * zi * inv;
+                        float2 q = s_coef32[warp][P - 1];
+#pragma unroll
+                        for (int k = P - 2; k >= 0; --k) {
+                            const float2 d = s_coef32[warp][k];
+                            q = make_float2(fmaf(q.x, ur, fmaf(-q.y, ui, d.x)),
+                                            fmaf(q.x, ui, fmaf(q.y, ur, d.y)));
+                        }
+                        two_sum_add(sh, sl, ur * q.x - ui * q.y);
+                        far += mm * log(r2) * 0.5;
+                    } else {
+                        const double inv = 1.0 / r2;
+                        const cplx u = {rz * inv, -iz * inv};
+                        cplx q = s_coef[warp][P - 1];
+#pragma unroll
+                        for (int k = P - 2; k >= 0; --k) q = cfma(q, u, s_coef[warp][k]);
+                        far += mm * log(r2) * 0.5 + (u.re * q.re - u.im * q.im);
                     }
                 }
             }
+            if (MIXED) far += (double)sh + (double)sl;
         }
-        if (valid) out[j] = 0.5 * near + far;
+
+        // P2P (potential-kernels.m4:19-57): 0.5 sum v log(r2 + eps), sources
+        // [part * PT_SEG, (part + 1) * PT_SEG) of the group's listed leaves
+        {
+            const int b1 = offs[ngroups + g], e1 = offs[ngroups + g + 1];
+            int skip = part * PT_SEG, budget = PT_SEG;
+            float nh = 0, nl = 0, txh = 0, txl = 0, tyh = 0, tyl = 0;
+            if (MIXED) {
+                split2(x - xref, txh, txl);
+                split2(y - yref, tyh, tyl);
+            }
+            const float ln2 = 0.6931471805599453f, epsf = (float)eps;
+            for (int it = b1; it < e1 && budget > 0; ++it) {
+                const int2 ent = lists[it];
+                const int2 rg = range[ent.x];
+                const int cnt_leaf = rg.y - rg.x;
+                if (skip >= cnt_leaf) {
+                    skip -= cnt_leaf;
+                    continue;
+                }
+                const int sbeg = rg.x + skip;
+                const int send = min(rg.y, sbeg + budget);
+                budget -= send - sbeg;
+                skip = 0;
+                const bool mine = (ent.y >> lane) & 1;
+                for (int s0 = sbeg; s0 < send; s0 += PE_CHUNK) {
+                    const int cnt = min(PE_CHUNK, send - s0);
+                    __syncwarp();
+                    if (lane < cnt) {
+                        if (MIXED) {
+                            float a, b2, c2, d2;
+                            split2(xs[s0 + lane] - xref, a, b2);
+                            split2(ys[s0 + lane] - yref, c2, d2);
+                            s_off[warp][lane] = make_float4(a, b2, c2, d2);
+                            s_v32[warp][lane] = (float)vs[s0 + lane];
+                        } else {
+                            s_xy[warp][lane] = make_double2(xs[s0 + lane], ys[s0 + lane]);
+                            s_v[warp][lane] = vs[s0 + lane];
+                        }
+                    }
+                    __syncwarp();
+                    if (mine) {
+                        if (MIXED) {
+                            float acc = 0;
+#pragma unroll 4
+                            for (int k = 0; k < cnt; ++k) {
+                                const float4 o = s_off[warp][k];
+                                const float dx = (txh - o.x) + (txl - o.y);
+                                const float dy = (tyh - o.z) + (tyl - o.w);
+                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), s_v32[warp][k], acc);
+                            }
+                            two_sum_add(nh, nl, acc * ln2);
+                        } else {
+                            for (int k = 0; k < cnt; ++k) {
+                                const double2 sp = s_xy[warp][k];
+                                const double xr = x - sp.x, yr = y - sp.y;
+                                near += log(xr * xr + yr * yr + eps) * s_v[warp][k];
+                            }
+                        }
+                    }
+                }
+            }
+            if (MIXED) near = (double)nh + (double)nl;
+        }
+        const double res = 0.5 * near + far;
+        if (nparts == 1) {
+            if (valid) out[j] = res;
+        } else {
+            partial[(size_t)task * 32 + lane] = res;
+        }
         __syncwarp();
+    }
+}
+
+__global__ void k_task_map_groups(int ngroups, const int *__restrict__ offs,
+                                  int *__restrict__ task_group) {
+    const int *toff = offs + 2 * ngroups;
+    const int tbase = toff[0];
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x)
+        for (int t = toff[g]; t < toff[g + 1]; ++t) task_group[t - tbase] = g;
+}
+
+// Sum of the parts of every multi-task group, in task order (deterministic).
+__global__ void k_potential_gather_parts(int ngroups, int m, const int *__restrict__ tperm,
+                                         const int *__restrict__ offs,
+                                         const double *__restrict__ partial,
+                                         double *__restrict__ out) {
+    const int lane = lane_id();
+    const int *toff = offs + 2 * ngroups;
+    const int tbase = toff[0];
+    for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups;
+         g += (gridDim.x * blockDim.x) >> 5) {
+        const int t0 = toff[g] - tbase, np = toff[g + 1] - toff[g];
+        if (np <= 1) continue;
+        double s = 0;
+        for (int p = 0; p < np; ++p) s += partial[(size_t)(t0 + p) * 32 + lane];
+        const int t = g * 32 + lane;
+        if (t < m) out[tperm[t]] = s;
+    }
+}
+
+// Mixed form: a_k / R^(k+1) in FP32, R = the cell's power-of-two radius (see force.cu).
+template <int P>
+__global__ void k_scale_coeffs_pot(int nnodes, const TNode *__restrict__ tnode,
+                                   const double *__restrict__ exps, float2 *__restrict__ sexp,
+                                   float *__restrict__ sscale) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)nnodes * P;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int node = (int)(i / P), k = (int)(i % P);
+        const double r = tnode[node].r;
+        int e = 0;
+        if (r > 0 && r < 1e300) frexp(r, &e);
+        const double *ex = exps + (size_t)node * 2 * P;
+        sexp[i] = make_float2((float)ldexp(ex[k], -e * (k + 1)), (float)ldexp(ex[P + k], -e * (k + 1)));
+        if (k == 0) sscale[node] = (float)ldexp(1.0, e);
     }
 }
 
@@ -225,9 +391,10 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     if ((rc = radix_sort_pairs(c, tkeys, nullptr, m, 2 * LMAX, tkeys2, tperm2, tkeys, tperm, &ko, &vo)))
         return rc;
     const int ngroups = (m + 31) / 32;
+    // counts / offsets: E2P | P2P list lengths and evaluation tasks, ngroups each
     int *counts, *offs;
-    if ((rc = ensure(c, S_PCOUNT, (size_t)2 * ngroups, &counts)) ||
-        (rc = ensure(c, S_POFF, (size_t)2 * ngroups + 1, &offs)))
+    if ((rc = ensure(c, S_PCOUNT, (size_t)3 * ngroups, &counts)) ||
+        (rc = ensure(c, S_POFF, (size_t)3 * ngroups + 1, &offs)))
         return rc;
     const TNode *tnode = slot_ptr<TNode>(c, S_TNODE);
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
@@ -237,11 +404,13 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
                                                                   tnode, c.nnodes, counts, nullptr, nullptr,
                                                                   err, nullptr);
     TC_KERNEL_CHECK();
-    if ((rc = exclusive_scan(c, counts, offs, 2 * ngroups))) return rc;
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, offs + ngroups, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 1, offs + 2 * ngroups, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    if ((rc = exclusive_scan(c, counts, offs, 3 * ngroups))) return rc;
+    for (int k = 0; k < 3; ++k)
+        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + k, offs + (k + 1) * ngroups, sizeof(int),
+                                    cudaMemcpyDeviceToHost, c.stream));
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
     const int n_e2p = (int)c.h_pinned[0], total = (int)c.h_pinned[1];
+    const int ntasks = (int)c.h_pinned[2] - total;
     c.counts.n_e2p = n_e2p;
     c.counts.n_p2p = total - n_e2p;
     c.counts.n_e2l = 0;
@@ -254,13 +423,47 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
                                                                  slot_ptr<unsigned long long>(c, S_STATS));
     TC_KERNEL_CHECK();
     phase_mark(c, 4);
-    const int egrid = (int)std::min<long long>((ngroups + PE_WARPS - 1) / PE_WARPS,
-                                               (long long)sm_count_p() * 8);
-    k_potential_eval<ORDER_POTENTIAL><<<egrid, PE_WARPS * 32, 0, c.stream>>>(
+    int *task_ctr, *task_group;
+    double *partial;
+    if ((rc = ensure(c, S_BRICK_CTR, 4, &task_ctr)) ||
+        (rc = ensure(c, S_TASKMAP, (size_t)ntasks, &task_group)) ||
+        (rc = ensure(c, S_FPART, (size_t)ntasks * 32, &partial)))
+        return rc;
+    TC_CUDA_TRY(cudaMemsetAsync(task_ctr, 0, sizeof(int), c.stream));
+    k_task_map_groups<<<(int)std::min<long long>((ngroups + 255) / 256, (long long)sm_count_p() * 8),
+                        256, 0, c.stream>>>(ngroups, offs, task_group);
+    TC_KERNEL_CHECK();
+    const bool mixed = c.precision == 1;
+    float2 *sexp = nullptr;
+    float *sscale = nullptr;
+    if (mixed) {
+        if ((rc = ensure(c, S_SEXP, (size_t)c.nnodes * ORDER_POTENTIAL, &sexp)) ||
+            (rc = ensure(c, S_SSCALE, (size_t)c.nnodes, &sscale)))
+            return rc;
+        const long long items = (long long)c.nnodes * ORDER_POTENTIAL;
+        k_scale_coeffs_pot<ORDER_POTENTIAL>
+            <<<(int)std::min<long long>((items + 255) / 256, (long long)sm_count_p() * 8), 256, 0,
+               c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
+        TC_KERNEL_CHECK();
+    }
+    static int occ[2] = {0, 0};
+    auto eval = mixed ? k_potential_eval<ORDER_POTENTIAL, true> : k_potential_eval<ORDER_POTENTIAL, false>;
+    if (!occ[mixed]) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[mixed], eval, PE_WARPS * 32, 0);
+        if (occ[mixed] <= 0) occ[mixed] = 1;
+    }
+    const int egrid = (int)std::min<long long>((ntasks + PE_WARPS - 1) / PE_WARPS,
+                                               (long long)sm_count_p() * occ[mixed]);
+    eval<<<egrid, PE_WARPS * 32, 0, c.stream>>>(
         ngroups, m, xt, yt, vo, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
         slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-        slot_ptr<double>(c, S_VS), offs, lists, out);
+        slot_ptr<double>(c, S_VS), offs, lists, out, partial, task_ctr, task_group, sexp, sscale);
     TC_KERNEL_CHECK();
+    if (ntasks > ngroups) {
+        k_potential_gather_parts<<<(int)std::min<long long>((ngroups + 7) / 8, (long long)sm_count_p() * 16),
+                                   256, 0, c.stream>>>(ngroups, m, vo, offs, partial, out);
+        TC_KERNEL_CHECK();
+    }
     return TC_OK;
 }
 
