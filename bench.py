@@ -1,17 +1,21 @@
 #!/usr/bin/env python
 """Benchmark of the B200 treecode: one JSON line on stdout (rank 0).
 
-A step is one treecode_force_mrag solve (sort, tree, upward pass, interaction lists,
-far + near field) of the vortex-sheet workload: 16,777,216 sources on a perturbed sheet,
-4096 MRAG blocks of 32 x 32 targets (4,194,304 targets), theta = 0.5, plain FP64.
+A step is one force_mrag solve (sort, tree, upward pass, interaction lists, far + near field)
+of the vortex-sheet workload: 16,777,216 sources on a perturbed sheet, 4096 MRAG blocks of
+32 x 32 targets (4,194,304 targets), theta = 0.5, in the mixed-precision form (default) or the
+plain FP64 form (--precision fp64).  With the mixed form the line also carries the plain FP64
+form measured on the same inputs (`plain_fp64`), so the mixed-vs-FP64 ratio is in one run.
 
   value     whole-job throughput (Mtargets/s) with inputs resident in HBM, CUDA events on the
             library's stream, max over ranks
-  e2e       the same metric through the reference-compatible C entry point treecode_force_mrag
-            with pinned host buffers (host->device copies and the result read-back timed)
-  roofline  the dominant kernel (k_force_eval): algorithmic FP64 flops per launch / its event
-            time, against the measured FP64 FMA throughput of this GPU; DRAM traffic per launch
-            from the committed ncu capture
+  accuracy  relative L2 / max error against the FP64 direct sum on a strided target sample
+  e2e       the same metric through the C ABI with pinned host buffers (host->device copies and
+            the result read-back timed): tc_force_mrag_host at the run's precision, and the
+            reference-compatible treecode_force_mrag (FP64) beside it
+  roofline  the evaluation kernel (k_force_eval): algorithmic flops per launch / its event time,
+            against the measured FMA throughput of this GPU (FP64, or FP32 for the mixed form);
+            DRAM traffic per launch from the committed ncu capture
   cpu_baseline  the reference's drivers (oracle/_ref) on the host cores, bounded sample
 
 --impl reference times the reference's own CPU implementation instead (rank 0 only).
@@ -21,11 +25,14 @@ scaling, seeds differ by rank); only the timing barrier/max-reduction is collect
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -53,7 +60,7 @@ def parse_args():
     p.add_argument("--accuracy-targets", type=int, default=4096)
     p.add_argument("--single", action="store_true",
                    help="only `warmup` + `steps` device solves and a timing line (for profilers)")
-    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     return p.parse_args()
 
 
@@ -177,7 +184,7 @@ def read_profile_traffic():
 
 
 # ------------------------------------------------------------------------------- CPU reference
-def cpu_reference_step(w, sample_blocks=128, threads=None):
+def cpu_reference_step(w, sample_blocks=512, threads=None):
     """One bounded step of the reference's CPU implementation (oracle/_ref: the reference's
     drivers compiled verbatim + the restated ISPC kernels, node capacity raised for large
     inputs): the full tree build plus the evaluation of `sample_blocks` evenly strided blocks,
@@ -188,28 +195,36 @@ def cpu_reference_step(w, sample_blocks=128, threads=None):
     nb = len(w["x0s"])
     stride = max(1, nb // sample_blocks)
     idx = np.arange(0, nb, stride)[:sample_blocks]
-    devnull = os.open(os.devnull, os.O_WRONLY)
+    libc = ctypes.CDLL(None)
+    log = tempfile.TemporaryFile(mode="w+b")
     saved = os.dup(1)
     try:
         sys.stdout.flush()
-        os.dup2(devnull, 1)   # the reference's force driver prints per-thread timers
+        os.dup2(log.fileno(), 1)   # the reference's force driver prints its own phase timers
         t0 = time.perf_counter()
-        O.force_mrag(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"][:0], w["y0s"][:0],
-                     w["hs"][:0], mode="big")
-        t1 = time.perf_counter()
         O.force_mrag(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"][idx], w["y0s"][idx],
                      w["hs"][idx], mode="big")
-        t2 = time.perf_counter()
+        t1 = time.perf_counter()
+        libc.fflush(None)
     finally:
         os.dup2(saved, 1)
         os.close(saved)
-        os.close(devnull)
-    build = t1 - t0
-    evals = max(t2 - t1 - build, 0.0)
+    log.seek(0)
+    text = log.read().decode(errors="replace")
+    log.close()
+    # drivers/treecode-force.cpp:234 prints "UP: <s>s DW: <s>s" (tree build + upward pass,
+    # then the evaluation of the requested blocks)
+    m = re.findall(r"UP:\s*([0-9.eE+-]+)s\s+DW:\s*([0-9.eE+-]+)s", text)
+    if not m:
+        raise RuntimeError("the reference driver printed no UP/DW timers")
+    evals = float(m[-1][1])
+    wall = t1 - t0
+    build = wall - evals
     full = build + evals * nb / len(idx)
-    desc = (f"full tree build ({len(w['xs'])} sources) + evaluation of {len(idx)} of {nb} "
-            f"blocks (every {stride}th), evaluation time scaled by {nb}/{len(idx)}; "
-            f"build {build:.2f} s, sampled evaluation {evals:.2f} s")
+    desc = (f"tree build + upward pass of all {len(w['xs'])} sources, evaluation of {len(idx)} "
+            f"of {nb} blocks (every {stride}th) scaled by {nb}/{len(idx)}; the evaluation time "
+            f"is the reference driver's own DW timer ({evals:.3f} s), the rest is wall time "
+            f"({build:.2f} s)")
     return full, desc
 
 
@@ -250,6 +265,7 @@ def run_reference(args, ws, rank):
 
 # ------------------------------------------------------------------------------- GPU arm
 def run_b200(args, ws, rank, local):
+    import ctypes
     import torch
     import treecodes as T
 
@@ -259,7 +275,8 @@ def run_b200(args, ws, rank, local):
     dev = torch.device("cuda", local)
     w = make_workload(args.workload, seed_offset=rank)
     kind = w["kind"]
-    ctx = T.Context(device=local, precision=1 if args.precision == "mixed" else 0)
+    mixed = args.precision == "mixed"
+    ctx = T.Context(device=local, precision=1 if mixed else 0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     d = {k: torch.as_tensor(w[k]).to(dev) for k in w if isinstance(w[k], np.ndarray)}
     m = n_targets(w)
@@ -280,87 +297,123 @@ def run_b200(args, ws, rank, local):
         for _ in range(args.steps):
             solve()
         torch.cuda.synchronize()
-        print(json.dumps({"single": w["name"], "ms_per_step": (time.perf_counter() - t0) * 1e3
-                          / max(args.steps, 1), "stats": ctx.stats()}))
+        print(json.dumps({"single": w["name"], "precision": args.precision,
+                          "ms_per_step": (time.perf_counter() - t0) * 1e3 / max(args.steps, 1),
+                          "stats": ctx.stats()}))
         ctx.close()
         return 0
 
-    # ---- device-resident throughput (value)
-    for _ in range(max(args.warmup, 3)):
-        solve()
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
-    barrier(ws)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    launches = 0
-    for _ in range(args.steps):
-        solve()
-        launches += ctx.stats()["launches"]
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier(ws)
-    clocks = sampler.stop()
-    ms_local = e0.elapsed_time(e1) / args.steps
-    ms = max_over_ranks(ms_local, ws, dev)
-    value = ws * m / (ms * 1e-3) / 1e6
+    def timed(precision, steps, sample_clocks=False):
+        """Device time per step of `steps` solves (CUDA events on the library's stream, max over
+        ranks), after warm-up; returns (ms, kernel launches, clock record)."""
+        ctx.set_precision(precision)
+        for _ in range(max(args.warmup, 3)):
+            solve()
+        torch.cuda.synchronize()
+        sampler = None
+        if sample_clocks:
+            sampler = ClockSampler(local)
+            sampler.start()
+            time.sleep(0.3)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launches = 0
+        for _ in range(steps):
+            solve()
+            launches += ctx.stats()["launches"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        clocks = sampler.stop() if sampler else None
+        return max_over_ranks(e0.elapsed_time(e1) / steps, ws, dev), launches, clocks
 
-    # ---- dominant kernel: evaluation launch timed with events on the library's stream
-    ctx.set_timing(True)
-    ev_ms = []
-    for _ in range(3):
-        solve()
-        ev_ms.append(ctx.stats()["eval_ms"])
-    st = ctx.stats()
-    ctx.set_timing(False)
-    eval_ms = statistics.median(ev_ms)
-    flops = algorithmic_flops(st) if kind == "force" else None
-    fp64_peak = T.measure_fma_peak(True)
-    roofline = None
-    if flops is not None:
-        achieved = flops / (eval_ms * 1e-3) / 1e12
-        roofline = {"kernel": "k_force_eval", "bound": "fp64", "achieved": achieved,
-                    "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
-                    "traffic": read_profile_traffic(),
-                    "peak_source": "measured FP64 FMA throughput of this GPU (tc_measure_fma_peak)",
-                    "algorithmic_flops_per_launch": flops, "launch_ms": eval_ms,
-                    "phase_ms": {k: st[k] for k in ("sort_ms", "tree_ms", "upward_ms",
-                                                     "lists_ms", "eval_ms", "total_ms")}}
+    def phases(precision):
+        """Phase times of one solve (events inside the library) and its work counters."""
+        ctx.set_precision(precision)
+        ctx.set_timing(True)
+        runs = []
+        for _ in range(3):
+            solve()
+            runs.append(ctx.stats())
+        ctx.set_timing(False)
+        st = dict(runs[-1])
+        for k in ("sort_ms", "tree_ms", "upward_ms", "lists_ms", "eval_ms", "total_ms"):
+            st[k] = statistics.median(r[k] for r in runs)
+        return st
 
-    # ---- accuracy vs the FP64 direct sum on a strided target subsample (GPU direct sum)
-    acc = None
-    if kind == "force":
+    def accuracy(precision):
+        """Relative L2 / max error against the FP64 direct sum on a strided target sample."""
+        ctx.set_precision(precision)
         solve()
         torch.cuda.synchronize()
         step = max(1, m // args.accuracy_targets)
         idx = torch.arange(7, m, step, device=dev)[: args.accuracy_targets]
-        ib, rem = idx // 1024, idx % 1024
-        iy, ix = rem // 32, rem % 32
-        xt = d["x0s"][ib] + ix.double() * d["hs"][ib]
-        yt = d["y0s"][ib] + iy.double() * d["hs"][ib]
-        rx = torch.empty(len(idx), dtype=torch.float64, device=dev)
-        ry = torch.empty_like(rx)
-        ctx.direct_force_device(d["xs"], d["ys"], d["vs"], xt, yt, rx, ry)
-        gx, gy = out[0][idx], out[1][idx]
-        num = torch.sqrt(((gx - rx) ** 2 + (gy - ry) ** 2).sum())
-        den = torch.sqrt((rx ** 2 + ry ** 2).sum())
-        acc = {"rel_l2_vs_fp64_direct": float(num / den),
-               "max_abs_err": float(torch.maximum((gx - rx).abs(), (gy - ry).abs()).max()),
-               "targets_sampled": int(len(idx))}
+        if kind == "force":
+            ib, rem = idx // 1024, idx % 1024
+            xt = d["x0s"][ib] + (rem % 32).double() * d["hs"][ib]
+            yt = d["y0s"][ib] + (rem // 32).double() * d["hs"][ib]
+            rx = torch.empty(len(idx), dtype=torch.float64, device=dev)
+            ry = torch.empty_like(rx)
+            ctx.direct_force_device(d["xs"], d["ys"], d["vs"], xt, yt, rx, ry)
+            got, ref = torch.cat([out[0][idx], out[1][idx]]), torch.cat([rx, ry])
+        else:
+            ref = torch.empty(len(idx), dtype=torch.float64, device=dev)
+            ctx.direct_potential_device(d["xs"], d["ys"], d["vs"], d["xt"][idx], d["yt"][idx], ref)
+            got = out[0][idx]
+        return {"rel_l2_vs_fp64_direct": float((got - ref).norm() / ref.norm()),
+                "max_abs_err": float((got - ref).abs().max()), "targets_sampled": int(len(idx))}
 
-    # ---- end to end through the reference-compatible C entry point, pinned host buffers
+    prec = 1 if mixed else 0
+    ms, launches, clocks = timed(prec, args.steps, sample_clocks=True)
+    value = ws * m / (ms * 1e-3) / 1e6
+    st = phases(prec)
+    acc = accuracy(prec)
+    other = None
+    if mixed:   # the plain FP64 form on the same inputs, for the mixed-vs-FP64 ratio
+        ms64, _, _ = timed(0, args.steps)
+        other = {"precision": "fp64", "value": ws * m / (ms64 * 1e-3) / 1e6, "unit": "Mtargets/s",
+                 "ms_per_step": ms64, "accuracy": accuracy(0),
+                 "phase_ms": {k: v for k, v in phases(0).items() if k.endswith("_ms")}}
+    ctx.set_precision(prec)
+
+    # ---- dominant kernel: the evaluation launch, timed by events on the library's stream
+    roofline = None
+    if kind == "force":
+        flops = algorithmic_flops(st)
+        peak = T.measure_fma_peak(not mixed)
+        achieved = flops / (st["eval_ms"] * 1e-3) / 1e12
+        roofline = {"kernel": "k_force_eval", "bound": "fp32" if mixed else "fp64",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": read_profile_traffic() if not mixed else None,
+                    "peak_source": ("measured %s FMA throughput of this GPU (tc_measure_fma_peak)"
+                                    % ("FP32" if mixed else "FP64")),
+                    "algorithmic_flops_per_launch": flops, "launch_ms": st["eval_ms"],
+                    "phase_ms": {k: st[k] for k in ("sort_ms", "tree_ms", "upward_ms", "lists_ms",
+                                                     "eval_ms", "total_ms")}}
+
+    # ---- end to end through the C ABI with pinned host buffers (host -> device copies and the
+    # read-back of the results inside the timed region)
     lib = T.load()
-    import ctypes
-    pin = {k: torch.as_tensor(w[k]).pin_memory() for k in ("xs", "ys", "vs", "x0s", "y0s", "hs")} \
-        if kind == "force" else {k: torch.as_tensor(w[k]).pin_memory() for k in ("xs", "ys", "vs", "xt", "yt")}
+    keys = ("xs", "ys", "vs", "x0s", "y0s", "hs") if kind == "force" else ("xs", "ys", "vs", "xt", "yt")
+    pin = {k: torch.as_tensor(w[k]).pin_memory() for k in keys}
     hout = [torch.empty(m, dtype=torch.float64).pin_memory() for _ in out]
     P = lambda t: ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))  # noqa: E731
     n = len(w["xs"])
 
-    def solve_host():
+    def solve_host_ctx():   # tc_force_mrag_host / tc_potential_host: the context's precision
+        if kind == "force":
+            rc = lib.tc_force_mrag_host(ctx.h, w["theta"], P(pin["xs"]), P(pin["ys"]), P(pin["vs"]), n,
+                                        P(pin["x0s"]), P(pin["y0s"]), P(pin["hs"]), len(w["x0s"]),
+                                        P(hout[0]), P(hout[1]))
+        else:
+            rc = lib.tc_potential_host(ctx.h, w["theta"], P(pin["xs"]), P(pin["ys"]), P(pin["vs"]), n,
+                                       P(pin["xt"]), P(pin["yt"]), m, P(hout[0]))
+        if rc != 0:
+            raise RuntimeError(lib.treecode_last_error().decode())
+
+    def solve_host_ref():   # the reference-compatible entry points (plain FP64)
         if kind == "force":
             lib.treecode_force_mrag(w["theta"], P(pin["xs"]), P(pin["ys"]), P(pin["vs"]), n,
                                     P(pin["x0s"]), P(pin["y0s"]), P(pin["hs"]), len(w["x0s"]),
@@ -371,20 +424,28 @@ def run_b200(args, ws, rank, local):
         if lib.treecode_last_status() != 0:
             raise RuntimeError(lib.treecode_last_error().decode())
 
-    for _ in range(max(args.warmup, 3)):
-        solve_host()
-    barrier(ws)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        solve_host()
-    t1 = time.perf_counter()
-    e2e_ms = max_over_ranks((t1 - t0) / args.steps * 1e3, ws, dev)
+    def wall(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fn()
+        t1 = time.perf_counter()
+        return max_over_ranks((t1 - t0) / args.steps * 1e3, ws, dev)
+
     h2d = sum(t.numel() * 8 for t in pin.values())
     d2h = sum(t.numel() * 8 for t in hout)
+    e2e_ms = wall(solve_host_ctx)
+    e2e_ref_ms = wall(solve_host_ref)
     e2e = {"value": ws * m / (e2e_ms * 1e-3) / 1e6, "unit": "Mtargets/s", "ms_per_step": e2e_ms,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "api": "treecode_force_mrag (C ABI, host pointers)" if kind == "force"
-           else "treecode_potential (C ABI, host pointers)"}
+           "api": ("tc_force_mrag_host" if kind == "force" else "tc_potential_host")
+           + " (C ABI, host pointers, %s)" % args.precision,
+           "reference_entry_point": {
+               "api": ("treecode_force_mrag" if kind == "force" else "treecode_potential")
+               + " (C ABI, host pointers, FP64)",
+               "value": ws * m / (e2e_ref_ms * 1e-3) / 1e6, "ms_per_step": e2e_ref_ms}}
 
     # ---- CPU baseline (rank 0, N = 1)
     cpu = None
@@ -401,13 +462,16 @@ def run_b200(args, ws, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": "Mtargets/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if mixed else "f64",
             "data": "synthetic (seeded PCG64; the reference's datasets are not available)",
-            "config": {"workload": w["name"], "theta": w["theta"], "order": ORDER_FORCE
-                       if kind == "force" else 12, "sources": len(w["xs"]), "targets": m,
-                       "precision": "fp64", "parallelism": f"{ws} independent solves (one per GPU)",
+            "config": {"workload": w["name"], "theta": w["theta"],
+                       "order": ORDER_FORCE if kind == "force" else 12,
+                       "sources": len(w["xs"]), "targets": m, "precision": args.precision,
+                       "parallelism": f"{ws} independent solves (one per GPU)",
                        "l2": "inputs larger than L2 (384 MB of sources per step)"},
             "accuracy": acc,
+            "plain_fp64": other,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
