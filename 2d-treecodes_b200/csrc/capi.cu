@@ -127,6 +127,9 @@ static void finish_timing(Context &c) {
     float tot = 0;
     cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
     c.times.total_ms = tot;
+    float k = 0;
+    cudaEventElapsedTime(&k, c.ev[6], c.ev[7]);
+    c.times.eval_kernel_ms = k;
 }
 
 // Sort, topology and upward pass for `kind` (0 potential, 1 force).
@@ -384,6 +387,7 @@ TC_API int tc_get_stats(tc_context *ctx, tc_stats *out) {
     out->e2l_pairs = c.counts.e2l_pairs;
     out->l2p_targets = c.counts.l2p_targets;
     out->launches = c.counts.launches;
+    out->eval_kernel_ms = c.times.eval_kernel_ms;
     return TC_OK;
 }
 

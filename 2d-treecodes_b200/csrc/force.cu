@@ -721,12 +721,14 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
                                                 (long long)sm_count() * occ[mixed]);
     auto eval = mixed ? k_force_eval<ORDER_FORCE, true> : k_force_eval<ORDER_FORCE, false>;
+    phase_mark(c, 6);
     eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
         nbricks, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
         slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
         slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr, sexp, sscale,
         task_brick);
     TC_KERNEL_CHECK();
+    phase_mark(c, 7);
     if (ntasks > nbricks) {
         k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8, (long long)sm_count() * 16),
                                256, 0, c.stream>>>(nbricks, offs, partial, xout, yout);

@@ -454,11 +454,13 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     }
     const int egrid = (int)std::min<long long>((ntasks + PE_WARPS - 1) / PE_WARPS,
                                                (long long)sm_count_p() * occ[mixed]);
+    phase_mark(c, 6);
     eval<<<egrid, PE_WARPS * 32, 0, c.stream>>>(
         ngroups, m, xt, yt, vo, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
         slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
         slot_ptr<double>(c, S_VS), offs, lists, out, partial, task_ctr, task_group, sexp, sscale);
     TC_KERNEL_CHECK();
+    phase_mark(c, 7);
     if (ntasks > ngroups) {
         k_potential_gather_parts<<<(int)std::min<long long>((ngroups + 7) / 8, (long long)sm_count_p() * 16),
                                    256, 0, c.stream>>>(ngroups, m, vo, offs, partial, out);

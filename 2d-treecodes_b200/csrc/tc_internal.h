@@ -41,7 +41,7 @@ enum Slot {
 };
 
 struct PhaseTimes {
-    float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms;
+    float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms, eval_kernel_ms;
 };
 
 struct Counts {

@@ -89,6 +89,7 @@ typedef struct {
     long long e2l_pairs;             /* (brick, cell) multipole-to-local translations */
     long long l2p_targets;           /* targets evaluated from local expansions */
     long long launches;              /* kernels launched by the last solve */
+    float eval_kernel_ms;            /* the evaluation kernel alone (timing enabled) */
 } tc_stats;
 
 /* device < 0 selects the current device; stream may be NULL (the context creates one). */

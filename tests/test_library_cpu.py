@@ -107,9 +107,13 @@ def test_bench_flop_model_and_profile_parse(tmp_path):
     assert bench.algorithmic_flops(st) == 110 + 2 * (16 * p + 8) + 3 * (4 * p * p + 20 * p) + 64 * 10 * p
     f = tmp_path / "x.txt"
     f.write_text("kernel: k_force_eval\ndram_bytes_per_launch: 123456 (read + write)\n")
-    old = bench.PROFILE_TRAFFIC
+    old = bench.PROFILE_TRAFFIC, bench.PROFILE_TRAFFIC_MIXED
     bench.PROFILE_TRAFFIC = str(f)
+    bench.PROFILE_TRAFFIC_MIXED = str(tmp_path / "missing.txt")
     try:
-        assert bench.read_profile_traffic() == 123456.0
+        assert bench.read_profile_traffic(False) == 123456.0
+        assert bench.read_profile_traffic(True) is None
     finally:
-        bench.PROFILE_TRAFFIC = old
+        bench.PROFILE_TRAFFIC, bench.PROFILE_TRAFFIC_MIXED = old
+    # the committed summaries of both forms carry the traffic line
+    assert bench.read_profile_traffic(False) > 0 and bench.read_profile_traffic(True) > 0
