@@ -204,17 +204,6 @@ __device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
 }
 
 // z^e for e = 1..31 by binary powering
-__device__ __forceinline__ cplx cpow_int(cplx z, int e) {
-    cplx r = {1.0, 0.0};
-    cplx b = z;
-#pragma unroll
-    for (int bit = 0; bit < 5; ++bit) {
-        if (e & (1 << bit)) r = cmul(r, b);
-        b = cmul(b, b);
-    }
-    return r;
-}
-
 // MIXED = false: plain FP64.  MIXED = true: P2P and E2P in FP32 (float offsets from the brick
 // corner split into hi + lo parts, scaled multipole coefficients, compensated per-target
 // sums); the local expansion (E2L, L2P) stays FP64.

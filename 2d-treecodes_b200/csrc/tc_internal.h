@@ -40,6 +40,12 @@ enum Slot {
     S_NUM_SLOTS
 };
 
+// First node id of each level (breadth-first numbering): level l occupies [off[l], off[l+1]),
+// off[LMAX + 1] = number of nodes.  Passed to kernels by value.
+struct LevelOffsets {
+    int off[LMAX + 3];
+};
+
 struct PhaseTimes {
     float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms, eval_kernel_ms;
 };

@@ -35,4 +35,16 @@ __device__ __forceinline__ cplx cfma(cplx a, cplx b, cplx c) {
     return {fma(a.re, b.re, fma(-a.im, b.im, c.re)), fma(a.re, b.im, fma(a.im, b.re, c.im))};
 }
 
+// z^e for 0 <= e < 32 by square-and-multiply
+__device__ __forceinline__ cplx cpow_int(cplx z, int e) {
+    cplx r = {1.0, 0.0};
+    cplx b = z;
+#pragma unroll
+    for (int bit = 0; bit < 5; ++bit) {
+        if (e & (1 << bit)) r = cmul(r, b);
+        b = cmul(b, b);
+    }
+    return r;
+}
+
 }  // namespace tc

@@ -157,9 +157,6 @@ __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned shor
     }
 }
 
-struct LevelOffsets {
-    int off[LMAX + 2];
-};
 
 __global__ void k_tree_root(int n, int leafcap, TNode *tnode, int2 *range, int4 *cell) {
     range[0] = make_int2(0, n);

@@ -1,12 +1,14 @@
 // upward.cu -- the upward pass: leaf setup + P2E, then E2E level by level.
 //
-// k_upward_leaves: persistent warps, one leaf at a time (drivers/upward.cpp:61-93,
-// kernels/upward-common.ispc:13-57, kernels/upward-kernels.m4:18-93).
-// k_upward_level: one launch per tree level, deepest first; one warp per inner node merges its
-// four children and shifts their expansions into it (upward.cpp:95-218,
-// kernels/upward-kernels.m4:95-149).  Children were finished by the previous launch, so no
-// atomics or fences are needed; the reference does the same merges in the order its OpenMP
-// tasks happen to finish.
+// k_leaf_setup: four threads per node run the leaf setup with the reference's four strided
+// accumulators (drivers/upward.cpp:61-93, kernels/upward-common.ispc:13-57).
+// k_leaf_p2e: one warp per leaf forms its multipole expansion, lanes over sources with the P
+// coefficients in registers (kernels/upward-kernels.m4:18-93).
+// k_upward_level: one launch per deep tree level, deepest first, one warp per inner node; the
+// small top levels run in one single-block launch that walks them with a block barrier between
+// levels (upward.cpp:95-218, kernels/upward-kernels.m4:95-149).  Children were finished before
+// their parent's level starts, so no atomics or fences are needed; the reference does the same
+// merges in the order its OpenMP tasks happen to finish.
 //
 // Bit-exact restatements (decisions of the traversals depend on these values):
 //  * leaf mass / |v| weights / weighted sums: four strided lane accumulators, reduced as
@@ -20,6 +22,8 @@
 //    child 3 -- the last child to arrive in the reference's sequential subtree order -- becomes
 //    an empty leaf (upward.cpp:173-180); with exactly three negligible children the remaining
 //    child's coefficients are copied unshifted (upward.cpp:182-188).
+// The expansion coefficients themselves are sums whose order is free (the parity gate on them
+// is a relative tolerance), so P2E and E2E use whatever order suits the GPU.
 //
 // Expansion layout: exps[node][0][k] real parts, exps[node][1][k] imaginary parts, k < ORDER.
 #include <algorithm>
@@ -29,291 +33,445 @@
 
 namespace tc {
 
-__constant__ BinomTable c_binom_up = make_binom_table();
+__constant__ BinomTable c_binom_up = make_binom_table();   // uniform indices only
+__device__ const BinomTable g_binom_up = make_binom_table();   // per-lane indices
 
-constexpr int UP_WARPS = 4;
-constexpr int UP_CHUNK = 256;   // leaf sources staged in shared memory per pass (multiple of 4)
+constexpr int UP_WARPS = 4;          // warps per block of the leaf and per-level merge kernels
+constexpr int UP_TOP_WARPS = 16;     // warps of the single-block launch over the top levels
+constexpr int UP_TOP_MAX_NODES = 64;     // a level this small joins the single-block launch
+constexpr int UP_WIDE_MIN_NODES = 2048;  // a level with this many inner nodes: thread per node
+constexpr int UP_WIDE_WARPS = 1;         // warps per block of the thread-per-node kernel
 
-// Per-warp scratch of the leaf kernel; the phases of a leaf use it one after the other.
-template <int P>
-struct LeafShared {
-    union {
-        struct {
-            double sx[UP_CHUNK], sy[UP_CHUNK], sv[UP_CHUNK];   // staged leaf sources (setup)
-        } stage;
-        struct {
-            double re[32][P + 1], im[32][P + 1];   // v z^(n+1) of a 32-source chunk (P2E)
-        } terms;
-    };
-};
-
-// Per-warp scratch of the merge kernel.
-template <int P>
-struct MergeShared {
-    double zr[4][P + 1], zi[4][P + 1];   // z0^-k per child
-    double cr[4][P + 1], ci[4][P + 1];   // a_{k-1} z0^-k per child
-    double pr[4][P], pi[4][P];           // shifted contribution of child c to coefficient l
-};
 
 __device__ __forceinline__ bool is_leaf(int2 rg, int4 cl, int leafcap) {
     return (rg.y - rg.x <= leafcap) || cl.x == LMAX;
 }
 
 // ------------------------------------------------------------------------------ leaves
-template <int P>
-__device__ __forceinline__ void upward_leaf(
-    int node, int nnodes, int nsrc, int leafcap, const double *__restrict__ xs,
-    const double *__restrict__ ys, const double *__restrict__ vs, const int2 *__restrict__ range,
-    const int4 *__restrict__ cell, TNode *tnode, double *mass, double *wgt, double *wxs,
-    double *wys, double *exps, const Frame *__restrict__ frame, unsigned *err,
-    LeafShared<P> &sh) {
-    const int lane = lane_id();
-    const int2 rg = range[node];
-    const int4 cl = cell[node];
-    if (!is_leaf(rg, cl, leafcap)) return;
-    if (rg.x < 0 || rg.y < rg.x || rg.y > nsrc || cl.w >= nnodes || cl.x < 0 || cl.x > LMAX) {
-        if (lane == 0) atomicOr(err, DEVERR_BOUNDS);
-        return;
-    }
-    const Frame f = *frame;
-    const int s = rg.x, e = rg.y;
-
-    // Leaf sources pass through shared memory in chunks of UP_CHUNK (coalesced loads by all
-    // lanes); a leaf that fits one chunk is loaded once for both setup passes.
-    const int nch = (e - s + UP_CHUNK - 1) / UP_CHUNK;
-    auto stage = [&](int c0, int cnt) {
-        __syncwarp();
-        for (int j = lane; j < cnt; j += 32) {
-            sh.stage.sx[j] = xs[c0 + j];
-            sh.stage.sy[j] = ys[c0 + j];
-            sh.stage.sv[j] = vs[c0 + j];
-        }
-        __syncwarp();
-    };
-
-    // ---- upward_setup: four strided lane accumulators (upward-common.ispc:24-42); chunks
-    // start at multiples of 4 from s, so element i still goes to lane (i - s) % 4.
-    double ms = 0, ws = 0, wxs_l = 0, wys_l = 0;
-    for (int ch = 0; ch < nch; ++ch) {
-        const int c0 = s + ch * UP_CHUNK, cnt = min(UP_CHUNK, e - c0);
-        stage(c0, cnt);
-        if (lane < 4)
-#pragma unroll 4
-            for (int j = lane; j < cnt; j += 4) {
-                const double x = sh.stage.sx[j], y = sh.stage.sy[j], m = sh.stage.sv[j];
-                const double w = fabs(m);
-                ms = __dadd_rn(ms, m);
-                ws = __dadd_rn(ws, w);
-                wxs_l = __dadd_rn(wxs_l, __dmul_rn(x, w));
-                wys_l = __dadd_rn(wys_l, __dmul_rn(y, w));
+// k_leaf_setup: lane quad per node (4 threads each, in the order of the node ids).  Only the
+// quads of leaves do work; the others still take part in the quad shuffles.
+__global__ __launch_bounds__(256) void k_leaf_setup(
+    int nnodes, int nsrc, int leafcap, const double *__restrict__ xs, const double *__restrict__ ys,
+    const double *__restrict__ vs, const int2 *__restrict__ range, const int4 *__restrict__ cell,
+    TNode *tnode, double *mass, double *wgt, double *wxs, double *wys,
+    const Frame *__restrict__ frame, unsigned *err) {
+    const int lane = lane_id(), q = lane & 3, qbase = lane & ~3;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int node = (int)(tid >> 2);
+    bool act = false;
+    int s = 0, e = 0;
+    int4 cl = {0, 0, 0, 0};
+    if (node < nnodes) {
+        const int2 rg = range[node];
+        cl = cell[node];
+        if (is_leaf(rg, cl, leafcap)) {
+            if (rg.x < 0 || rg.y < rg.x || rg.y > nsrc || cl.w >= nnodes || cl.x < 0 || cl.x > LMAX) {
+                if (q == 0) atomicOr(err, DEVERR_BOUNDS);
+            } else {
+                act = true;
+                s = rg.x;
+                e = rg.y;
             }
+        }
     }
+    // four strided accumulators: element i goes to lane (i - s) % 4 (upward-common.ispc:24-42)
+    double ms = 0, ws = 0, wxl = 0, wyl = 0;
+    if (act)
+#pragma unroll 8
+        for (int j = s + q; j < e; j += 4) {
+            const double x = __ldg(xs + j), y = __ldg(ys + j), m = __ldg(vs + j);
+            const double w = fabs(m);
+            ms = __dadd_rn(ms, m);
+            ws = __dadd_rn(ws, w);
+            wxl = __dadd_rn(wxl, __dmul_rn(x, w));
+            wyl = __dadd_rn(wyl, __dmul_rn(y, w));
+        }
+    // (l0 + l1) + (l2 + l3) within the quad, broadcast to its four lanes
     auto reduce4 = [&](double v) {
-        const double a = __dadd_rn(v, __shfl_down_sync(FULL_MASK, v, 1));   // lane0: l0+l1, lane2: l2+l3
-        return __shfl_sync(FULL_MASK, __dadd_rn(a, __shfl_down_sync(FULL_MASK, a, 2)), 0);
+        const double a = __dadd_rn(v, __shfl_down_sync(FULL_MASK, v, 1));
+        return __shfl_sync(FULL_MASK, __dadd_rn(a, __shfl_down_sync(FULL_MASK, a, 2)), qbase);
     };
-    const double msum = reduce4(ms);
-    const double wsum = reduce4(ws);
-    const double xsum = reduce4(wxs_l);
-    const double ysum = reduce4(wys_l);
-
+    const double msum = reduce4(ms), wsum = reduce4(ws), xsum = reduce4(wxl), ysum = reduce4(wyl);
     // radius about the per-lane centre (upward-common.ispc:44-56)
     double r2 = 0;
-    {
+    if (act) {
         const double lx = ws != 0 ? __ddiv_rn(xsum, wsum) : 0.0;
         const double ly = ws != 0 ? __ddiv_rn(ysum, wsum) : 0.0;
-        for (int ch = 0; ch < nch; ++ch) {
-            const int c0 = s + ch * UP_CHUNK, cnt = min(UP_CHUNK, e - c0);
-            if (nch > 1) stage(c0, cnt);
-            if (lane < 4)
-#pragma unroll 4
-                for (int j = lane; j < cnt; j += 4) {
-                    const double xr = __dsub_rn(sh.stage.sx[j], lx), yr = __dsub_rn(sh.stage.sy[j], ly);
-                    r2 = fmax(r2, __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(yr, yr)));
-                }
+#pragma unroll 8
+        for (int j = s + q; j < e; j += 4) {
+            const double xr = __dsub_rn(__ldg(xs + j), lx), yr = __dsub_rn(__ldg(ys + j), ly);
+            r2 = fmax(r2, __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(yr, yr)));
         }
     }
-    r2 = fmax(r2, __shfl_down_sync(FULL_MASK, r2, 1));
-    r2 = fmax(r2, __shfl_down_sync(FULL_MASK, r2, 2));
-    const double radius = __dsqrt_rn(__shfl_sync(FULL_MASK, r2, 0));
-
-    // com (upward.cpp:71-72; x0 = fma(cx, h, xmin) as in build_tree)
-    double xcom, ycom;
-    if (wsum != 0) {
-        xcom = __ddiv_rn(xsum, wsum);
-        ycom = __ddiv_rn(ysum, wsum);
-    } else {
-        const double h = __ddiv_rn(f.ext, (double)(1 << cl.x));
-        xcom = __fma_rn(0.5, h, __fma_rn((double)cl.y, h, f.xmin));
-        ycom = __fma_rn(0.5, h, __fma_rn((double)cl.z, h, f.ymin));
-    }
-
-    // ---- upward_p2e: a_n = -sum v (z - c)^(n+1) / (n+1).  For each chunk of 32 sources, lane i
-    // writes the terms v z_i^(n+1) of its source to shared memory (row i); lane n then adds up
-    // column n.  No per-lane coefficient arrays and no cross-lane reduction are needed.
-    double accr = 0, acci = 0;
-    for (int c0 = s; c0 < e; c0 += 32) {
-        const int cnt = min(32, e - c0);
-        __syncwarp();
-        if (lane < cnt) {
-            const double r0 = xs[c0 + lane] - xcom, i0 = ys[c0 + lane] - ycom;
-            const double v = vs[c0 + lane];
-            double pr = r0, pim = i0;
-#pragma unroll
-            for (int n = 0; n < P; ++n) {
-                sh.terms.re[lane][n] = pr * v;
-                sh.terms.im[lane][n] = pim * v;
-                const double tr = pr * r0 - pim * i0;
-                const double ti = pr * i0 + pim * r0;
-                pr = tr;
-                pim = ti;
-            }
+    r2 = fmax(r2, __shfl_xor_sync(FULL_MASK, r2, 1));
+    r2 = fmax(r2, __shfl_xor_sync(FULL_MASK, r2, 2));
+    if (act && q == 0) {
+        // com (upward.cpp:71-72; x0 = fma(cx, h, xmin) as in build_tree)
+        double xcom, ycom;
+        if (wsum != 0) {
+            xcom = __ddiv_rn(xsum, wsum);
+            ycom = __ddiv_rn(ysum, wsum);
+        } else {
+            const Frame f = *frame;
+            const double h = __ddiv_rn(f.ext, (double)(1 << cl.x));
+            xcom = __fma_rn(0.5, h, __fma_rn((double)cl.y, h, f.xmin));
+            ycom = __fma_rn(0.5, h, __fma_rn((double)cl.z, h, f.ymin));
         }
-        __syncwarp();
-        if (lane < P)
-            for (int i = 0; i < cnt; ++i) {
-                accr += sh.terms.re[i][lane];
-                acci += sh.terms.im[i][lane];
-            }
-    }
-    __syncwarp();
-    double *ex = exps + (size_t)node * 2 * P;
-    if (lane < P) {
-        const double f = -1.0 / (lane + 1);
-        ex[lane] = accr * f;
-        ex[P + lane] = acci * f;
-    }
-    if (lane == 0) {
         tnode[node].xcom = xcom;
         tnode[node].ycom = ycom;
-        tnode[node].r = radius;
+        tnode[node].r = __dsqrt_rn(r2);
         mass[node] = msum;
         wgt[node] = wsum;
         wxs[node] = xsum;
         wys[node] = ysum;
     }
-
 }
 
+// k_leaf_p2e: a_n = -1/(n+1) sum_i v_i (z_i - c)^(n+1), one warp per leaf, lanes over sources
+// with the P coefficients in registers; the 32 partial sums of each coefficient meet in shared
+// memory, transposed so that lane n adds up coefficient n.
 template <int P>
-__global__ __launch_bounds__(UP_WARPS * 32) void k_upward_leaves(
+struct LeafShared {
+    double v[32][2 * P + 1];
+};
+
+
+template <int P>
+__global__ __launch_bounds__(UP_WARPS * 32) void k_leaf_p2e(
     int nnodes, int nsrc, int leafcap, const double *__restrict__ xs, const double *__restrict__ ys,
     const double *__restrict__ vs, const int2 *__restrict__ range, const int4 *__restrict__ cell,
-    TNode *tnode, double *mass, double *wgt, double *wxs, double *wys, double *exps,
-    const Frame *__restrict__ frame, unsigned *err) {
+    const TNode *__restrict__ tnode, double *exps) {
+    constexpr int U = P > 16 ? 6 : 4;   // sources per lane in flight
     extern __shared__ __align__(16) unsigned char leaf_smem[];
-    LeafShared<P> *shared = reinterpret_cast<LeafShared<P> *>(leaf_smem);
-    const int warp = threadIdx.x >> 5;
-    for (int node = blockIdx.x * UP_WARPS + warp; node < nnodes; node += gridDim.x * UP_WARPS)
-        upward_leaf<P>(node, nnodes, nsrc, leafcap, xs, ys, vs, range, cell, tnode, mass, wgt,
-                       wxs, wys, exps, frame, err, shared[warp]);
+    LeafShared<P> &sh = reinterpret_cast<LeafShared<P> *>(leaf_smem)[threadIdx.x >> 5];
+    const int lane = lane_id();
+    const int stride = gridDim.x * UP_WARPS;
+    int next = blockIdx.x * UP_WARPS + (threadIdx.x >> 5);
+    // the next node's record is loaded while the current leaf is expanded
+    int2 nrg = {0, 0};
+    int4 ncl = {0, 0, 0, 0};
+    double ncx = 0, ncy = 0;
+    if (next < nnodes) {
+        nrg = range[next];
+        ncl = cell[next];
+        ncx = tnode[next].xcom;
+        ncy = tnode[next].ycom;
+    }
+    while (next < nnodes) {
+        const int node = next;
+        const int2 rg = nrg;
+        const int4 cl = ncl;
+        const double cx = ncx, cy = ncy;
+        next += stride;
+        if (next < nnodes) {
+            nrg = range[next];
+            ncl = cell[next];
+            ncx = tnode[next].xcom;
+            ncy = tnode[next].ycom;
+        }
+        if (!is_leaf(rg, cl, leafcap) || rg.x < 0 || rg.y < rg.x || rg.y > nsrc) continue;
+        double ar[P], ai[P];
+#pragma unroll
+        for (int n = 0; n < P; ++n) ar[n] = ai[n] = 0.0;
+        for (int base = rg.x; base < rg.y; base += 32 * U) {
+            const int nu = min(U, (rg.y - base + 31) >> 5);   // warp-uniform
+            double zr[U], zi[U], v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = base + 32 * u + lane;
+                const bool ok = u < nu && j < rg.y;
+                zr[u] = ok ? __ldg(xs + j) - cx : 0.0;
+                zi[u] = ok ? __ldg(ys + j) - cy : 0.0;
+                v[u] = ok ? __ldg(vs + j) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (u >= nu) break;
+                double pr = v[u] * zr[u], pim = v[u] * zi[u];
+#pragma unroll
+                for (int n = 0; n < P; ++n) {
+                    ar[n] += pr;
+                    ai[n] += pim;
+                    const double tr = fma(pr, zr[u], -pim * zi[u]);
+                    pim = fma(pr, zi[u], pim * zr[u]);
+                    pr = tr;
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int n = 0; n < P; ++n) {
+            sh.v[lane][n] = ar[n];
+            sh.v[lane][P + n] = ai[n];
+        }
+        __syncwarp();
+        if (lane < P) {
+            double sr0 = 0, sr1 = 0, si0 = 0, si1 = 0;
+#pragma unroll 8
+            for (int i = 0; i < 32; i += 2) {
+                sr0 += sh.v[i][lane];
+                sr1 += sh.v[i + 1][lane];
+                si0 += sh.v[i][P + lane];
+                si1 += sh.v[i + 1][P + lane];
+            }
+            const double fac = -1.0 / (lane + 1);
+            double *ex = exps + (size_t)node * 2 * P;
+            ex[lane] = (sr0 + sr1) * fac;
+            ex[P + lane] = (si0 + si1) * fac;
+        }
+        __syncwarp();
+    }
 }
 
 // ------------------------------------------------------------------------------ merge (E2E)
-// b_l = sum_c z0^l [ -m/l + sum_{k=1..l} C(l-1,k-1) a_{k-1} z0^-k ], z0 = child com - parent com
+// b_l = sum_c z0^l [ -m_c/l + sum_{k=1..l} C(l-1,k-1) a_{c,k-1} z0^-k ],  z0 = child com - parent
+// com.  Lane l-1 (l = 1..P) owns coefficient l of the parent for all four children; the
+// binomials C(l-1, k-1) (zero for k > l) are read from a block-shared table, row k.
 template <int P>
-__device__ void shift_children(MergeShared<P> &sh, const double *exps, int cb, const double *cm,
-                               const double *cx, const double *cy, double px, double py,
-                               double *dst, const double (*bin)[P]) {
-    const int lane = lane_id();
-    if (lane < 4) {
-        const int c = lane;
-        const double x0 = cx[c] - px, y0 = cy[c] - py;
-        const double r2z0 = x0 * x0 + y0 * y0;
-        const double rinv = x0 / r2z0, iinv = -y0 / r2z0;
-        double zr = rinv, zi = iinv;
-        sh.zr[c][1] = zr;
-        sh.zi[c][1] = zi;
-        for (int j = 2; j <= P; ++j) {
-            const double tr = zr * rinv - zi * iinv;
-            const double ti = zr * iinv + zi * rinv;
-            zr = tr;
-            zi = ti;
-            sh.zr[c][j] = zr;
-            sh.zi[c][j] = zi;
-        }
+struct MergeShared {
+    cplx coef[4][P];   // a_{c,k-1} z0_c^-k, k = 1..P
+};
+
+template <int P>
+struct BinomRows {
+    double b[P][32];   // b[k][lane] = C(lane, k) for k <= lane < P, else 0
+};
+
+template <int P>
+__device__ __forceinline__ void fill_binom_rows(BinomRows<P> &t) {
+    for (int i = threadIdx.x; i < P * 32; i += blockDim.x) {
+        const int k = i / 32, l = i % 32;
+        t.b[k][l] = (l < P && k <= l) ? g_binom_up.c[l][k] : 0.0;
     }
-    __syncwarp();
-    for (int it = lane; it < 4 * P; it += 32) {
-        const int c = it / P, k = it % P + 1;
-        const double *ex = exps + (size_t)(cb + c) * 2 * P;
-        const double ar = ex[k - 1], ai = ex[P + k - 1];
-        sh.cr[c][k] = ar * sh.zr[c][k] - ai * sh.zi[c][k];
-        sh.ci[c][k] = ar * sh.zi[c][k] + ai * sh.zr[c][k];
-    }
-    __syncwarp();
-    // P lanes; lane j takes children (0,1) or (2,3) and the coefficient pair (l, P + 1 - l), so
-    // every busy lane runs the same 2 * (P + 1) inner iterations.
-    if (lane < P) {
-        const int half = P / 2;
-        const int c0 = lane < half ? 0 : 2;
-        const int jj = lane % half;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int l = q == 0 ? jj + 1 : P - jj;
-            const double minv = -1.0 / l;
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const int c = c0 + cc;
-                double rtmp = l == 1 ? -cm[c] : cm[c] * minv;
-                double itmp = 0;
-                for (int k = 1; k <= l; ++k) {
-                    const double b = bin[k - 1][l - 1];
-                    rtmp += sh.cr[c][k] * b;
-                    itmp += sh.ci[c][k] * b;
-                }
-                const double zr = sh.zr[c][l], zi = sh.zi[c][l];
-                const double invz2 = zr * zr + zi * zi;
-                const double inv = invz2 != 0 ? 1.0 / invz2 : 0.0;
-                const double rz = zr * inv, iz = -zi * inv;
-                sh.pr[c][l - 1] = rtmp * rz - itmp * iz;
-                sh.pi[c][l - 1] = rtmp * iz + itmp * rz;
-            }
-        }
-    }
-    __syncwarp();
-    if (lane < P) {
-        dst[lane] = (sh.pr[0][lane] + sh.pr[1][lane]) + (sh.pr[2][lane] + sh.pr[3][lane]);
-        dst[P + lane] = (sh.pi[0][lane] + sh.pi[1][lane]) + (sh.pi[2][lane] + sh.pi[3][lane]);
-    }
-    __syncwarp();
 }
 
 template <int P>
-__global__ __launch_bounds__(UP_WARPS * 32) void k_upward_level(
+__device__ __forceinline__ void merge_node(int parent, int nnodes, int leafcap, double ext,
+                                           const int2 *__restrict__ range,
+                                           const int4 *__restrict__ cell, TNode *tnode,
+                                           double *mass, double *wgt, double *wxs, double *wys,
+                                           double *exps, unsigned *err, const BinomRows<P> &bt,
+                                           MergeShared<P> &sh) {
+    const int lane = lane_id();
+    const int2 prg = range[parent];
+    const int4 pcl = cell[parent];
+    const int cb = tnode[parent].child;
+    if (is_leaf(prg, pcl, leafcap)) return;
+    if (cb <= parent || cb + 4 > nnodes) {
+        if (lane == 0) atomicOr(err, DEVERR_BOUNDS);
+        return;
+    }
+    // this lane's coefficient of each child, loaded together with the children's moments
+    double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
+    if (lane < P)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double *ex = exps + (size_t)(cb + c) * 2 * P;
+            er[c] = ex[lane];
+            ei[c] = ex[P + lane];
+        }
+    double cm[4], cw[4], cwx[4], cwy[4], cxc[4], cyc[4], cr[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        cm[c] = mass[cb + c];
+        cw[c] = wgt[cb + c];
+        cwx[c] = wxs[cb + c];
+        cwy[c] = wys[cb + c];
+        cxc[c] = tnode[cb + c].xcom;
+        cyc[c] = tnode[cb + c].ycom;
+        cr[c] = tnode[cb + c].r;
+    }
+    const double pm = __dadd_rn(__dadd_rn(cm[0], cm[3]), __dadd_rn(cm[1], cm[2]));
+    const double pw = __dadd_rn(__dadd_rn(cw[0], cw[3]), __dadd_rn(cw[1], cw[2]));
+    const double pwx = __dadd_rn(__dadd_rn(cwx[0], cwx[3]), __dadd_rn(cwx[1], cwx[2]));
+    const double pwy = __dadd_rn(__dadd_rn(cwy[0], cwy[3]), __dadd_rn(cwy[1], cwy[2]));
+    const double px = __ddiv_rn(pwx, pw), py = __ddiv_rn(pwy, pw);
+    double rr = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        if (cw[c] != 0) {
+            const double rx = __dsub_rn(px, cxc[c]), ry = __dsub_rn(py, cyc[c]);
+            const double cand = __dadd_rn(__dsqrt_rn(__fma_rn(rx, rx, __dmul_rn(ry, ry))), cr[c]);
+            rr = cand > rr ? cand : rr;
+        }
+    const double cap = __ddiv_rn(__dmul_rn((double)1.4143f, ext), (double)(1 << pcl.x));
+    const double prad = cap < rr ? cap : rr;
+
+    int zcount = 0, nz = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const bool negl = fabs(cw[c]) < 1.1e-16;
+        zcount += negl;
+        if (!negl) nz = c;
+    }
+    double *dst = exps + (size_t)parent * 2 * P;
+    if (zcount == 4) {
+        for (int k = lane; k < 2 * P; k += 32) dst[k] = 0.0;
+        if (lane == 0) {
+            tnode[cb + 3].child = -1;
+            tnode[cb + 3].count = 0;
+        }
+    } else if (zcount == 3) {
+        double sr = 0, si = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (c == nz) {
+                sr = er[c];
+                si = ei[c];
+            }
+        if (lane < P) {
+            dst[lane] = sr;
+            dst[P + lane] = si;
+        }
+    } else {
+        const int l = lane + 1;
+        cplx zl[4];   // z0_c^-l for this lane's l
+        __syncwarp();
+        if (lane < P) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double x0 = cxc[c] - px, y0 = cyc[c] - py;
+                const double r2z0 = x0 * x0 + y0 * y0;
+                zl[c] = cpow_int({x0 / r2z0, -y0 / r2z0}, l);
+                sh.coef[c][lane] = cmul({er[c], ei[c]}, zl[c]);
+            }
+        }
+        __syncwarp();
+        if (lane < P) {
+            const double minv = -1.0 / l;
+            double tr[4], ti[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                tr[c] = l == 1 ? -cm[c] : cm[c] * minv;
+                ti[c] = 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const double b = bt.b[k][lane];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const cplx a = sh.coef[c][k];
+                    tr[c] = fma(b, a.re, tr[c]);
+                    ti[c] = fma(b, a.im, ti[c]);
+                }
+            }
+            // z0^l = 1 / z0^-l
+            double sr[4], si[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double invz2 = zl[c].re * zl[c].re + zl[c].im * zl[c].im;
+                const double inv = invz2 != 0 ? 1.0 / invz2 : 0.0;
+                const double rz = zl[c].re * inv, iz = -zl[c].im * inv;
+                sr[c] = tr[c] * rz - ti[c] * iz;
+                si[c] = tr[c] * iz + ti[c] * rz;
+            }
+            dst[lane] = (sr[0] + sr[1]) + (sr[2] + sr[3]);
+            dst[P + lane] = (si[0] + si[1]) + (si[2] + si[3]);
+        }
+    }
+    if (lane == 0) {
+        tnode[parent].xcom = px;
+        tnode[parent].ycom = py;
+        tnode[parent].r = prad;
+        mass[parent] = pm;
+        wgt[parent] = pw;
+        wxs[parent] = pwx;
+        wys[parent] = pwy;
+    }
+}
+
+// One level: inner nodes [lo, hi), one warp each.
+template <int P>
+__global__ __launch_bounds__(UP_WARPS * 32, 5) void k_upward_level(
     int lo, int hi, int nnodes, int leafcap, const int2 *__restrict__ range,
     const int4 *__restrict__ cell, TNode *tnode, double *mass, double *wgt, double *wxs,
     double *wys, double *exps, const Frame *__restrict__ frame, unsigned *err) {
     __shared__ MergeShared<P> shared[UP_WARPS];
-    __shared__ double s_bin[P][P];   // s_bin[k-1][l-1] = C(l-1, k-1): lane l reads a row
-    for (int i = threadIdx.x; i < P * P; i += blockDim.x) {
-        const int k = i / P, l = i % P;
-        s_bin[k][l] = c_binom_up.c[l][k];
-    }
+    __shared__ BinomRows<P> bt;
+    fill_binom_rows<P>(bt);
     __syncthreads();
-    const int lane = lane_id(), warp = threadIdx.x >> 5;
-    MergeShared<P> &sh = shared[warp];
     const double ext = frame->ext;
-    for (int parent = lo + blockIdx.x * UP_WARPS + warp; parent < hi;
-         parent += gridDim.x * UP_WARPS) {
-        const int2 prg = range[parent];
-        const int4 pcl = cell[parent];
-        if (is_leaf(prg, pcl, leafcap)) continue;
-        const int cb = tnode[parent].child;
-        if (cb <= parent || cb + 4 > nnodes) {
-            if (lane == 0) atomicOr(err, DEVERR_BOUNDS);
-            continue;
+    MergeShared<P> &sh = shared[threadIdx.x >> 5];
+    for (int parent = lo + blockIdx.x * UP_WARPS + (threadIdx.x >> 5); parent < hi;
+         parent += gridDim.x * UP_WARPS)
+        merge_node<P>(parent, nnodes, leafcap, ext, range, cell, tnode, mass, wgt, wxs, wys, exps,
+                      err, bt, sh);
+}
+
+// Wide levels: one thread per inner node.  Inner node r of level l owns the children
+// off[l+1] + 4r .. +3 and is their common parent cell[off[l+1] + 4r].w.  A warp takes 32
+// consecutive inner nodes; child c of all 32 is staged through shared memory (coalesced runs of
+// 2P coefficients), transposed to one column per node, and every thread then shifts its own
+// child with the binomial sums fully unrolled (uniform constant-bank operands).
+template <int P>
+struct WideShared {
+    double a[2][2 * P][33];   // a[b][t][j]: coefficient t of node j's child, two buffers
+    double o[2 * P][33];      // o[t][j]: coefficient t of node j's result
+    int parent[32];
+};
+
+// 8-byte asynchronous global -> shared copies (no register staging), grouped per child.
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Child c of the warp's 32 inner nodes r0.. into buf[t][j] (node j's 2P coefficients, column j).
+template <int P>
+__device__ __forceinline__ void stage_children(double (*buf)[33], const double *exps, int cbase,
+                                               int r0, int ninner, int c) {
+    for (int idx = lane_id(); idx < 32 * 2 * P; idx += 32) {
+        const int j = idx / (2 * P), t = idx - j * (2 * P);
+        if (r0 + j < ninner)
+            cp_async8(&buf[t][j], exps + (size_t)(cbase + 4 * (r0 + j) + c) * 2 * P + t);
+        else
+            buf[t][j] = 0.0;
+    }
+    cp_async_commit();
+}
+
+template <int P>
+__global__ __launch_bounds__(UP_WIDE_WARPS * 32, 8) void k_upward_wide(
+    int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, TNode *tnode, double *mass,
+    double *wgt, double *wxs, double *wys, double *exps, const Frame *__restrict__ frame,
+    unsigned *err) {
+    __shared__ WideShared<P> shared[UP_WIDE_WARPS];
+    WideShared<P> &st = shared[threadIdx.x >> 5];
+    const int lane = lane_id();
+    const int cbase = lo.off[l + 1];
+    const int ninner = (lo.off[l + 2] - cbase) / 4;
+    const double ext = frame->ext;
+    for (int r0 = (blockIdx.x * UP_WIDE_WARPS + (threadIdx.x >> 5)) * 32; r0 < ninner;
+         r0 += gridDim.x * UP_WIDE_WARPS * 32) {
+        const int r = r0 + lane;
+        const int cb = cbase + 4 * r;
+        bool act = r < ninner;
+        int parent = -1;
+        if (act) {
+            parent = cell[cb].w;
+            if (parent < lo.off[l] || parent >= lo.off[l + 1] || tnode[parent].child != cb ||
+                cb + 4 > nnodes) {
+                atomicOr(err, DEVERR_TREE);
+                act = false;
+            }
         }
+        st.parent[lane] = act ? parent : -1;
         double cm[4], cw[4], cwx[4], cwy[4], cxc[4], cyc[4], cr[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            cm[c] = mass[cb + c];
-            cw[c] = wgt[cb + c];
-            cwx[c] = wxs[cb + c];
-            cwy[c] = wys[cb + c];
-            cxc[c] = tnode[cb + c].xcom;
-            cyc[c] = tnode[cb + c].ycom;
-            cr[c] = tnode[cb + c].r;
+            const int id = act ? cb + c : 0;
+            cm[c] = mass[id];
+            cw[c] = wgt[id];
+            cwx[c] = wxs[id];
+            cwy[c] = wys[id];
+            cxc[c] = tnode[id].xcom;
+            cyc[c] = tnode[id].ycom;
+            cr[c] = tnode[id].r;
         }
         const double pm = __dadd_rn(__dadd_rn(cm[0], cm[3]), __dadd_rn(cm[1], cm[2]));
         const double pw = __dadd_rn(__dadd_rn(cw[0], cw[3]), __dadd_rn(cw[1], cw[2]));
@@ -328,9 +486,6 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_upward_level(
                 const double cand = __dadd_rn(__dsqrt_rn(__fma_rn(rx, rx, __dmul_rn(ry, ry))), cr[c]);
                 rr = cand > rr ? cand : rr;
             }
-        const double cap = __ddiv_rn(__dmul_rn((double)1.4143f, ext), (double)(1 << pcl.x));
-        const double prad = cap < rr ? cap : rr;
-
         int zcount = 0, nz = 0;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -338,29 +493,104 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_upward_level(
             zcount += negl;
             if (!negl) nz = c;
         }
-        double *dst = exps + (size_t)parent * 2 * P;
-        if (zcount == 4) {
-            for (int k = lane; k < 2 * P; k += 32) dst[k] = 0.0;
-            if (lane == 0) {
-                tnode[cb + 3].child = -1;
-                tnode[cb + 3].count = 0;
-            }
-        } else if (zcount == 3) {
-            const double *src = exps + (size_t)(cb + nz) * 2 * P;
-            for (int k = lane; k < 2 * P; k += 32) dst[k] = src[k];
-        } else {
-            shift_children<P>(sh, exps, cb, cm, cxc, cyc, px, py, dst, s_bin);
-        }
-        if (lane == 0) {
+        if (act) {
+            const double cap = __ddiv_rn(__dmul_rn((double)1.4143f, ext), (double)(1 << l));
             tnode[parent].xcom = px;
             tnode[parent].ycom = py;
-            tnode[parent].r = prad;
+            tnode[parent].r = cap < rr ? cap : rr;
             mass[parent] = pm;
             wgt[parent] = pw;
             wxs[parent] = pwx;
             wys[parent] = pwy;
+            if (zcount == 4) {
+                tnode[cb + 3].child = -1;
+                tnode[cb + 3].count = 0;
+            }
         }
+        const bool shift = act && zcount <= 2;
+#pragma unroll
+        for (int k = 0; k < 2 * P; ++k) st.o[k][lane] = 0.0;
         __syncwarp();
+        stage_children<P>(st.a[0], exps, cbase, r0, ninner, 0);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            double (*a)[33] = st.a[c & 1];
+            // the next child's copies run while this one is shifted
+            if (c < 3) {
+                stage_children<P>(st.a[(c + 1) & 1], exps, cbase, r0, ninner, c + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncwarp();
+            if (act && zcount == 3 && c == nz)
+#pragma unroll
+                for (int k = 0; k < 2 * P; ++k) st.o[k][lane] = a[k][lane];
+            if (shift) {
+                // C_k = a_{k-1} z0^-k in place, then
+                // out_l += z0^l (-m/l + sum_{k<=l} C(l-1, k-1) C_k)
+                const double x0 = cxc[c] - px, y0 = cyc[c] - py;
+                const double r2z0 = x0 * x0 + y0 * y0;
+                const cplx zinv = {x0 / r2z0, -y0 / r2z0};
+                cplx zp = zinv;
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    const cplx v = cmul({a[k][lane], a[P + k][lane]}, zp);
+                    a[k][lane] = v.re;
+                    a[P + k][lane] = v.im;
+                    zp = cmul(zp, zinv);
+                }
+                const cplx z0 = {x0, y0};
+                cplx zl = z0;
+#pragma unroll
+                for (int L = 1; L <= P; ++L) {
+                    double tr = L == 1 ? -cm[c] : cm[c] * (-1.0 / L), ti = 0.0;
+#pragma unroll
+                    for (int k = 1; k <= L; ++k) {
+                        const double b = c_binom_up.c[L - 1][k - 1];
+                        tr = fma(b, a[k - 1][lane], tr);
+                        ti = fma(b, a[P + k - 1][lane], ti);
+                    }
+                    const cplx o = cfma({tr, ti}, zl, {st.o[L - 1][lane], st.o[P + L - 1][lane]});
+                    st.o[L - 1][lane] = o.re;
+                    st.o[P + L - 1][lane] = o.im;
+                    zl = cmul(zl, z0);
+                }
+            }
+            // this buffer is restaged two children later: all lanes must be done with it
+            __syncwarp();
+        }
+        // results written as runs of 2P per parent
+        __syncwarp();
+        for (int idx = lane; idx < 32 * 2 * P; idx += 32) {
+            const int j = idx / (2 * P), t = idx - j * (2 * P);
+            const int pj = st.parent[j];
+            if (pj >= 0) exps[(size_t)pj * 2 * P + t] = st.o[t][j];
+        }
+    }
+}
+
+// Levels ltop .. 0 (deepest first) in one block; the block barrier between levels orders each
+// level's writes before its parents' reads.
+template <int P>
+__global__ __launch_bounds__(UP_TOP_WARPS * 32) void k_upward_top(
+    int ltop, LevelOffsets level_off, int nnodes, int leafcap,
+    const int2 *__restrict__ range, const int4 *__restrict__ cell, TNode *tnode, double *mass,
+    double *wgt, double *wxs, double *wys, double *exps, const Frame *__restrict__ frame,
+    unsigned *err) {
+    __shared__ MergeShared<P> shared[UP_TOP_WARPS];
+    __shared__ BinomRows<P> bt;
+    fill_binom_rows<P>(bt);
+    __syncthreads();
+    const double ext = frame->ext;
+    const int warp = threadIdx.x >> 5;
+    MergeShared<P> &sh = shared[warp];
+    for (int l = ltop; l >= 0; --l) {
+        const int lo = level_off.off[l], hi = level_off.off[l + 1];
+        for (int parent = lo + warp; parent < hi; parent += UP_TOP_WARPS)
+            merge_node<P>(parent, nnodes, leafcap, ext, range, cell, tnode, mass, wgt, wxs, wys,
+                          exps, err, bt, sh);
+        __syncthreads();
     }
 }
 
@@ -387,26 +617,49 @@ static int run_upward(Context &c, double *mass, double *w, double *wx, double *w
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     const int sms = sm_count_up();
 
+    k_leaf_setup<<<(int)(((long long)nn * 4 + 255) / 256), 256, 0, c.stream>>>(
+        nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell, tnode, mass, w, wx, wy, frame, err);
+    TC_KERNEL_CHECK();
     static int occ = 0;
     const size_t smem = UP_WARPS * sizeof(LeafShared<P>);
     if (!occ) {
-        TC_CUDA_TRY(cudaFuncSetAttribute(k_upward_leaves<P>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_upward_leaves<P>,
+        TC_CUDA_TRY(cudaFuncSetAttribute(k_leaf_p2e<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+        TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_leaf_p2e<P>,
                                                                   UP_WARPS * 32, smem));
         occ = std::max(occ, 1);
     }
     const int grid = (int)std::min<long long>((nn + UP_WARPS - 1) / UP_WARPS, (long long)sms * occ);
-    k_upward_leaves<P><<<grid, UP_WARPS * 32, smem, c.stream>>>(
-        nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell, tnode, mass, w, wx, wy, exps, frame, err);
+    k_leaf_p2e<P><<<grid, UP_WARPS * 32, smem, c.stream>>>(nn, c.nsrc, c.leafcap, xs, ys, vs,
+                                                         range, cell, tnode, exps);
     TC_KERNEL_CHECK();
-    // inner nodes exist on levels 0 .. LMAX-1; level l occupies [level_off[l], level_off[l+1])
-    for (int l = LMAX - 1; l >= 0; --l) {
+    // Inner nodes exist on levels 0 .. LMAX-1; level l occupies [level_off[l], level_off[l+1]).
+    // Levels 0 .. ltop are all small: they run in one single-block launch after the others.
+    int ltop = -1;
+    while (ltop + 1 < LMAX && c.level_off[ltop + 2] - c.level_off[ltop + 1] <= UP_TOP_MAX_NODES)
+        ++ltop;
+    LevelOffsets offs;
+    for (int l = 0; l < LMAX + 3; ++l) offs.off[l] = c.level_off[l];
+    for (int l = LMAX - 1; l > ltop; --l) {
         const int lo = c.level_off[l], hi = c.level_off[l + 1];
-        if (hi <= lo) continue;
-        const int g = (int)std::min<long long>((hi - lo + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
-        k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(lo, hi, nn, c.leafcap, range, cell,
-                                                             tnode, mass, w, wx, wy, exps, frame, err);
+        const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
+        if (hi <= lo || ninner <= 0) continue;
+        if (ninner >= UP_WIDE_MIN_NODES) {
+            const int g = (int)std::min<long long>(
+                (ninner + UP_WIDE_WARPS * 32 - 1) / (UP_WIDE_WARPS * 32), (long long)sms * 8);
+            k_upward_wide<P><<<g, UP_WIDE_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
+                                                                wx, wy, exps, frame, err);
+        } else {
+            const int g = (int)std::min<long long>((hi - lo + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
+            k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(lo, hi, nn, c.leafcap, range,
+                                                                 cell, tnode, mass, w, wx, wy,
+                                                                 exps, frame, err);
+        }
+        TC_KERNEL_CHECK();
+    }
+    if (ltop >= 0) {
+        k_upward_top<P><<<1, UP_TOP_WARPS * 32, 0, c.stream>>>(
+            ltop, offs, nn, c.leafcap, range, cell, tnode, mass, w, wx, wy, exps, frame, err);
         TC_KERNEL_CHECK();
     }
     return TC_OK;
