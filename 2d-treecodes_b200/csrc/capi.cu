@@ -73,6 +73,16 @@ static unsigned long long stat_counter(Context &c, int slot) {
     return reinterpret_cast<unsigned long long *>(c.h_pinned + 16)[slot];
 }
 
+int device_sm_count() {
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 148;
+    }();
+    return sms;
+}
+
 static int context_init(Context &c, int device, cudaStream_t stream) {
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -365,6 +375,29 @@ TC_API int tc_set_timing(tc_context *ctx, int enabled) {
 }
 
 TC_API void *tc_get_stream(tc_context *ctx) { return ctx ? (void *)ctx->c.stream : nullptr; }
+
+TC_API size_t tc_context_device_bytes(tc_context *ctx) {
+    if (!ctx) return 0;
+    size_t b = 0;
+    for (const auto &d : ctx->c.buf) b += d.bytes;
+    return b;
+}
+
+TC_API int tc_context_trim(tc_context *ctx) {
+    if (!ctx) return TC_ERR_INVALID;
+    Context &c = ctx->c;
+    cudaSetDevice(c.device);
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    for (int s = 0; s < S_NUM_SLOTS; ++s) {
+        if (s == S_ERR || s == S_STATS) continue;   // created with the context, tiny
+        DevBuf &b = c.buf[s];
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    c.nnodes = c.nsrc = 0;
+    return TC_OK;
+}
 
 TC_API int tc_get_stats(tc_context *ctx, tc_stats *out) {
     if (!ctx || !out) return TC_ERR_INVALID;

@@ -620,16 +620,7 @@ __global__ void k_force_gather_parts(int nbricks, const int *__restrict__ offs,
     }
 }
 
-static int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    return sms;
-}
+static int sm_count() { return device_sm_count(); }
 
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
                int nblocks, double *xout, double *yout) {
@@ -697,18 +688,10 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
         TC_KERNEL_CHECK();
     }
-    static int occ[2] = {0, 0};
-    if (!occ[mixed]) {
-        if (mixed)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_force_eval<ORDER_FORCE, true>,
-                                                          EV_WARPS * 32, 0);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_force_eval<ORDER_FORCE, false>,
-                                                          EV_WARPS * 32, 0);
-        if (occ[mixed] <= 0) occ[mixed] = 1;
-    }
+    const int occ = mixed ? blocks_per_sm<k_force_eval<ORDER_FORCE, true>>(EV_WARPS * 32, 0)
+                          : blocks_per_sm<k_force_eval<ORDER_FORCE, false>>(EV_WARPS * 32, 0);
     const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
-                                                (long long)sm_count() * occ[mixed]);
+                                                (long long)sm_count() * occ);
     auto eval = mixed ? k_force_eval<ORDER_FORCE, true> : k_force_eval<ORDER_FORCE, false>;
     phase_mark(c, 6);
     eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(

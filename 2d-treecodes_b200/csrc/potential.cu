@@ -364,16 +364,7 @@ __global__ void k_scale_coeffs_pot(int nnodes, const TNode *__restrict__ tnode,
     }
 }
 
-static int sm_count_p() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    return sms;
-}
+static int sm_count_p() { return device_sm_count(); }
 
 int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out) {
     if (c.order != ORDER_POTENTIAL) {
@@ -446,14 +437,11 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
                c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
         TC_KERNEL_CHECK();
     }
-    static int occ[2] = {0, 0};
     auto eval = mixed ? k_potential_eval<ORDER_POTENTIAL, true> : k_potential_eval<ORDER_POTENTIAL, false>;
-    if (!occ[mixed]) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[mixed], eval, PE_WARPS * 32, 0);
-        if (occ[mixed] <= 0) occ[mixed] = 1;
-    }
+    const int occ = mixed ? blocks_per_sm<k_potential_eval<ORDER_POTENTIAL, true>>(PE_WARPS * 32, 0)
+                          : blocks_per_sm<k_potential_eval<ORDER_POTENTIAL, false>>(PE_WARPS * 32, 0);
     const int egrid = (int)std::min<long long>((ntasks + PE_WARPS - 1) / PE_WARPS,
-                                               (long long)sm_count_p() * occ[mixed]);
+                                               (long long)sm_count_p() * occ);
     phase_mark(c, 6);
     eval<<<egrid, PE_WARPS * 32, 0, c.stream>>>(
         ngroups, m, xt, yt, vo, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),

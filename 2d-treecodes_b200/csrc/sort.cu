@@ -657,12 +657,9 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     TC_KERNEL_CHECK();
     k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
     TC_KERNEL_CHECK();
-    static bool attr = false;
-    if (!attr) {
-        TC_CUDA_TRY(cudaFuncSetAttribute(k_onesweep_xyv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)XYV_SMEM));
-        attr = true;
-    }
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_onesweep_xyv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XYV_SMEM);
+    TC_CUDA_TRY(attr_rc);
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in the sorted arrays");
     for (int p = 0; p < npasses; ++p) {

@@ -110,6 +110,21 @@ int ensure(Context &c, Slot s, size_t count, T **out) {
 template <class T>
 T *slot_ptr(Context &c, Slot s) { return static_cast<T *>(c.buf[s].p); }
 
+// Streaming multiprocessors of the current device (queried once; thread-safe).
+int device_sm_count();
+
+// Resident blocks per SM of a kernel at a block size and dynamic shared memory size, computed
+// once per kernel instance (thread-safe initialisation of a function-local static).
+template <auto Kernel>
+int blocks_per_sm(int threads, size_t smem) {
+    static const int occ = [&] {
+        int o = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, Kernel, threads, smem);
+        return o > 0 ? o : 1;
+    }();
+    return occ;
+}
+
 // ---- sort.cu
 int exclusive_scan(Context &c, const int *d_in, int *d_out, int n);   // d_out has n+1 entries
 int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, int nbits,

@@ -594,16 +594,7 @@ __global__ __launch_bounds__(UP_TOP_WARPS * 32) void k_upward_top(
     }
 }
 
-static int sm_count_up() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    return sms;
-}
+static int sm_count_up() { return device_sm_count(); }
 
 template <int P>
 static int run_upward(Context &c, double *mass, double *w, double *wx, double *wy, double *exps) {
@@ -620,15 +611,11 @@ static int run_upward(Context &c, double *mass, double *w, double *wx, double *w
     k_leaf_setup<<<(int)(((long long)nn * 4 + 255) / 256), 256, 0, c.stream>>>(
         nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell, tnode, mass, w, wx, wy, frame, err);
     TC_KERNEL_CHECK();
-    static int occ = 0;
     const size_t smem = UP_WARPS * sizeof(LeafShared<P>);
-    if (!occ) {
-        TC_CUDA_TRY(cudaFuncSetAttribute(k_leaf_p2e<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-        TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_leaf_p2e<P>,
-                                                                  UP_WARPS * 32, smem));
-        occ = std::max(occ, 1);
-    }
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_leaf_p2e<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    TC_CUDA_TRY(attr_rc);
+    const int occ = blocks_per_sm<k_leaf_p2e<P>>(UP_WARPS * 32, smem);
     const int grid = (int)std::min<long long>((nn + UP_WARPS - 1) / UP_WARPS, (long long)sms * occ);
     k_leaf_p2e<P><<<grid, UP_WARPS * 32, smem, c.stream>>>(nn, c.nsrc, c.leafcap, xs, ys, vs,
                                                          range, cell, tnode, exps);

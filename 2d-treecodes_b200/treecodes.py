@@ -51,9 +51,47 @@ SIGNATURES = {
     "tc_direct_potential_device": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp]),
     "tc_direct_force_device": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp]),
     "tc_sort_sources_noalloc": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "tc_context_device_bytes": (ctypes.c_size_t, [_vp]),
+    "tc_context_trim": (_i, [_vp]),
+    "tc_server_create": (_i, [ctypes.POINTER(_vp), _i, _i, ctypes.c_size_t]),
+    "tc_server_destroy": (None, [_vp]),
+    "tc_server_submit": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "tc_server_wait": (_i, [_vp, ctypes.c_longlong, _vp]),
+    "tc_server_release_client": (_i, [_vp, ctypes.c_longlong]),
+    "tc_server_get_stats": (_i, [_vp, _vp]),
+    "tc_request_footprint": (ctypes.c_size_t, [_i, _i, _i, _i, _i]),
     "tc_measure_fma_peak": (_i, [_i, _dp]),
     "tc_version": (ctypes.c_char_p, []),
 }
+
+REQUEST_POTENTIAL, REQUEST_FORCE_MRAG = 0, 1
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("kind", _i), ("precision", _i), ("theta", _d), ("client", ctypes.c_longlong),
+                ("nsources", _i), ("xsources", _dp), ("ysources", _dp), ("sourcevalues", _dp),
+                ("ntargets", _i), ("xtargets", _dp), ("ytargets", _dp),
+                ("nblocks", _i), ("x0s", _dp), ("y0s", _dp), ("hs", _dp),
+                ("out0", _dp), ("out1", _dp)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("status", _i), ("slot", _i), ("queue_ms", _d), ("service_ms", _d),
+                ("latency_ms", _d), ("footprint_bytes", ctypes.c_size_t)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("evictions", ctypes.c_longlong),
+                ("hbm_budget", ctypes.c_size_t), ("hbm_charged", ctypes.c_size_t),
+                ("hbm_peak", ctypes.c_size_t), ("slots", _i), ("max_in_service", _i),
+                ("resident_clients", _i)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class TreecodeError(RuntimeError):
@@ -261,3 +299,86 @@ class Context:
         out["n"] = nn
         out["order"] = order
         return out
+
+
+    def device_bytes(self):
+        return int(self.lib.tc_context_device_bytes(self.h))
+
+    def trim(self):
+        _check(self.lib.tc_context_trim(self.h))
+
+
+def request_footprint(kind, nsources, ntargets=0, nblocks=0, precision=0):
+    """Device-memory estimate (bytes) the server charges for a request of these sizes."""
+    return int(load().tc_request_footprint(int(kind), int(nsources), int(ntargets), int(nblocks),
+                                           int(precision)))
+
+
+class Server:
+    """The serving loop: concurrent solves on `slots` streams under a device-memory budget.
+
+    ``submit_*`` return a ticket at once; ``wait(ticket)`` returns the outputs with the
+    request's queue / service / latency times.  Host arrays are kept alive here until waited.
+    """
+
+    def __init__(self, slots=4, hbm_budget_bytes=32 << 30, device=-1):
+        self.lib = load()
+        h = _vp()
+        _check(self.lib.tc_server_create(ctypes.byref(h), int(device), int(slots),
+                                         int(hbm_budget_bytes)))
+        self.h = h
+        self._live = {}
+
+    def _submit(self, req, keep, outs):
+        t = ctypes.c_longlong()
+        _check(self.lib.tc_server_submit(self.h, ctypes.byref(req), ctypes.byref(t)))
+        self._live[t.value] = (req, keep, outs)
+        return t.value
+
+    def submit_potential(self, theta, xs, ys, vs, xt, yt, precision=0, client=0):
+        xs, ys, vs, xt, yt = map(_f64, (xs, ys, vs, xt, yt))
+        out = np.empty(len(xt))
+        req = Request(kind=REQUEST_POTENTIAL, precision=int(precision), theta=float(theta),
+                      client=int(client), nsources=len(xs), xsources=_p(xs), ysources=_p(ys),
+                      sourcevalues=_p(vs), ntargets=len(xt), xtargets=_p(xt), ytargets=_p(yt),
+                      out0=_p(out))
+        return self._submit(req, (xs, ys, vs, xt, yt), (out,))
+
+    def submit_force(self, theta, xs, ys, vs, x0s, y0s, hs, precision=0, client=0):
+        xs, ys, vs, x0, y0, h = map(_f64, (xs, ys, vs, x0s, y0s, hs))
+        nt = len(x0) * BLOCKSIZE * BLOCKSIZE
+        xo, yo = np.empty(nt), np.empty(nt)
+        req = Request(kind=REQUEST_FORCE_MRAG, precision=int(precision), theta=float(theta),
+                      client=int(client), nsources=len(xs), xsources=_p(xs), ysources=_p(ys),
+                      sourcevalues=_p(vs), nblocks=len(x0), x0s=_p(x0), y0s=_p(y0), hs=_p(h),
+                      out0=_p(xo), out1=_p(yo))
+        return self._submit(req, (xs, ys, vs, x0, y0, h), (xo, yo))
+
+    def wait(self, ticket):
+        """(outputs tuple, result dict); raises if the solve failed."""
+        res = RequestResult()
+        rc = self.lib.tc_server_wait(self.h, ctypes.c_longlong(ticket), ctypes.byref(res))
+        _, _, outs = self._live.pop(ticket)
+        if rc != 0:
+            raise TreecodeError(f"request {ticket} failed with status {rc}")
+        return outs, res.as_dict()
+
+    def release_client(self, client):
+        _check(self.lib.tc_server_release_client(self.h, ctypes.c_longlong(client)))
+
+    def stats(self):
+        s = ServerStats()
+        _check(self.lib.tc_server_get_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tc_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

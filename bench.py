@@ -63,6 +63,12 @@ def parse_args():
     p.add_argument("--single", action="store_true",
                    help="only `warmup` + `steps` device solves and a timing line (for profilers)")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    p.add_argument("--serving-requests", type=int, default=400,
+                   help="requests of the serving stream (the full stream has 2000)")
+    p.add_argument("--serving-rate", type=float, default=200.0, help="Poisson arrival rate, 1/s")
+    p.add_argument("--serving-slots", type=int, default=4)
+    p.add_argument("--serving-budget-gb", type=float, default=40.0)
+    p.add_argument("--no-serving", action="store_true")
     return p.parse_args()
 
 
@@ -460,6 +466,11 @@ def run_b200(args, ws, rank, local):
             cpu = {"value": None, "unit": "Mtargets/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"unavailable: {exc}"}
 
+    # ---- serving stream (N = 1): the same stream in the mixed and the plain FP64 form
+    serving = None
+    if ws == 1 and not args.no_serving and args.serving_requests > 0:
+        serving = run_serving(args, T)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mtargets/s", "n_gpus": ws,
@@ -479,10 +490,34 @@ def run_b200(args, ws, rank, local):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": launches,
+            "serving": serving,
         }
         print(json.dumps(line))
     ctx.close()
     return 0
+
+
+def run_serving(args, T):
+    """The serving stream on a request server: p50/p99 latency from arrival and aggregate
+    Mtargets/s, mixed and plain FP64 on the same seeded stream."""
+    import serving as S
+    specs = S.make_stream(nreq=args.serving_requests, rate_hz=args.serving_rate)
+    out = {"config": {"requests": len(specs), "rate_hz": args.serving_rate,
+                      "slots": args.serving_slots, "hbm_budget_gb": args.serving_budget_gb,
+                      "sources": "log-uniform [2^12, 2^22]", "force_share": 0.7,
+                      "followup_share": 0.2, "theta": list(S.THETAS),
+                      "distributions": list(S.DISTRIBUTIONS),
+                      "latency": "scheduled arrival to completion (host clock)"}}
+    for precision, name in ((1, "mixed"), (0, "fp64")):
+        m = S.Materialiser()
+        srv = T.Server(slots=args.serving_slots,
+                       hbm_budget_bytes=int(args.serving_budget_gb * (1 << 30)))
+        try:
+            summary, _ = S.run_stream(srv, specs, precision, m)
+        finally:
+            srv.close()
+        out[name] = summary
+    return out
 
 
 def main():

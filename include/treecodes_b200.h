@@ -178,6 +178,70 @@ TC_API int tc_sort_sources_noalloc(const double *xsources, const double *ysource
                                    int *perm, double *xsorted, double *ysorted, double *vsorted,
                                    double *frame, void *cuda_stream);
 
+/* Device memory held by a context's grow-only buffers, in bytes. */
+TC_API size_t tc_context_device_bytes(tc_context *ctx);
+/* Frees a context's device buffers; the next solve on it allocates them again. */
+TC_API int tc_context_trim(tc_context *ctx);
+
+/* ---- serving loop ---------------------------------------------------------------------
+ * A request server on one GPU: solves submitted from any thread are queued, admitted in
+ * arrival order as execution slots and device memory free up, and run concurrently, one
+ * context (and CUDA stream) per slot or per resident client, so the work of admitted requests
+ * overlaps on the device.  Admission charges each request's device-memory footprint (estimated
+ * from its sizes, corrected by the context's actual size once known) against a budget; idle
+ * resident clients are released, least recently used first, when a request does not fit.
+ * A request with client > 0 runs on that client's own context, whose device buffers (sorted
+ * sources, tree, expansions, interaction lists, staged inputs) stay resident between its
+ * requests; requests of one client run one at a time in submission order.  Results are the
+ * same as those of a solve on its own context (the kernels are deterministic). */
+typedef struct tc_server tc_server;
+
+typedef enum { TC_REQUEST_POTENTIAL = 0, TC_REQUEST_FORCE_MRAG = 1 } tc_request_kind;
+
+typedef struct {
+    int kind;                       /* tc_request_kind */
+    int precision;                  /* tc_precision */
+    double theta;
+    long long client;               /* > 0: resident client id; 0: one-off request */
+    int nsources;
+    const double *xsources, *ysources, *sourcevalues;   /* host arrays */
+    int ntargets;                   /* potential */
+    const double *xtargets, *ytargets;
+    int nblocks;                    /* force_mrag */
+    const double *x0s, *y0s, *hs;
+    double *out0;                   /* potential: values; force_mrag: x components */
+    double *out1;                   /* force_mrag: y components */
+} tc_request;                       /* all arrays must stay valid until the request completes */
+
+typedef struct {
+    int status;                     /* tc_status of the solve */
+    int slot;                       /* execution slot that ran it */
+    double queue_ms;                /* submission to admission */
+    double service_ms;              /* admission to completion */
+    double latency_ms;              /* submission to completion */
+    size_t footprint_bytes;         /* device memory charged at admission */
+} tc_request_result;
+
+typedef struct {
+    long long submitted, completed, failed, evictions;
+    size_t hbm_budget, hbm_charged, hbm_peak;
+    int slots, max_in_service, resident_clients;
+} tc_server_stats;
+
+/* slots: concurrent solves (>= 1); hbm_budget_bytes: device memory the server may hold. */
+TC_API int tc_server_create(tc_server **srv, int device, int slots, size_t hbm_budget_bytes);
+/* Waits for all submitted requests, then frees every context. */
+TC_API void tc_server_destroy(tc_server *srv);
+TC_API int tc_server_submit(tc_server *srv, const tc_request *req, long long *ticket);
+/* Blocks until the request has completed; each ticket is waited for once. */
+TC_API int tc_server_wait(tc_server *srv, long long ticket, tc_request_result *result);
+/* Releases a resident client's device memory once its queued requests are done. */
+TC_API int tc_server_release_client(tc_server *srv, long long client);
+TC_API int tc_server_get_stats(tc_server *srv, tc_server_stats *out);
+/* Device-memory estimate used for admission (bytes) of a request of the given sizes. */
+TC_API size_t tc_request_footprint(int kind, int nsources, int ntargets, int nblocks,
+                                   int precision);
+
 /* Measured FMA throughput of the current device in TFLOP/s (fp64 != 0: FP64, else FP32). */
 TC_API int tc_measure_fma_peak(int fp64, double *tflops);
 

@@ -1,0 +1,123 @@
+"""GPU tests of the serving loop (tc_server_*): a request stream runs with several solves in
+flight on separate streams, under a device-memory budget, with resident clients; every result
+must equal the same request solved alone on a fresh context (tolerance 0: the kernels are
+deterministic, so the mix may not change a single bit)."""
+import numpy as np
+import pytest
+
+import serving as S
+import treecodes as T
+
+pytestmark = pytest.mark.gpu
+
+LOG2_MAX = 16
+
+
+@pytest.fixture(scope="module")
+def materialiser():
+    return S.Materialiser(log2_max=LOG2_MAX, seed=77)
+
+
+def solo(spec, data, precision):
+    ctx = T.Context(device=0, precision=precision)
+    try:
+        if spec["kind"] == "potential":
+            return (ctx.potential_host(spec["theta"], data["xs"], data["ys"], data["vs"],
+                                       data["xt"], data["yt"]),)
+        return ctx.force_mrag_host(spec["theta"], data["xs"], data["ys"], data["vs"],
+                                   data["x0s"], data["y0s"], data["hs"])
+    finally:
+        ctx.close()
+
+
+def replay_solo(specs, precision):
+    m = S.Materialiser(log2_max=LOG2_MAX, seed=77)
+    return [solo(s, m(s), precision) for s in specs]
+
+
+def assert_same(mixed_outs, solo_outs):
+    for i, (a, b) in enumerate(zip(mixed_outs, solo_outs)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), f"request {i}: result differs from the solo solve"
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_stream_results_equal_solo(precision):
+    specs = S.make_stream(nreq=48, rate_hz=5000.0, seed=31 + precision, log2_min=10,
+                          log2_max=LOG2_MAX, followup_share=0.3)
+    m = S.Materialiser(log2_max=LOG2_MAX, seed=77)
+    srv = T.Server(slots=4, hbm_budget_bytes=8 << 30, device=0)
+    try:
+        summary, outs = S.run_stream(srv, specs, precision, m, keep_outputs=True)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(specs) and st["failed"] == 0
+    assert st["max_in_service"] > 1, "no two solves were ever in service together"
+    assert any(s["followup"] for s in specs)
+    assert_same(outs, replay_solo(specs, precision))
+    assert summary["p99_ms"] >= summary["p50_ms"] > 0
+
+
+def test_budget_limits_concurrency_and_evicts():
+    specs = S.make_stream(nreq=24, rate_hz=5000.0, seed=41, log2_min=14, log2_max=LOG2_MAX,
+                          followup_share=0.4)
+    biggest = max(T.request_footprint(1 if s["kind"] == "force" else 0, s["n"],
+                                      s["n"], max(1, round((s["n"] / 2048) ** 0.5)) ** 2, 1)
+                  for s in specs)
+    budget = int(biggest * 1.6)
+    m = S.Materialiser(log2_max=LOG2_MAX, seed=77)
+    srv = T.Server(slots=4, hbm_budget_bytes=budget, device=0)
+    try:
+        _, outs = S.run_stream(srv, specs, 1, m, keep_outputs=True)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["failed"] == 0
+    assert st["hbm_peak"] <= budget
+    assert st["max_in_service"] <= 4
+    assert_same(outs, replay_solo(specs, 1))
+
+
+def test_oversize_request_fails_cleanly(materialiser):
+    spec = dict(kind="force", n=1 << 14, dist="uniform", theta=0.5, off=0, followup=False,
+                step=0, client=1, noise_off=0, last_step=0, resident=False, t=0.0)
+    data = materialiser(spec)
+    srv = T.Server(slots=2, hbm_budget_bytes=1 << 20, device=0)
+    try:
+        t = S.submit(srv, spec, data, 0)
+        with pytest.raises(T.TreecodeError, match="status 3"):
+            srv.wait(t)
+        # the server keeps serving requests that fit
+        srv2 = T.Server(slots=1, hbm_budget_bytes=4 << 30, device=0)
+        try:
+            t2 = S.submit(srv2, spec, data, 0)
+            outs, res = srv2.wait(t2)
+            assert res["status"] == 0
+            assert_same([outs], [solo(spec, data, 0)])
+        finally:
+            srv2.close()
+    finally:
+        srv.close()
+
+
+def test_resident_client_steps_in_order_and_release(materialiser):
+    base = dict(kind="potential", n=5000, dist="gaussian_mixture", theta=0.5, off=123,
+                followup=False, step=0, client=9, noise_off=0, last_step=3, resident=True,
+                t=0.0)
+    steps = [dict(base, step=k, followup=k > 0, noise_off=1000 * k) for k in range(4)]
+    m = S.Materialiser(log2_max=LOG2_MAX, seed=77)
+    datas = [m(s) for s in steps]
+    srv = T.Server(slots=3, hbm_budget_bytes=4 << 30, device=0)
+    try:
+        tickets = [S.submit(srv, s, d, 1) for s, d in zip(steps, datas)]
+        outs = [srv.wait(t)[0] for t in tickets]
+        st = srv.stats()
+        assert st["resident_clients"] == 1
+        srv.release_client(9)
+        assert srv.stats()["resident_clients"] == 0
+    finally:
+        srv.close()
+    assert_same(outs, [solo(s, d, 1) for s, d in zip(steps, datas)])
+    # the steps differ (each advects the previous one), so order mattered
+    assert not np.array_equal(outs[0][0], outs[1][0])
