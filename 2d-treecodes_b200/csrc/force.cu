@@ -15,10 +15,13 @@
 //    r_brick = 4.949747468305833 h), so every decision is the reference's.
 // 2. exclusive scan of the 3 x nbricks counts -> list offsets (E2L | E2P | P2P lists).
 // 3. k_force_lists<true>: same walk, writes node ids into the lists.
-// 4. k_force_eval: one warp per brick, 2 targets per lane; local expansion from the E2L list
-//    (lane l owns coefficient l), L2P, E2P from the E2P list, P2P over the leaves of the P2P
-//    list with source tiles staged in shared memory; results written straight into the
-//    ix + 32*(iy + 32*ib) layout (treecode-force.cpp:191-197).
+// 4. k_force_eval: persistent warps take evaluation tasks from an atomic counter; a task is a
+//    brick's far field plus its first P2P_SEG near-field sources, or a further P2P_SEG-source
+//    segment of its near field.  2 targets per lane; local expansion from the E2L list (lane l
+//    owns coefficient l), L2P, E2P from the E2P list, P2P over the leaves of the P2P list with
+//    source tiles staged in shared memory.  Single-task bricks write straight into the
+//    ix + 32*(iy + 32*ib) layout (treecode-force.cpp:191-197); the parts of multi-task bricks
+//    are added in task order by k_force_gather_parts, so results are deterministic.
 #include <cfloat>
 
 #include "tc_internal.h"
@@ -203,7 +206,6 @@ __device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
     lo = (float)(v - (double)hi);
 }
 
-// z^e for e = 1..31 by binary powering
 // MIXED = false: plain FP64.  MIXED = true: P2P and E2P in FP32 (float offsets from the brick
 // corner split into hi + lo parts, scaled multipole coefficients, compensated per-target
 // sums); the local expansion (E2L, L2P) stays FP64.

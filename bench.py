@@ -63,6 +63,7 @@ def parse_args():
     p.add_argument("--single", action="store_true",
                    help="only `warmup` + `steps` device solves and a timing line (for profilers)")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    p.add_argument("--theta", type=float, default=None, help="override the workload's theta")
     p.add_argument("--serving-requests", type=int, default=400,
                    help="requests of the serving stream (the full stream has 2000)")
     p.add_argument("--serving-rate", type=float, default=200.0, help="Poisson arrival rate, 1/s")
@@ -72,11 +73,15 @@ def parse_args():
     return p.parse_args()
 
 
-def make_workload(name, seed_offset=0):
+def make_workload(name, seed_offset=0, theta=None):
     fn = workloads.WORKLOADS[name]
     import inspect
     seed = inspect.signature(fn).parameters["seed"].default + seed_offset
-    return fn(seed=seed)
+    w = fn(seed=seed)
+    if theta is not None:
+        w["theta"] = float(theta)
+        w["name"] += f"_theta{theta:g}"
+    return w
 
 
 def n_targets(w):
@@ -95,7 +100,8 @@ def dist_setup(args):
         backend = "nccl" if torch.cuda.is_available() and args.impl == "b200" else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+        # a short timeout: a rank that never arrives ends the others' collective with an error
+        dist.init_process_group(backend, timeout=timedelta(seconds=60))
     return ws, rank, local
 
 
@@ -171,10 +177,15 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------- roofline
-def algorithmic_flops(stats, p=ORDER_FORCE):
-    """Per-solve flops of the evaluation kernel with fixed per-unit weights: P2P 11 per pair
-    (1 division), E2P 16p+8 per (target, cell), E2L 4p^2+20p per (brick, cell), L2P 10p per
-    target."""
+def algorithmic_flops(stats, kind="force"):
+    """Per-solve flops of the evaluation kernel with fixed per-unit weights.  force_mrag (p=24):
+    P2P 11 per pair (1 division), E2P 16p+8 per (target, cell), E2L 4p^2+20p per (brick, cell),
+    L2P 10p per target.  potential (p=12): P2P 8 per pair (1 log), E2P 10p+8 per (target,
+    cell)."""
+    if kind == "potential":
+        p = 12
+        return 8.0 * stats["p2p_pairs"] + (10 * p + 8) * stats["e2p_pairs"]
+    p = ORDER_FORCE
     return (11.0 * stats["p2p_pairs"] + (16 * p + 8) * stats["e2p_pairs"]
             + (4 * p * p + 20 * p) * stats["e2l_pairs"] + 10.0 * p * stats["l2p_targets"])
 
@@ -193,27 +204,16 @@ def read_profile_traffic(mixed):
 
 
 # ------------------------------------------------------------------------------- CPU reference
-def cpu_reference_step(w, sample_blocks=512, threads=None):
-    """One bounded step of the reference's CPU implementation (oracle/_ref: the reference's
-    drivers compiled verbatim + the restated ISPC kernels, node capacity raised for large
-    inputs): the full tree build plus the evaluation of `sample_blocks` evenly strided blocks,
-    extrapolated linearly to all blocks.  Returns (seconds for the full workload, description).
-    """
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O  # the checker / CPU baseline only
-    nb = len(w["x0s"])
-    stride = max(1, nb // sample_blocks)
-    idx = np.arange(0, nb, stride)[:sample_blocks]
+def _capture_stdout(fn):
+    """Runs fn() with file descriptor 1 redirected to a temporary file; returns (result, text).
+    The reference's force driver prints per-thread and phase timers on stdout."""
     libc = ctypes.CDLL(None)
     log = tempfile.TemporaryFile(mode="w+b")
     saved = os.dup(1)
     try:
         sys.stdout.flush()
-        os.dup2(log.fileno(), 1)   # the reference's force driver prints its own phase timers
-        t0 = time.perf_counter()
-        O.force_mrag(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"][idx], w["y0s"][idx],
-                     w["hs"][idx], mode="big")
-        t1 = time.perf_counter()
+        os.dup2(log.fileno(), 1)
+        out = fn()
         libc.fflush(None)
     finally:
         os.dup2(saved, 1)
@@ -221,13 +221,55 @@ def cpu_reference_step(w, sample_blocks=512, threads=None):
     log.seek(0)
     text = log.read().decode(errors="replace")
     log.close()
+    return out, text
+
+
+def cpu_reference_step(w, sample_blocks=512, sample_targets=1 << 19):
+    """One bounded step of the reference's CPU implementation (oracle/_ref: the reference's
+    drivers compiled verbatim + the restated ISPC kernels, node capacity raised for large
+    inputs, OpenMP on every host core).  force_mrag: the full tree build plus the evaluation of
+    `sample_blocks` evenly strided blocks, the evaluation (the driver's own DW timer) scaled to
+    all blocks.  potential: the tree build alone (no targets) and the build plus an evenly
+    strided sample of `sample_targets` targets; the difference is scaled to all targets.
+    Returns (seconds for the full workload, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the checker / CPU baseline only
+    if w["kind"] == "potential":
+        m = len(w["xt"])
+        stride = max(1, m // sample_targets)
+        idx = np.arange(0, m, stride)[:sample_targets]
+
+        def run(ix):
+            t0 = time.perf_counter()
+            O.potential(w["theta"], w["xs"], w["ys"], w["vs"], w["xt"][ix], w["yt"][ix],
+                        mode="big")
+            return time.perf_counter() - t0
+
+        build = run(idx[:0])
+        sample = run(idx)
+        evals = max(sample - build, 0.0)
+        full = build + evals * m / len(idx)
+        desc = (f"tree build of all {len(w['xs'])} sources ({build:.3f} s, timed alone) + "
+                f"evaluation of {len(idx)} of {m} targets (every {stride}th; {evals:.3f} s) "
+                f"scaled by {m}/{len(idx)}")
+        return full, desc
+    nb = len(w["x0s"])
+    stride = max(1, nb // sample_blocks)
+    idx = np.arange(0, nb, stride)[:sample_blocks]
+
+    def run():
+        t0 = time.perf_counter()
+        O.force_mrag(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"][idx], w["y0s"][idx],
+                     w["hs"][idx], mode="big")
+        return time.perf_counter() - t0
+
+    wall, text = _capture_stdout(run)
     # drivers/treecode-force.cpp:234 prints "UP: <s>s DW: <s>s" (tree build + upward pass,
     # then the evaluation of the requested blocks)
-    m = re.findall(r"UP:\s*([0-9.eE+-]+)s\s+DW:\s*([0-9.eE+-]+)s", text)
-    if not m:
+    mt = re.findall(r"UP:\s*([0-9.eE+-]+)s\s+DW:\s*([0-9.eE+-]+)s", text)
+    if not mt:
         raise RuntimeError("the reference driver printed no UP/DW timers")
-    evals = float(m[-1][1])
-    wall = t1 - t0
+    evals = float(mt[-1][1])
     build = wall - evals
     full = build + evals * nb / len(idx)
     desc = (f"tree build + upward pass of all {len(w['xs'])} sources, evaluation of {len(idx)} "
@@ -240,11 +282,7 @@ def cpu_reference_step(w, sample_blocks=512, threads=None):
 def run_reference(args, ws, rank):
     if rank != 0:
         return 0
-    w = make_workload(args.workload)
-    if w["kind"] != "force":
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "the reference arm is implemented for the force_mrag workloads"}))
-        return 0
+    w = make_workload(args.workload, theta=args.theta)
     cores = os.cpu_count()
     for _ in range(args.warmup):
         cpu_reference_step(w)
@@ -260,9 +298,9 @@ def run_reference(args, ws, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded PCG64)",
-        "config": {"workload": w["name"], "theta": w["theta"], "order": ORDER_FORCE,
-                   "sources": len(w["xs"]), "targets": n_targets(w), "precision": "fp64",
-                   "l2": "inputs larger than L2 (384 MB of sources)"},
+        "config": {"workload": w["name"], "theta": w["theta"],
+                   "order": ORDER_FORCE if w["kind"] == "force" else 12,
+                   "sources": len(w["xs"]), "targets": n_targets(w), "precision": "fp64"},
         "cpu_baseline": {"value": val, "unit": "Mtargets/s", "cores": cores, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": val, "unit": "Mtargets/s", "h2d_bytes_per_step": 0,
@@ -282,7 +320,7 @@ def run_b200(args, ws, rank, local):
         raise SystemExit("bench.py needs a CUDA GPU")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    w = make_workload(args.workload, seed_offset=rank)
+    w = make_workload(args.workload, seed_offset=rank, theta=args.theta)
     kind = w["kind"]
     mixed = args.precision == "mixed"
     ctx = T.Context(device=local, precision=1 if mixed else 0)
@@ -312,6 +350,11 @@ def run_b200(args, ws, rank, local):
         ctx.close()
         return 0
 
+    in_bytes = sum(int(a.nbytes) for a in w.values() if isinstance(a, np.ndarray))
+    l2_bytes = 126 << 20
+    flush = (torch.zeros((2 * l2_bytes) // 8, dtype=torch.float64, device=dev)
+             if in_bytes < 2 * l2_bytes else None)
+
     def timed(precision, steps, sample_clocks=False):
         """Device time per step of `steps` solves (CUDA events on the library's stream, max over
         ranks), after warm-up; returns (ms, kernel launches, clock record)."""
@@ -326,17 +369,33 @@ def run_b200(args, ws, rank, local):
             time.sleep(0.3)
         barrier(ws)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
         launches = 0
-        for _ in range(steps):
-            solve()
-            launches += ctx.stats()["launches"]
-        e1.record(stream)
-        torch.cuda.synchronize()
+        if flush is None:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                solve()
+                launches += ctx.stats()["launches"]
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total = e0.elapsed_time(e1)
+        else:
+            # inputs smaller than L2: every timed step starts after a write of a buffer twice
+            # the L2 size, outside the events
+            total = 0.0
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.add_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                solve()
+                e1.record(stream)
+                launches += ctx.stats()["launches"]
+                torch.cuda.synchronize()
+                total += e0.elapsed_time(e1)
         barrier(ws)
         clocks = sampler.stop() if sampler else None
-        return max_over_ranks(e0.elapsed_time(e1) / steps, ws, dev), launches, clocks
+        return max_over_ranks(total / steps, ws, dev), launches, clocks
 
     def phases(precision):
         """Phase times of one solve (events inside the library) and its work counters."""
@@ -388,18 +447,17 @@ def run_b200(args, ws, rank, local):
     ctx.set_precision(prec)
 
     # ---- dominant kernel: the evaluation launch, timed by events on the library's stream
-    roofline = None
-    if kind == "force":
-        flops = algorithmic_flops(st)
-        peak = T.measure_fma_peak(not mixed)
-        achieved = flops / (st["eval_kernel_ms"] * 1e-3) / 1e12
-        roofline = {"kernel": "k_force_eval", "bound": "fp32" if mixed else "fp64",
-                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": read_profile_traffic(mixed),
-                    "peak_source": ("measured %s FMA throughput of this GPU (tc_measure_fma_peak)"
-                                    % ("FP32" if mixed else "FP64")),
-                    "algorithmic_flops_per_launch": flops, "launch_ms": st["eval_kernel_ms"],
-                    "phase_ms": {k: st[k] for k in PHASES}}
+    flops = algorithmic_flops(st, kind)
+    peak = T.measure_fma_peak(not mixed)
+    achieved = flops / (st["eval_kernel_ms"] * 1e-3) / 1e12
+    roofline = {"kernel": "k_force_eval" if kind == "force" else "k_potential_eval",
+                "bound": "fp32" if mixed else "fp64",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": read_profile_traffic(mixed) if w["name"].startswith("vortex_sheet_force") else None,
+                "peak_source": ("measured %s FMA throughput of this GPU (tc_measure_fma_peak)"
+                                % ("FP32" if mixed else "FP64")),
+                "algorithmic_flops_per_launch": flops, "launch_ms": st["eval_kernel_ms"],
+                "phase_ms": {k: st[k] for k in PHASES}}
 
     # ---- end to end through the C ABI with pinned host buffers (host -> device copies and the
     # read-back of the results inside the timed region)
@@ -457,7 +515,7 @@ def run_b200(args, ws, rank, local):
 
     # ---- CPU baseline (rank 0, N = 1)
     cpu = None
-    if rank == 0 and ws == 1 and kind == "force" and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             t_full, desc = cpu_reference_step(w)
             cpu = {"value": m / t_full / 1e6, "unit": "Mtargets/s", "cores": os.cpu_count(),
@@ -482,7 +540,9 @@ def run_b200(args, ws, rank, local):
                        "order": ORDER_FORCE if kind == "force" else 12,
                        "sources": len(w["xs"]), "targets": m, "precision": args.precision,
                        "parallelism": f"{ws} independent solves (one per GPU)",
-                       "l2": "inputs larger than L2 (384 MB of sources per step)"},
+                       "l2": (f"inputs larger than L2 ({in_bytes / 1e6:.0f} MB per step)"
+                              if flush is None else
+                              f"L2 flushed before every timed step (inputs {in_bytes / 1e6:.1f} MB)")},
             "accuracy": acc,
             "plain_fp64": other,
             "e2e": e2e,

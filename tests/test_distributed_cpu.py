@@ -1,0 +1,72 @@
+"""Multi-process checks of the N > 1 path on the CPU (gloo, world size 2).
+
+bench.py runs one rank per GPU; ranks solve independent workloads (weak scaling, no data-path
+collective), meet at barriers around the timed region and reduce their timings with a MAX.
+These tests run the same helpers on gloo ranks, and the reference arm under torchrun, where
+only rank 0 works and prints."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, ws, port, out):
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(ws))
+    sys.path.insert(0, ROOT)
+    import bench
+    dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+    try:
+        bench.barrier(ws)
+        t = bench.max_over_ranks(1.5 + rank, ws)
+        w = bench.make_workload("uniform_potential", seed_offset=rank)
+        out.put((rank, t, float(w["xs"][0])))
+        bench.barrier(ws)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_barrier_and_max_over_ranks():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r for r, _, _ in res] == [0, 1]
+    assert all(t == 2.5 for _, t, _ in res)          # the max over ranks, on every rank
+    assert res[0][2] != res[1][2]                     # each rank solves its own inputs
+
+
+def test_reference_arm_under_torchrun():
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_potential_big.so")):
+        pytest.skip("the compiled reference (oracle/_ref) is not built")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+           "--master-addr=127.0.0.1", f"--master-port={_free_port()}", "bench.py", "--impl",
+           "reference", "--gpus", "2", "--workload", "uniform_potential", "--steps", "1",
+           "--warmup", "1"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = lines[0]
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference"
