@@ -40,12 +40,34 @@ __global__ __launch_bounds__(BBOX_THREADS) void k_bbox(const double *__restrict_
                                                        double4 *partials, unsigned *done,
                                                        Frame *frame) {
     double xmi = 1e13, xma = 0, ymi = 1e13, yma = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double xv = x[i], yv = y[i];
+    auto take = [&](double xv, double yv) {
         xmi = fmin(xmi, xv);
         xma = fmax(xma, xv);
         ymi = fmin(ymi, yv);
         yma = fmax(yma, yv);
+    };
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0) {
+        // 16-byte loads, two pairs per thread in flight
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        const double2 *y2 = reinterpret_cast<const double2 *>(y);
+        const int n2 = n / 2;
+        int i = gid;
+        for (; i + stride < n2; i += 2 * stride) {
+            const double2 a = x2[i], b = y2[i], c = x2[i + stride], e = y2[i + stride];
+            take(a.x, b.x);
+            take(a.y, b.y);
+            take(c.x, e.x);
+            take(c.y, e.y);
+        }
+        if (i < n2) {
+            const double2 a = x2[i], b = y2[i];
+            take(a.x, b.x);
+            take(a.y, b.y);
+        }
+        if ((n & 1) && gid == 0) take(x[n - 1], y[n - 1]);
+    } else {
+        for (int i = gid; i < n; i += stride) take(x[i], y[i]);
     }
     warp_minmax(xmi, xma, ymi, yma);
     __shared__ double4 s[BBOX_THREADS / 32];
@@ -177,6 +199,45 @@ __global__ __launch_bounds__(256) void k_hist(const int *__restrict__ keys, int 
     }
 }
 
+// Morton keys of the sources and the histograms of every 8-bit digit of them, in one pass
+// (k_keys followed by k_hist, without reading the keys back).
+__global__ __launch_bounds__(256) void k_keys_hist(const double *__restrict__ x,
+                                                   const double *__restrict__ y, int n,
+                                                   const Frame *__restrict__ frame,
+                                                   int *__restrict__ keys, int npasses,
+                                                   int *__restrict__ hist) {
+    __shared__ int s[RS_MAX_PASSES][RS_RADIX];
+    for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
+    __syncthreads();
+    const Frame f = *frame;
+    auto key_of = [&](double xv, double yv) {
+        const int k = spread_bits(quantize(xv, f.xmin, f.scale)) |
+                      (spread_bits(quantize(yv, f.ymin, f.scale)) << 1);
+        for (int p = 0; p < npasses; ++p) atomicAdd(&s[p][((unsigned)k >> (8 * p)) & 0xFF], 1);
+        return k;
+    };
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0 &&
+        (reinterpret_cast<uintptr_t>(keys) & 7) == 0) {
+        // 16-byte loads and 8-byte stores: two sources per thread and step
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        const double2 *y2 = reinterpret_cast<const double2 *>(y);
+        int2 *k2 = reinterpret_cast<int2 *>(keys);
+        for (int i = gid; i < n / 2; i += stride) {
+            const double2 a = x2[i], b = y2[i];
+            k2[i] = make_int2(key_of(a.x, b.x), key_of(a.y, b.y));
+        }
+        if ((n & 1) && gid == 0) keys[n - 1] = key_of(x[n - 1], y[n - 1]);
+    } else {
+        for (int i = gid; i < n; i += stride) keys[i] = key_of(x[i], y[i]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npasses * RS_RADIX; i += blockDim.x) {
+        const int c = (&s[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
 // Block-wide exclusive scan of one int per thread (blockDim.x a multiple of 32, <= 1024).
 __device__ int block_exclusive_scan(int v, int *total) {
     __shared__ int warp_sums[32];
@@ -212,6 +273,30 @@ __global__ __launch_bounds__(RS_RADIX) void k_hist_scan(const int *__restrict__ 
 
 __device__ __forceinline__ unsigned ld_volatile(const unsigned *p) {
     return *(const volatile unsigned *)p;
+}
+
+// Exclusive prefix of digit d over the tiles before `tile` (decoupled look-back): walk back
+// over the predecessors' statuses, adding aggregates, until the first inclusive prefix.  A
+// predecessor that has published nothing yet is read again; the number of such reads is
+// bounded (DEVERR_SPIN_LIMIT).  (Reading several predecessors per step measured slower.)
+__device__ __forceinline__ int lookback(const unsigned *status, int tile, int d, unsigned *err) {
+    int excl = 0;
+    int spins = 0;
+    for (int j = tile - 1; j >= 0;) {
+        const unsigned s = ld_volatile(status + (size_t)j * RS_RADIX + d);
+        const unsigned flag = s & ~RS_VALMASK;
+        if (flag == 0) {
+            if (++spins > RS_SPIN_LIMIT) {
+                atomicOr(err, DEVERR_SPIN_LIMIT);
+                break;
+            }
+            continue;
+        }
+        excl += (int)(s & RS_VALMASK);
+        if (flag == RS_FLAG_INC) break;
+        --j;
+    }
+    return excl;
 }
 
 __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
@@ -278,22 +363,7 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
         atomicExch(mine, RS_FLAG_INC | (unsigned)total);
     } else {
         atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
-        int j = tile - 1;
-        int spins = 0;
-        while (j >= 0) {
-            const unsigned s = ld_volatile(status + (size_t)j * RS_RADIX + d);
-            const unsigned flag = s & ~RS_VALMASK;
-            if (flag == 0) {
-                if (++spins > RS_SPIN_LIMIT) {
-                    atomicOr(err, DEVERR_SPIN_LIMIT);
-                    break;
-                }
-                continue;
-            }
-            excl += (int)(s & RS_VALMASK);
-            if (flag == RS_FLAG_INC) break;
-            --j;
-        }
+        excl = lookback(status, tile, d, err);
         atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
     }
 
@@ -331,15 +401,34 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
     }
 }
 
-// The same pass for the sources, carrying their coordinates and values along with the key and
-// the input index, so that the sorted x/y/v come out of the last pass without a random gather
-// (which costs ~300 B of DRAM traffic per source on HBM, against 24 + 24 B here).  The local
-// reordering goes through one shared buffer, one component at a time.
-constexpr size_t XYV_SMEM = (size_t)RS_TILE * sizeof(int) + (size_t)RS_TILE * sizeof(double) +
-                            (size_t)RS_WARPS * RS_RADIX * sizeof(int) + 2 * RS_RADIX * sizeof(int) +
+// L2 prefetch of [p, p + bytes) rounded inwards to 16-byte bounds (a hint: no data moves to
+// the SM, nothing is written).
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a))
+                     : "memory");
+}
+
+// The same pass for the sources, carrying the input index, coordinates and values along with
+// the key, so that the sorted x/y/v come out of the last pass without a random gather over the
+// whole array (~300 B of DRAM traffic per source on HBM, against 28 + 28 B here).
+//   * tiles of 2048 sources, 256 threads, 8 items per thread; three CTAs fit one SM;
+//   * at the start of a tile one thread asks for the tile's index/x/y/v ranges to be brought
+//     into L2 (cp.async.bulk.prefetch), so their DRAM latency overlaps ranking and look-back;
+//   * once the local positions are known every item's index, x, y and v are loaded together
+//     (32 loads in flight per thread, served by L2) and placed in sorted order in shared memory;
+//   * one output loop writes all five arrays, slot j going to s_global[digit] + j.
+constexpr int XYV_THREADS = 256;
+constexpr int XYV_WARPS = XYV_THREADS / 32;
+constexpr int XYV_ITEMS = 8;
+constexpr int XYV_TILE = XYV_THREADS * XYV_ITEMS;
+constexpr size_t XYV_SMEM = (size_t)XYV_TILE * (2 * sizeof(int) + 3 * sizeof(double)) +
+                            (size_t)XYV_WARPS * RS_RADIX * sizeof(int) + 2 * RS_RADIX * sizeof(int) +
                             16;
 
-__global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
+__global__ __launch_bounds__(XYV_THREADS) void k_onesweep_xyv(
     const int *__restrict__ keys_in, const int *__restrict__ idx_in,
     const double *__restrict__ x_in, const double *__restrict__ y_in,
     const double *__restrict__ v_in, int *__restrict__ keys_out, int *__restrict__ idx_out,
@@ -347,26 +436,34 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
     int shift, const int *__restrict__ digit_offsets, unsigned *status, int *tile_counter,
     unsigned *err) {
     extern __shared__ __align__(16) unsigned char xyv_smem[];
-    int *s_keys = reinterpret_cast<int *>(xyv_smem);
-    double *s_buf = reinterpret_cast<double *>(xyv_smem + RS_TILE * sizeof(int));
-    int *s_ibuf = reinterpret_cast<int *>(s_buf);
-    int(*s_whist)[RS_RADIX] = reinterpret_cast<int(*)[RS_RADIX]>(
-        xyv_smem + RS_TILE * (sizeof(int) + sizeof(double)));
-    int *s_tile_start = &s_whist[RS_WARPS][0];
+    double *s_x = reinterpret_cast<double *>(xyv_smem);
+    double *s_y = s_x + XYV_TILE;
+    double *s_v = s_y + XYV_TILE;
+    int *s_keys = reinterpret_cast<int *>(s_v + XYV_TILE);
+    int *s_idx = s_keys + XYV_TILE;
+    int(*s_whist)[RS_RADIX] = reinterpret_cast<int(*)[RS_RADIX]>(s_idx + XYV_TILE);
+    int *s_tile_start = &s_whist[XYV_WARPS][0];
     int *s_global = s_tile_start + RS_RADIX;
     int *s_tile = s_global + RS_RADIX;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) *s_tile = atomicAdd(tile_counter, 1);
-    for (int i = tid; i < RS_WARPS * RS_RADIX; i += RS_THREADS) (&s_whist[0][0])[i] = 0;
+    for (int i = tid; i < XYV_WARPS * RS_RADIX; i += XYV_THREADS) (&s_whist[0][0])[i] = 0;
     __syncthreads();
     const int tile = *s_tile;
-    const int tile_base = tile * RS_TILE;
-    const int warp_base = tile_base + warp * (RS_ITEMS * 32);
+    const int tile_base = tile * XYV_TILE;
+    const int tile_n = min(XYV_TILE, n - tile_base);
+    const int warp_base = tile_base + warp * (XYV_ITEMS * 32);
+    if (tid == 0) {
+        prefetch_l2(x_in + tile_base, sizeof(double) * tile_n);
+        prefetch_l2(y_in + tile_base, sizeof(double) * tile_n);
+        prefetch_l2(v_in + tile_base, sizeof(double) * tile_n);
+        if (idx_in) prefetch_l2(idx_in + tile_base, sizeof(int) * tile_n);
+    }
 
-    int key[RS_ITEMS], pos[RS_ITEMS];
+    int key[XYV_ITEMS], pos[XYV_ITEMS];
 #pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
+    for (int k = 0; k < XYV_ITEMS; ++k) {
         const int idx = warp_base + k * 32 + lane;
         key[k] = idx < n ? keys_in[idx] : 0;
     }
@@ -375,7 +472,7 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
     const unsigned lt = lanemask_lt();
     int *hist = s_whist[warp];
 #pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
+    for (int k = 0; k < XYV_ITEMS; ++k) {
         const int idx = warp_base + k * 32 + lane;
         const bool valid = idx < n;
         const unsigned vmask = __ballot_sync(FULL_MASK, valid);
@@ -390,10 +487,10 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
     }
     __syncthreads();
 
-    const int d = tid;
+    const int d = tid;   // one digit per thread
     int total = 0;
 #pragma unroll
-    for (int w = 0; w < RS_WARPS; ++w) {
+    for (int w = 0; w < XYV_WARPS; ++w) {
         const int c = s_whist[w][d];
         s_whist[w][d] = total;
         total += c;
@@ -404,22 +501,7 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
         atomicExch(mine, RS_FLAG_INC | (unsigned)total);
     } else {
         atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
-        int j = tile - 1;
-        int spins = 0;
-        while (j >= 0) {
-            const unsigned s = ld_volatile(status + (size_t)j * RS_RADIX + d);
-            const unsigned flag = s & ~RS_VALMASK;
-            if (flag == 0) {
-                if (++spins > RS_SPIN_LIMIT) {
-                    atomicOr(err, DEVERR_SPIN_LIMIT);
-                    break;
-                }
-                continue;
-            }
-            excl += (int)(s & RS_VALMASK);
-            if (flag == RS_FLAG_INC) break;
-            --j;
-        }
+        excl = lookback(status, tile, d, err);
         atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
     }
     const int start = block_exclusive_scan(total, nullptr);
@@ -427,54 +509,40 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep_xyv(
     s_global[d] = digit_offsets[d] + excl - start;
     __syncthreads();
 
-    // local sorted positions (pos held the in-warp rank); keys and input indices first
+    // every item to its sorted slot in shared memory, with its index, x, y and v
 #pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
+    for (int k = 0; k < XYV_ITEMS; ++k) {
         const int idx = warp_base + k * 32 + lane;
-        int p = -1;
         if (idx < n) {
             const int dk = (key[k] >> shift) & 0xFF;
-            p = s_tile_start[dk] + s_whist[warp][dk] + pos[k];
-            if ((unsigned)p >= (unsigned)RS_TILE) {
+            const int p = s_tile_start[dk] + s_whist[warp][dk] + pos[k];
+            if ((unsigned)p >= (unsigned)tile_n) {
                 atomicOr(err, DEVERR_BOUNDS);
-                p = -1;
             } else {
                 s_keys[p] = key[k];
-                s_ibuf[p] = idx_in ? idx_in[idx] : idx;
+                s_idx[p] = idx_in ? __ldg(idx_in + idx) : idx;
+                s_x[p] = __ldg(x_in + idx);
+                s_y[p] = __ldg(y_in + idx);
+                s_v[p] = __ldg(v_in + idx);
             }
         }
-        pos[k] = p;
     }
     __syncthreads();
 
-    const int tile_n = min(RS_TILE, n - tile_base);
-    // global position of local slot j
-    auto gpos = [&](int j) { return s_global[(s_keys[j] >> shift) & 0xFF] + j; };
-    for (int j = tid; j < tile_n; j += RS_THREADS) {
-        const int g = gpos(j);
+    // slot j goes to s_global[digit] + j: runs of equal digits are consecutive in memory
+#pragma unroll 4
+    for (int j = tid; j < tile_n; j += XYV_THREADS) {
+        const int kj = s_keys[j];
+        const int g = s_global[(kj >> shift) & 0xFF] + j;
         if ((unsigned)g >= (unsigned)n) {
             atomicOr(err, DEVERR_BOUNDS);
             continue;
         }
-        keys_out[g] = s_keys[j];
-        idx_out[g] = s_ibuf[j];
-    }
-    // then x, y and v, one component at a time through the same buffer
-#pragma unroll 1
-    for (int comp = 0; comp < 3; ++comp) {
-        const double *src = comp == 0 ? x_in : (comp == 1 ? y_in : v_in);
-        double *dst = comp == 0 ? x_out : (comp == 1 ? y_out : v_out);
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < RS_ITEMS; ++k) {
-            const int idx = warp_base + k * 32 + lane;
-            if (pos[k] >= 0) s_buf[pos[k]] = src[idx];
-        }
-        __syncthreads();
-        for (int j = tid; j < tile_n; j += RS_THREADS) {
-            const int g = gpos(j);
-            if ((unsigned)g < (unsigned)n) dst[g] = s_buf[j];
-        }
+        keys_out[g] = kj;
+        idx_out[g] = s_idx[j];
+        x_out[g] = s_x[j];
+        y_out[g] = s_y[j];
+        v_out[g] = s_v[j];
     }
 }
 
@@ -620,15 +688,13 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
         (rc = ensure(c, S_PERM2, n, &perm2)))
         return rc;
     // frame + bbox partials + completion counter share one small buffer
-    const int gb = grid_for(n, BBOX_THREADS, 4);
+    const int gb = grid_for(n, BBOX_THREADS, 8);
     if ((rc = ensure(c, S_FRAME, sizeof(Frame) + sizeof(double4) * (gb + 1) + 64, (char **)&frame)))
         return rc;
     partials = reinterpret_cast<double4 *>(reinterpret_cast<char *>(frame) + 64);
     unsigned *done = reinterpret_cast<unsigned *>(partials + gb);
     TC_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned), c.stream));
     k_bbox<<<gb, BBOX_THREADS, 0, c.stream>>>(x, y, n, partials, done, frame);
-    TC_KERNEL_CHECK();
-    k_keys<<<grid_for(n, 256), 256, 0, c.stream>>>(x, y, n, frame, keys);
     TC_KERNEL_CHECK();
 
     // four 8-bit passes carrying (index, x, y, v); the ping-pong
@@ -641,7 +707,7 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     int *hist, *counter;
     unsigned *status;
     const int npasses = (2 * LMAX + 7) / 8;
-    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    const int ntiles = (n + XYV_TILE - 1) / XYV_TILE;
     if ((rc = ensure(c, S_X2, n, &x2)) || (rc = ensure(c, S_Y2, n, &y2)) ||
         (rc = ensure(c, S_V2, n, &v2)) ||
         (rc = ensure(c, S_RS_HIST, 2 * RS_MAX_PASSES * RS_RADIX, &hist)) ||
@@ -653,7 +719,7 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
                                 c.stream));
-    k_hist<<<grid_for(n, 256, 4), 256, 0, c.stream>>>(keys, n, npasses, hist);
+    k_keys_hist<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, keys, npasses, hist);
     TC_KERNEL_CHECK();
     k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
     TC_KERNEL_CHECK();
@@ -671,12 +737,11 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
         const double *vi = p == 0 ? v : (odd ? v2 : vs);
         int *ko = odd ? keys : keys2, *io = odd ? perm : perm2;
         double *xo = odd ? xs : x2, *yo = odd ? ys : y2, *vo = odd ? vs : v2;
-        k_onesweep_xyv<<<ntiles, RS_THREADS, XYV_SMEM, c.stream>>>(
+        k_onesweep_xyv<<<ntiles, XYV_THREADS, XYV_SMEM, c.stream>>>(
             ki, ii, xi, yi, vi, ko, io, xo, yo, vo, n, 8 * p, offsets + p * RS_RADIX,
             status + (size_t)p * ntiles * RS_RADIX, counter + p, err);
         TC_KERNEL_CHECK();
     }
-    (void)perm2;
     c.nsrc = n;
     return TC_OK;
 }
@@ -784,7 +849,7 @@ extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const doub
     TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, s));
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX, s));
 
-    const int gb = std::min(grid_for(n, BBOX_THREADS, 4), NA_MAX_BBOX_BLOCKS);
+    const int gb = std::min(grid_for(n, BBOX_THREADS, 8), NA_MAX_BBOX_BLOCKS);
     k_bbox<<<gb, BBOX_THREADS, 0, s>>>(xsources, ysources, n, partials, done, fr);
     TC_KERNEL_CHECK();
     k_keys<<<grid_for(n, 256), 256, 0, s>>>(xsources, ysources, n, fr, keys);
