@@ -182,7 +182,8 @@ struct EvalShared {
     // mixed form: scaled E2P coefficients and the P2P tile as float offsets (hi + lo) from the
     // brick corner
     float2 coef32[P];
-    float sxh[EV_CHUNK], sxl[EV_CHUNK], syh[EV_CHUNK], syl[EV_CHUNK], sv32[EV_CHUNK];
+    float4 sxy32[EV_CHUNK];       // (x hi, x lo, y hi, y lo)
+    float sv32[EV_CHUNK];
 };
 
 __device__ __forceinline__ float rcp_approx_f32(float x) {
@@ -466,18 +467,24 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             if (MIXED) {
                 // FP32 pairs on offsets from the brick corner; differences of (hi, lo) splits
                 // keep the separation accurate to a few float ulps of itself
-                float txh, txl, ty0h, ty0l, ty1h, ty1l;
+                // the second target's y offset is the first one's plus 4h, added in float: one
+                // rounding of a quantity of the size of the offset itself
+                float txh, txl, ty0h, ty0l;
                 split_f32(tx * h, txh, txl);
                 split_f32(ty * h, ty0h, ty0l);
-                split_f32((ty + 4) * h, ty1h, ty1l);
+                const float four_h = (float)(4.0 * h);
                 const float epsf = (float)eps;
                 float hx0 = 0, lx0 = 0, hy0 = 0, ly0 = 0, hx1 = 0, lx1 = 0, hy1 = 0, ly1 = 0;
                 while (tn > 0) {
                     const int cnt = tn;
                     __syncwarp();
-                    split_f32(px - b.xlo, sh.sxh[lane], sh.sxl[lane]);
-                    split_f32(py - b.ylo, sh.syh[lane], sh.syl[lane]);
-                    sh.sv32[lane] = (float)pv;
+                    {
+                        float4 q;
+                        split_f32(px - b.xlo, q.x, q.y);
+                        split_f32(py - b.ylo, q.z, q.w);
+                        sh.sxy32[lane] = q;
+                        sh.sv32[lane] = (float)pv;
+                    }
                     __syncwarp();
                     next_tile(t0, tn);
                     if (lane < tn) {
@@ -489,11 +496,10 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
 #pragma unroll 4
                     for (int k = 0; k < cnt; ++k) {
                         const float v = sh.sv32[k];
-                        const float sxh = sh.sxh[k], sxl = sh.sxl[k];
-                        const float syh = sh.syh[k], syl = sh.syl[k];
-                        const float dx = (txh - sxh) + (txl - sxl);
-                        const float dy0 = (ty0h - syh) + (ty0l - syl);
-                        const float dy1 = (ty1h - syh) + (ty1l - syl);
+                        const float4 q = sh.sxy32[k];
+                        const float dx = (txh - q.x) + (txl - q.y);
+                        const float dy0 = (ty0h - q.z) + (ty0l - q.w);
+                        const float dy1 = dy0 + four_h;
                         const float dx2e = fmaf(dx, dx, epsf);
                         const float f0 = v * rcp_approx_f32(fmaf(dy0, dy0, dx2e));
                         const float f1 = v * rcp_approx_f32(fmaf(dy1, dy1, dx2e));

@@ -3,7 +3,8 @@
 // k_leaf_setup: four threads per node run the leaf setup with the reference's four strided
 // accumulators (drivers/upward.cpp:61-93, kernels/upward-common.ispc:13-57).
 // k_leaf_p2e: one warp per leaf forms its multipole expansion, lanes over sources with the P
-// coefficients in registers (kernels/upward-kernels.m4:18-93).
+// coefficients in registers (kernels/upward-kernels.m4:18-93); FP32 lane sums in the
+// mixed-precision form.
 // k_upward_level: one launch per deep tree level, deepest first, one warp per inner node; the
 // small top levels run in one single-block launch that walks them with a block barrier between
 // levels (upward.cpp:95-218, kernels/upward-kernels.m4:95-149).  Children were finished before
@@ -27,6 +28,7 @@
 //
 // Expansion layout: exps[node][0][k] real parts, exps[node][1][k] imaginary parts, k < ORDER.
 #include <algorithm>
+#include <type_traits>
 
 #include "tc_internal.h"
 #include "tc_math.cuh"
@@ -130,21 +132,27 @@ __global__ __launch_bounds__(256) void k_leaf_setup(
 // k_leaf_p2e: a_n = -1/(n+1) sum_i v_i (z_i - c)^(n+1), one warp per leaf, lanes over sources
 // with the P coefficients in registers; the 32 partial sums of each coefficient meet in shared
 // memory, transposed so that lane n adds up coefficient n.
-template <int P>
+template <int P, class T = double>
 struct LeafShared {
-    double v[32][2 * P + 1];
+    T v[32][2 * P + 1];
 };
 
 
-template <int P>
-__global__ __launch_bounds__(UP_WARPS * 32) void k_leaf_p2e(
+// MIXED: the mixed-precision form accumulates in FP32 on offsets scaled by R, the power of two
+// at or above the cell's half-diagonal (every source of the leaf lies in its cell, and so does
+// the com, so |z / R| <= 1 and no power under- or overflows).  Each lane sums at most
+// leafcap/32 terms in FP32; the 32 lane sums are added in FP64 and rescaled by R^(n+1) exactly.
+template <int P, bool MIXED>
+__global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 5 : 3) void k_leaf_p2e(
     int nnodes, int nsrc, int leafcap, const double *__restrict__ xs, const double *__restrict__ ys,
     const double *__restrict__ vs, const int2 *__restrict__ range, const int4 *__restrict__ cell,
-    const TNode *__restrict__ tnode, double *exps) {
-    constexpr int U = P > 16 ? 6 : 4;   // sources per lane in flight
+    const TNode *__restrict__ tnode, double *exps, const Frame *__restrict__ frame) {
+    using acc_t = typename std::conditional<MIXED, float, double>::type;
+    constexpr int U = MIXED ? 4 : (P > 16 ? 6 : 4);   // sources per lane in flight
     extern __shared__ __align__(16) unsigned char leaf_smem[];
-    LeafShared<P> &sh = reinterpret_cast<LeafShared<P> *>(leaf_smem)[threadIdx.x >> 5];
+    LeafShared<P, acc_t> &sh = reinterpret_cast<LeafShared<P, acc_t> *>(leaf_smem)[threadIdx.x >> 5];
     const int lane = lane_id();
+    const double ext = frame->ext;
     const int stride = gridDim.x * UP_WARPS;
     int next = blockIdx.x * UP_WARPS + (threadIdx.x >> 5);
     // the next node's record is loaded while the current leaf is expanded
@@ -170,29 +178,32 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_leaf_p2e(
             ncy = tnode[next].ycom;
         }
         if (!is_leaf(rg, cl, leafcap) || rg.x < 0 || rg.y < rg.x || rg.y > nsrc) continue;
-        double ar[P], ai[P];
+        int e = 0;   // R = 2^e (mixed form)
+        if (MIXED) frexp(1.4142135623730951 * (1.0 + 1e-12) * ldexp(ext, -cl.x), &e);
+        const double inv_r = MIXED ? ldexp(1.0, -e) : 1.0;
+        acc_t ar[P], ai[P];
 #pragma unroll
-        for (int n = 0; n < P; ++n) ar[n] = ai[n] = 0.0;
+        for (int n = 0; n < P; ++n) ar[n] = ai[n] = acc_t(0);
         for (int base = rg.x; base < rg.y; base += 32 * U) {
             const int nu = min(U, (rg.y - base + 31) >> 5);   // warp-uniform
-            double zr[U], zi[U], v[U];
+            acc_t zr[U], zi[U], v[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int j = base + 32 * u + lane;
                 const bool ok = u < nu && j < rg.y;
-                zr[u] = ok ? __ldg(xs + j) - cx : 0.0;
-                zi[u] = ok ? __ldg(ys + j) - cy : 0.0;
-                v[u] = ok ? __ldg(vs + j) : 0.0;
+                zr[u] = ok ? acc_t((__ldg(xs + j) - cx) * inv_r) : acc_t(0);
+                zi[u] = ok ? acc_t((__ldg(ys + j) - cy) * inv_r) : acc_t(0);
+                v[u] = ok ? acc_t(__ldg(vs + j)) : acc_t(0);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (u >= nu) break;
-                double pr = v[u] * zr[u], pim = v[u] * zi[u];
+                acc_t pr = v[u] * zr[u], pim = v[u] * zi[u];
 #pragma unroll
                 for (int n = 0; n < P; ++n) {
                     ar[n] += pr;
                     ai[n] += pim;
-                    const double tr = fma(pr, zr[u], -pim * zi[u]);
+                    const acc_t tr = fma(pr, zr[u], -pim * zi[u]);
                     pim = fma(pr, zi[u], pim * zr[u]);
                     pr = tr;
                 }
@@ -209,12 +220,13 @@ __global__ __launch_bounds__(UP_WARPS * 32) void k_leaf_p2e(
             double sr0 = 0, sr1 = 0, si0 = 0, si1 = 0;
 #pragma unroll 8
             for (int i = 0; i < 32; i += 2) {
-                sr0 += sh.v[i][lane];
-                sr1 += sh.v[i + 1][lane];
-                si0 += sh.v[i][P + lane];
-                si1 += sh.v[i + 1][P + lane];
+                sr0 += (double)sh.v[i][lane];
+                sr1 += (double)sh.v[i + 1][lane];
+                si0 += (double)sh.v[i][P + lane];
+                si1 += (double)sh.v[i + 1][P + lane];
             }
-            const double fac = -1.0 / (lane + 1);
+            double fac = -1.0 / (lane + 1);
+            if (MIXED) fac = ldexp(fac, e * (lane + 1));
             double *ex = exps + (size_t)node * 2 * P;
             ex[lane] = (sr0 + sr1) * fac;
             ex[P + lane] = (si0 + si1) * fac;
@@ -611,14 +623,21 @@ static int run_upward(Context &c, double *mass, double *w, double *wx, double *w
     k_leaf_setup<<<(int)(((long long)nn * 4 + 255) / 256), 256, 0, c.stream>>>(
         nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell, tnode, mass, w, wx, wy, frame, err);
     TC_KERNEL_CHECK();
-    const size_t smem = UP_WARPS * sizeof(LeafShared<P>);
-    static const cudaError_t attr_rc = cudaFuncSetAttribute(
-        k_leaf_p2e<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    TC_CUDA_TRY(attr_rc);
-    const int occ = blocks_per_sm<k_leaf_p2e<P>>(UP_WARPS * 32, smem);
+    const bool mixed = c.precision == 1;
+    const size_t smem64 = UP_WARPS * sizeof(LeafShared<P, double>);
+    const size_t smem32 = UP_WARPS * sizeof(LeafShared<P, float>);
+    const size_t smem = mixed ? smem32 : smem64;
+    static const cudaError_t attr_rc[2] = {
+        cudaFuncSetAttribute(k_leaf_p2e<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem64),
+        cudaFuncSetAttribute(k_leaf_p2e<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)};
+    TC_CUDA_TRY(attr_rc[0]);
+    TC_CUDA_TRY(attr_rc[1]);
+    const int occ = mixed ? blocks_per_sm<k_leaf_p2e<P, true>>(UP_WARPS * 32, smem32)
+                          : blocks_per_sm<k_leaf_p2e<P, false>>(UP_WARPS * 32, smem64);
     const int grid = (int)std::min<long long>((nn + UP_WARPS - 1) / UP_WARPS, (long long)sms * occ);
-    k_leaf_p2e<P><<<grid, UP_WARPS * 32, smem, c.stream>>>(nn, c.nsrc, c.leafcap, xs, ys, vs,
-                                                         range, cell, tnode, exps);
+    auto p2e = mixed ? k_leaf_p2e<P, true> : k_leaf_p2e<P, false>;
+    p2e<<<grid, UP_WARPS * 32, smem, c.stream>>>(nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell,
+                                                 tnode, exps, frame);
     TC_KERNEL_CHECK();
     // Inner nodes exist on levels 0 .. LMAX-1; level l occupies [level_off[l], level_off[l+1]).
     // Levels 0 .. ltop are all small: they run in one single-block launch after the others.
