@@ -20,10 +20,25 @@
 namespace tc {
 
 constexpr int PT_WARPS = 4;
-constexpr int PT_STACK = 64;   // depth-first, one entry popped per step: <= 3 * LMAX + 4 live entries
 // A group's evaluation is split into tasks of at most PT_SEG near-field sources (task 0 also
 // does the far field), so that groups inside dense clusters do not serialise the kernel.
 constexpr int PT_SEG = 4096;
+
+// Lists of one group of 32 targets.  The warp pops up to 32 stack entries (node, target mask)
+// at a time, one per lane, so the latency of the node reads is shared by a whole batch.  A lane
+// decides its node for the entry's targets with the group's bounding box first: when every
+// point of the box is clearly far (or clearly near) -- with a relative margin of 1e-12, far
+// above the rounding of the per-target test -- the whole mask follows; otherwise the exact
+// per-target test (r^2 < theta^2 |t - com|^2, treecode-potential.cpp:48-50) runs for each
+// target of the mask.  Far targets give an E2P entry (node, far); the rest give a P2P entry for
+// a leaf or push the node's four children with the rest.  Every target thus gets exactly the
+// nodes its own depth-first traversal in the reference would give it.  Entries are written in
+// the (deterministic) processing order; the count pass and the fill pass take the same steps.
+// Stack entries per warp.  A batch of nb entries pushes at most 4 nb, so batches are taken only
+// while top <= PL_STACK - 160; above that the walk pops one entry at a time (depth first), which
+// grows the stack by at most 3 per level, 45 in all, before it shrinks again.  The stack thus
+// never holds more than PL_STACK - 160 + 96 + 45 entries.
+constexpr int PL_STACK = 512;
 
 template <bool FILL>
 __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
@@ -31,9 +46,12 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
     const int *__restrict__ tperm, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int2 *__restrict__ lists,
     unsigned *err, unsigned long long *stats) {
-    __shared__ int2 stack_all[PT_WARPS][PT_STACK];
+    __shared__ int2 stack_all[PT_WARPS][PL_STACK];
+    __shared__ double2 targ_all[PT_WARPS][32];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     int2 *stack = stack_all[warp];
+    double2 *targ = targ_all[warp];
+    const unsigned lt = (1u << lane) - 1u;
     const double theta2 = theta * theta;
     unsigned long long e2p_pairs = 0, p2p_pairs = 0;   // warp-uniform work counters
 
@@ -47,6 +65,15 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             y = yt[j];
         }
         const unsigned vmask = __ballot_sync(FULL_MASK, valid);
+        // bounding box of the group's targets
+        double bxlo = valid ? x : 1e300, bxhi = valid ? x : -1e300;
+        double bylo = valid ? y : 1e300, byhi = valid ? y : -1e300;
+        for (int o = 16; o; o >>= 1) {
+            bxlo = fmin(bxlo, __shfl_xor_sync(FULL_MASK, bxlo, o));
+            bxhi = fmax(bxhi, __shfl_xor_sync(FULL_MASK, bxhi, o));
+            bylo = fmin(bylo, __shfl_xor_sync(FULL_MASK, bylo, o));
+            byhi = fmax(byhi, __shfl_xor_sync(FULL_MASK, byhi, o));
+        }
         int o0 = 0, o1 = 0, l0 = 0, l1 = 0;
         if (FILL) {
             o0 = offs[g];
@@ -54,58 +81,92 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             o1 = offs[ngroups + g];
             l1 = offs[ngroups + g + 1];
         }
-        int n0 = 0, n1 = 0, gsrc = 0;
-        int top = 0;
-        if (lane == 0) stack[0] = make_int2(0, (int)vmask);
-        top = 1;
         __syncwarp();
-        while (top > 0) {
-            --top;
-            const int2 ent = stack[top];
+        targ[lane] = make_double2(x, y);
+        if (lane == 0) stack[0] = make_int2(0, (int)vmask);
+        __syncwarp();
+        int n0 = 0, n1 = 0, gsrc = 0, top = 1;
+        bool overflow = false;
+        while (top > 0 && !overflow) {
+            const int nb = top > PL_STACK - 160 ? 1 : min(32, top), base = top - nb;
+            const bool act = lane < nb;
+            int2 ent = make_int2(0, 0);
+            if (act) ent = stack[base + lane];
             __syncwarp();
+            top = base;
             const unsigned mask = (unsigned)ent.y;
-            if ((unsigned)ent.x >= (unsigned)nnodes) {
-                if (lane == 0) atomicOr(err, DEVERR_BOUNDS);
-                continue;
+            bool ok = act && mask != 0;
+            if (act && (unsigned)ent.x >= (unsigned)nnodes) {
+                atomicOr(err, DEVERR_BOUNDS);
+                ok = false;
             }
-            const TNode nd = tnode[ent.x];
-            // r2 = (xt - xcom)^2 + (yt - ycom)^2 without contraction, as the compiled reference
-            const double dx = __dsub_rn(x, nd.xcom), dy = __dsub_rn(y, nd.ycom);
-            const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-            const bool accept = ((mask >> lane) & 1u) && __dmul_rn(nd.r, nd.r) < __dmul_rn(theta2, r2);
-            const unsigned far = __ballot_sync(FULL_MASK, accept);
+            TNode nd = {};
+            if (ok) nd = tnode[ent.x];
+            unsigned far = 0;
+            if (ok) {
+                const double rr = __dmul_rn(nd.r, nd.r);
+                const double ex = fmax(fmax(bxlo - nd.xcom, nd.xcom - bxhi), 0.0);
+                const double ey = fmax(fmax(bylo - nd.ycom, nd.ycom - byhi), 0.0);
+                const double fx = fmax(nd.xcom - bxlo, bxhi - nd.xcom);
+                const double fy = fmax(nd.ycom - bylo, byhi - nd.ycom);
+                const double dmin2 = ex * ex + ey * ey, dmax2 = fx * fx + fy * fy;
+                if (rr < theta2 * dmin2 * (1.0 - 1e-12)) {
+                    far = mask;                         // every target of the box is far
+                } else if (rr >= theta2 * dmax2 * (1.0 + 1e-12)) {
+                    far = 0;                            // every target of the box is near
+                } else {
+                    for (unsigned mm = mask; mm; mm &= mm - 1) {
+                        const int tl = __ffs(mm) - 1;
+                        const double2 tp = targ[tl];
+                        // r2 without contraction, as the compiled reference
+                        const double dx = __dsub_rn(tp.x, nd.xcom), dy = __dsub_rn(tp.y, nd.ycom);
+                        const double r2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+                        if (rr < __dmul_rn(theta2, r2)) far |= 1u << tl;
+                    }
+                }
+            }
             const unsigned rest = mask & ~far;
-            if (far) {
-                e2p_pairs += __popc(far);
-                if (FILL && lane == 0) {
-                    if (o0 + n0 < l0) lists[o0 + n0] = make_int2(ent.x, (int)far);
+            const bool leaf = nd.child < 0;
+            const bool f_far = ok && far != 0;
+            const bool f_near = ok && rest != 0 && leaf && nd.count > 0;
+            bool f_push = ok && rest != 0 && !leaf;
+            if (f_push && (nd.child <= ent.x || nd.child + 4 > nnodes)) {
+                atomicOr(err, DEVERR_BOUNDS);
+                f_push = false;
+            }
+            const unsigned bf = __ballot_sync(FULL_MASK, f_far);
+            const unsigned bn = __ballot_sync(FULL_MASK, f_near);
+            const unsigned bp = __ballot_sync(FULL_MASK, f_push);
+            if (FILL) {
+                if (f_far) {
+                    const int at = o0 + n0 + __popc(bf & lt);
+                    if (at < l0) lists[at] = make_int2(ent.x, (int)far);
                     else atomicOr(err, DEVERR_BOUNDS);
                 }
-                ++n0;
-            }
-            if (rest) {
-                if (nd.child < 0) {
-                    if (nd.count > 0) {
-                        p2p_pairs += (unsigned long long)__popc(rest) * (unsigned)nd.count;
-                        gsrc += nd.count;
-                        if (FILL && lane == 0) {
-                            if (o1 + n1 < l1) lists[o1 + n1] = make_int2(ent.x, (int)rest);
-                            else atomicOr(err, DEVERR_BOUNDS);
-                        }
-                        ++n1;
-                    }
-                } else {
-                    if (nd.child <= ent.x || nd.child + 4 > nnodes) {
-                        if (lane == 0) atomicOr(err, DEVERR_BOUNDS);
-                        continue;
-                    }
-                    if (top + 4 > PT_STACK) {
-                        if (lane == 0) atomicOr(err, DEVERR_STACK);
-                        break;
-                    }
-                    if (lane < 4) stack[top + lane] = make_int2(nd.child + 3 - lane, (int)rest);
-                    top += 4;
+                if (f_near) {
+                    const int at = o1 + n1 + __popc(bn & lt);
+                    if (at < l1) lists[at] = make_int2(ent.x, (int)rest);
+                    else atomicOr(err, DEVERR_BOUNDS);
                 }
+            }
+            n0 += __popc(bf);
+            n1 += __popc(bn);
+            e2p_pairs += (unsigned)__reduce_add_sync(FULL_MASK, f_far ? __popc(far) : 0);
+            const unsigned cnt = f_near ? (unsigned)nd.count : 0u;
+            gsrc += (int)__reduce_add_sync(FULL_MASK, cnt);
+            p2p_pairs += __reduce_add_sync(FULL_MASK, f_near ? (unsigned)__popc(rest) * cnt : 0u);
+            const int npush = 4 * __popc(bp);
+            if (top + npush > PL_STACK) {
+                if (lane == 0) atomicOr(err, DEVERR_STACK);
+                overflow = true;
+            } else {
+                if (f_push) {
+                    const int at = top + 4 * __popc(bp & lt);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        stack[at + c] = make_int2(nd.child + 3 - c, (int)rest);
+                }
+                top += npush;
             }
             __syncwarp();
         }
