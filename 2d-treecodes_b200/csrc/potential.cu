@@ -232,6 +232,7 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
     __shared__ double s_v[PE_WARPS][PE_CHUNK];
     __shared__ float4 s_off[PE_WARPS][PE_CHUNK];   // (x hi, x lo, y hi, y lo) from the reference
     __shared__ float s_v32[PE_WARPS][PE_CHUNK];
+    __shared__ double s_part[PE_WARPS][32];        // P2P lane partials of a sparse mask
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     const double eps = 10 * DBL_EPSILON;
     const int *toff = offs + 2 * ngroups;
@@ -259,30 +260,47 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
         const double xref = __shfl_sync(FULL_MASK, x, 0), yref = __shfl_sync(FULL_MASK, y, 0);
         double far = 0, near = 0;
 
-        // E2P (potential-kernels.m4:59-89): m log(r2)/2 + Re sum_{j=1..p} a_{j-1} z^-j
+        // E2P (potential-kernels.m4:59-89): m log(r2)/2 + Re sum_{j=1..p} a_{j-1} z^-j.  The next
+        // entry's cell record and coefficients are loaded while the current one is evaluated.
         if (part == 0) {
             const int b0 = offs[g], e0 = offs[g + 1];
             float sh = 0, sl = 0;
+            int2 ent_n = make_int2(0, 0);
+            TNode nd_n = {};
+            double m_n = 0, cr_n = 0, ci_n = 0;
+            float R_n = 1.f;
+            float2 c32_n = make_float2(0.f, 0.f);
+            auto fetch = [&](int at) {
+                ent_n = lists[at];
+                nd_n = tnode[ent_n.x];
+                m_n = mass[ent_n.x];
+                if (MIXED) {
+                    R_n = sscale[ent_n.x];
+                    if (lane < P) c32_n = sexp[(size_t)ent_n.x * P + lane];
+                } else if (lane < P) {
+                    const double *ex = exps + (size_t)ent_n.x * 2 * P;
+                    cr_n = ex[lane];
+                    ci_n = ex[P + lane];
+                }
+            };
+            if (b0 < e0) fetch(b0);
             for (int it = b0; it < e0; ++it) {
-                const int2 ent = lists[it];
-                const TNode nd = tnode[ent.x];
-                const double mm = mass[ent.x];
+                const int2 ent = ent_n;
+                const TNode nd = nd_n;
+                const double mm = m_n;
+                const float R = R_n;
                 __syncwarp();
                 if (lane < P) {
-                    if (MIXED) {
-                        s_coef32[warp][lane] = sexp[(size_t)ent.x * P + lane];
-                    } else {
-                        const double *ex = exps + (size_t)ent.x * 2 * P;
-                        s_coef[warp][lane] = {ex[lane], ex[P + lane]};
-                    }
+                    if (MIXED) s_coef32[warp][lane] = c32_n;
+                    else s_coef[warp][lane] = {cr_n, ci_n};
                 }
                 __syncwarp();
+                if (it + 1 < e0) fetch(it + 1);
                 if ((ent.y >> lane) & 1) {
                     const double rz = x - nd.xcom, iz = y - nd.ycom;
                     const double r2 = rz * rz + iz * iz;
                     if (MIXED) {
                         // series: Re(u' Q(u')), u' = R / z, Q(u') = sum_j D_j u'^j
-                        const float R = sscale[ent.x];
                         const float zr = (float)rz, zi = (float)iz;
                         const float inv = rcp_approx(zr * zr + zi * zi);
                         const float ur = R * zr * inv, ui = -R * zi * inv;
@@ -309,64 +327,146 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
         }
 
         // P2P (potential-kernels.m4:19-57): 0.5 sum v log(r2 + eps), sources
-        // [part * PT_SEG, (part + 1) * PT_SEG) of the group's listed leaves
+        // [part * PT_SEG, (part + 1) * PT_SEG) of the group's listed leaves.  Tiles of up to
+        // PE_CHUNK consecutive sources of one leaf; the next tile is loaded into registers while
+        // the current one is evaluated.
         {
             const int b1 = offs[ngroups + g], e1 = offs[ngroups + g + 1];
-            int skip = part * PT_SEG, budget = PT_SEG;
+            int it = b1, skip = part * PT_SEG, budget = PT_SEG;
+            int s_next = 0, e_next = 0;
+            unsigned mask_next = 0;
+            while (it < e1) {
+                const int2 ent = lists[it++];
+                const int2 rg = range[ent.x];
+                const int cnt = rg.y - rg.x;
+                if (skip < cnt) {
+                    s_next = rg.x + skip;
+                    e_next = rg.y;
+                    mask_next = (unsigned)ent.y;
+                    break;
+                }
+                skip -= cnt;
+            }
+            auto next_tile = [&](int &t0, int &tn, unsigned &msk) {
+                while (s_next >= e_next && it < e1) {
+                    const int2 ent = lists[it++];
+                    const int2 rg = range[ent.x];
+                    s_next = rg.x;
+                    e_next = rg.y;
+                    mask_next = (unsigned)ent.y;
+                }
+                t0 = s_next;
+                tn = min(min(PE_CHUNK, e_next - s_next), budget);
+                if (tn < 0) tn = 0;
+                msk = mask_next;
+                s_next += tn;
+                budget -= tn;
+            };
+            int t0, tn;
+            unsigned msk;
+            next_tile(t0, tn, msk);
+            double px = 0, py = 0, pv = 0;
+            if (lane < tn) {
+                px = xs[t0 + lane];
+                py = ys[t0 + lane];
+                pv = vs[t0 + lane];
+            }
             float nh = 0, nl = 0, txh = 0, txl = 0, tyh = 0, tyl = 0;
             if (MIXED) {
                 split2(x - xref, txh, txl);
                 split2(y - yref, tyh, tyl);
             }
             const float ln2 = 0.6931471805599453f, epsf = (float)eps;
-            for (int it = b1; it < e1 && budget > 0; ++it) {
-                const int2 ent = lists[it];
-                const int2 rg = range[ent.x];
-                const int cnt_leaf = rg.y - rg.x;
-                if (skip >= cnt_leaf) {
-                    skip -= cnt_leaf;
-                    continue;
-                }
-                const int sbeg = rg.x + skip;
-                const int send = min(rg.y, sbeg + budget);
-                budget -= send - sbeg;
-                skip = 0;
-                const bool mine = (ent.y >> lane) & 1;
-                for (int s0 = sbeg; s0 < send; s0 += PE_CHUNK) {
-                    const int cnt = min(PE_CHUNK, send - s0);
-                    __syncwarp();
-                    if (lane < cnt) {
-                        if (MIXED) {
-                            float a, b2, c2, d2;
-                            split2(xs[s0 + lane] - xref, a, b2);
-                            split2(ys[s0 + lane] - yref, c2, d2);
-                            s_off[warp][lane] = make_float4(a, b2, c2, d2);
-                            s_v32[warp][lane] = (float)vs[s0 + lane];
-                        } else {
-                            s_xy[warp][lane] = make_double2(xs[s0 + lane], ys[s0 + lane]);
-                            s_v[warp][lane] = vs[s0 + lane];
-                        }
+            while (tn > 0) {
+                const int cnt = tn;
+                const unsigned cmask = msk;   // this tile's targets (msk moves on to the next tile)
+                const bool mine = (cmask >> lane) & 1;
+                __syncwarp();
+                if (lane < cnt) {
+                    if (MIXED) {
+                        float a, b2, c2, d2;
+                        split2(px - xref, a, b2);
+                        split2(py - yref, c2, d2);
+                        s_off[warp][lane] = make_float4(a, b2, c2, d2);
+                        s_v32[warp][lane] = (float)pv;
+                    } else {
+                        s_xy[warp][lane] = make_double2(px, py);
+                        s_v[warp][lane] = pv;
                     }
-                    __syncwarp();
+                }
+                __syncwarp();
+                next_tile(t0, tn, msk);
+                if (lane < tn) {
+                    px = xs[t0 + lane];
+                    py = ys[t0 + lane];
+                    pv = vs[t0 + lane];
+                }
+                // A tile needed by few targets of the group (k <= 16; k <= 8 in the mixed form,
+                // whose per-pair cost is lower) is spread over the lanes:
+                // lane l takes target q = l % k of the mask and sources l / k, l / k + r, ...
+                // (r = 32 / k), and each target adds its r lane partials in lane order.  Denser
+                // tiles keep one target per lane.
+                const int k = __popc(cmask);
+                if (k > (MIXED ? 8 : 16)) {
                     if (mine) {
                         if (MIXED) {
                             float acc = 0;
 #pragma unroll 4
-                            for (int k = 0; k < cnt; ++k) {
-                                const float4 o = s_off[warp][k];
+                            for (int q = 0; q < cnt; ++q) {
+                                const float4 o = s_off[warp][q];
                                 const float dx = (txh - o.x) + (txl - o.y);
                                 const float dy = (tyh - o.z) + (tyl - o.w);
-                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), s_v32[warp][k], acc);
+                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), s_v32[warp][q], acc);
                             }
                             two_sum_add(nh, nl, acc * ln2);
                         } else {
-                            for (int k = 0; k < cnt; ++k) {
-                                const double2 sp = s_xy[warp][k];
+#pragma unroll 2
+                            for (int q = 0; q < cnt; ++q) {
+                                const double2 sp = s_xy[warp][q];
                                 const double xr = x - sp.x, yr = y - sp.y;
-                                near += log(xr * xr + yr * yr + eps) * s_v[warp][k];
+                                near += log(xr * xr + yr * yr + eps) * s_v[warp][q];
                             }
                         }
                     }
+                } else if (k > 0) {
+                    const int r = 32 / k;
+                    const int qt = lane % k;
+                    const int tl = (int)__fns(cmask, 0, qt + 1);   // lane of this lane's target
+                    double part = 0;
+                    if (MIXED) {
+                        const float qxh = __shfl_sync(FULL_MASK, txh, tl);
+                        const float qxl = __shfl_sync(FULL_MASK, txl, tl);
+                        const float qyh = __shfl_sync(FULL_MASK, tyh, tl);
+                        const float qyl = __shfl_sync(FULL_MASK, tyl, tl);
+                        float acc = 0;
+                        if (lane < r * k)
+                            for (int q = lane / k; q < cnt; q += r) {
+                                const float4 o = s_off[warp][q];
+                                const float dx = (qxh - o.x) + (qxl - o.y);
+                                const float dy = (qyh - o.z) + (qyl - o.w);
+                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), s_v32[warp][q], acc);
+                            }
+                        part = (double)acc;
+                    } else {
+                        const double qx = __shfl_sync(FULL_MASK, x, tl);
+                        const double qy = __shfl_sync(FULL_MASK, y, tl);
+                        if (lane < r * k)
+                            for (int q = lane / k; q < cnt; q += r) {
+                                const double2 sp = s_xy[warp][q];
+                                const double xr = qx - sp.x, yr = qy - sp.y;
+                                part += log(xr * xr + yr * yr + eps) * s_v[warp][q];
+                            }
+                    }
+                    s_part[warp][lane] = part;
+                    __syncwarp();
+                    if (mine) {
+                        const int q = __popc(cmask & ((1u << lane) - 1u));
+                        double sum = 0;
+                        for (int i = 0; i < r; ++i) sum += s_part[warp][q + i * k];
+                        if (MIXED) two_sum_add(nh, nl, (float)sum * ln2);
+                        else near += sum;
+                    }
+                    __syncwarp();
                 }
             }
             if (MIXED) near = (double)nh + (double)nl;
