@@ -101,6 +101,10 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
         TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
     }
+    TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_totals, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaMallocHost(&c.h_pinned, 4096));
     for (auto &ev : c.ev) TC_CUDA_TRY(cudaEventCreate(&ev));
     unsigned *err;
@@ -118,8 +122,12 @@ static void context_free(Context &c) {
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto &b : c.buf)
         if (b.p) cudaFree(b.p);
+    if (c.aux) cudaStreamSynchronize(c.aux);
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join})
+        if (ev) cudaEventDestroy(ev);
+    if (c.aux) cudaStreamDestroy(c.aux);
     if (c.h_pinned) cudaFreeHost(c.h_pinned);
     if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
 }
@@ -143,8 +151,11 @@ static void finish_timing(Context &c) {
 }
 
 // Sort, topology and upward pass for `kind` (0 potential, 1 force).
-static int build_tree(Context &c, int kind, const double *x, const double *y, const double *v,
-                      int n) {
+// Sort, topology and the moments of every node for `kind` (0 potential, 1 force): all that the
+// traversals read.  The expansions follow separately (upward_expansions), so that they can be
+// formed while the interaction lists are built.
+static int build_tree_moments(Context &c, int kind, const double *x, const double *y,
+                              const double *v, int n) {
     int rc;
     g_launches = 0;
     TC_CUDA_TRY(cudaMemsetAsync(slot_ptr<unsigned>(c, S_ERR), 0, sizeof(unsigned), c.stream));
@@ -154,9 +165,25 @@ static int build_tree(Context &c, int kind, const double *x, const double *y, co
     phase_mark(c, 1);
     if ((rc = build_topology(c, kind ? LEAF_FORCE : LEAF_POTENTIAL))) return rc;
     phase_mark(c, 2);
-    if ((rc = upward_pass(c, kind ? ORDER_FORCE : ORDER_POTENTIAL))) return rc;
+    if ((rc = upward_prepare(c, kind ? ORDER_FORCE : ORDER_POTENTIAL)) || (rc = upward_moments(c)))
+        return rc;
+    return TC_OK;
+}
+
+// The whole tree with its expansions (tree inspection).
+static int build_tree(Context &c, int kind, const double *x, const double *y, const double *v,
+                      int n) {
+    int rc;
+    if ((rc = build_tree_moments(c, kind, x, y, v, n)) || (rc = upward_expansions(c))) return rc;
     phase_mark(c, 3);
     return TC_OK;
+}
+
+// Run on the main stream while the lists are built: the expansions, then the phase mark.
+static int expansions_then_mark(Context &c) {
+    const int rc = upward_expansions(c);
+    phase_mark(c, 3);
+    return rc;
 }
 
 static int potential_device(Context &c, double theta, const double *xs, const double *ys,
@@ -174,8 +201,8 @@ static int potential_device(Context &c, double theta, const double *xs, const do
     }
     int rc;
     phase_mark(c, 0);
-    if ((rc = build_tree(c, 0, xs, ys, vs, n))) return rc;
-    if ((rc = potential(c, theta, xt, yt, m, out))) return rc;
+    if ((rc = build_tree_moments(c, 0, xs, ys, vs, n))) return rc;
+    if ((rc = potential(c, theta, xt, yt, m, out, expansions_then_mark))) return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_potential"))) return rc;
     c.counts.e2p_pairs = (long long)stat_counter(c, STAT_E2P_PAIRS);
@@ -205,8 +232,8 @@ static int force_device(Context &c, double theta, const double *xs, const double
     }
     int rc;
     phase_mark(c, 0);
-    if ((rc = build_tree(c, 1, xs, ys, vs, n))) return rc;
-    if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo))) return rc;
+    if ((rc = build_tree_moments(c, 1, xs, ys, vs, n))) return rc;
+    if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo, expansions_then_mark))) return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_force_mrag"))) return rc;
     c.counts.p2p_pairs = (long long)stat_counter(c, STAT_P2P_SOURCES) * TILE * TILE;

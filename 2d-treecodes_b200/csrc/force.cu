@@ -630,8 +630,11 @@ __global__ void k_force_gather_parts(int nbricks, const int *__restrict__ offs,
 
 static int sm_count() { return device_sm_count(); }
 
+// The lists are counted, scanned and filled on the auxiliary stream; `between` (the expansion
+// work, which the traversal does not read) runs on the main stream meanwhile, and the
+// evaluation waits for both.
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
-               int nblocks, double *xout, double *yout) {
+               int nblocks, double *xout, double *yout, OverlapFn between) {
     if (c.order != ORDER_FORCE) {
         set_error(TC_ERR_INVALID, "force evaluation needs an order-%d tree", ORDER_FORCE);
         return TC_ERR_INVALID;
@@ -648,17 +651,26 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     const int trgrid = (int)std::min<long long>((nbricks + TR_WARPS - 1) / TR_WARPS,
                                                 (long long)sm_count() * 16);
-    k_force_lists<false><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(nbricks, x0s, y0s, hs, theta,
-                                                                 tnode, c.nnodes, counts, nullptr, nullptr,
-                                                                 err, nullptr);
-    TC_KERNEL_CHECK();
-    if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
+    TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
+    {
+        AuxScope on_aux(c);
+        TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_fork, 0));
+        k_force_lists<false><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
+            nbricks, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, err, nullptr);
+        TC_KERNEL_CHECK();
+        if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
+        for (int k = 0; k < 4; ++k)
+            TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 32 + k, offs + (k + 1) * nbricks, sizeof(int),
+                                        cudaMemcpyDeviceToHost, c.stream));
+        TC_CUDA_TRY(cudaEventRecord(c.ev_totals, c.stream));
+    }
+    if (between && (rc = between(c))) {
+        cudaStreamSynchronize(c.aux);   // leave nothing of this solve in flight
+        return rc;
+    }
+    TC_CUDA_TRY(cudaEventSynchronize(c.ev_totals));
     int tot[4];
-    for (int k = 0; k < 4; ++k)
-        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + k, offs + (k + 1) * nbricks, sizeof(int),
-                                    cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[k];
+    for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[32 + k];
     const int ntasks = tot[3] - tot[2];
     c.counts.n_e2l = tot[0];
     c.counts.n_e2p = tot[1] - tot[0];
@@ -667,11 +679,16 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     c.counts.e2p_pairs = c.counts.n_e2p * TILE * TILE;
     c.counts.l2p_targets = (long long)nbricks * TILE * TILE;
     int *lists;
-    if ((rc = ensure(c, S_E2L, (size_t)tot[2] + 1, &lists))) return rc;
-    k_force_lists<true><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(nbricks, x0s, y0s, hs, theta,
-                                                                tnode, c.nnodes, nullptr, offs, lists, err,
-                                                                slot_ptr<unsigned long long>(c, S_STATS));
-    TC_KERNEL_CHECK();
+    {
+        AuxScope on_aux(c);
+        if ((rc = ensure(c, S_E2L, (size_t)tot[2] + 1, &lists))) return rc;
+        k_force_lists<true><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
+            nbricks, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, err,
+            slot_ptr<unsigned long long>(c, S_STATS));
+        TC_KERNEL_CHECK();
+        TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
+    }
+    TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
     phase_mark(c, 4);
     int *brick_ctr, *task_brick;
     double *partial;

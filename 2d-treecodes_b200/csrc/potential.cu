@@ -527,20 +527,19 @@ __global__ void k_scale_coeffs_pot(int nnodes, const TNode *__restrict__ tnode,
 
 static int sm_count_p() { return device_sm_count(); }
 
-int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out) {
+// Target sort and lists run on the auxiliary stream; `between` (the expansion work) runs on the
+// main stream meanwhile, and the evaluation waits for both.
+int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out,
+              OverlapFn between) {
     if (c.order != ORDER_POTENTIAL) {
         set_error(TC_ERR_INVALID, "potential evaluation needs an order-%d tree", ORDER_POTENTIAL);
         return TC_ERR_INVALID;
     }
-    if (m == 0) return TC_OK;
+    if (m == 0) return between ? between(c) : TC_OK;
     int rc;
     int *tkeys, *tperm, *tkeys2, *tperm2;
     if ((rc = ensure(c, S_TKEYS, m, &tkeys)) || (rc = ensure(c, S_TPERM, m, &tperm)) ||
         (rc = ensure(c, S_TKEYS2, m, &tkeys2)) || (rc = ensure(c, S_TPERM2, m, &tperm2)))
-        return rc;
-    if ((rc = target_keys(c, xt, yt, m, tkeys, nullptr))) return rc;
-    int *ko, *vo;
-    if ((rc = radix_sort_pairs(c, tkeys, nullptr, m, 2 * LMAX, tkeys2, tperm2, tkeys, tperm, &ko, &vo)))
         return rc;
     const int ngroups = (m + 31) / 32;
     // counts / offsets: E2P | P2P list lengths and evaluation tasks, ngroups each
@@ -552,28 +551,47 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     const int grid = (int)std::min<long long>((ngroups + PT_WARPS - 1) / PT_WARPS,
                                               (long long)sm_count_p() * 16);
-    k_potential_lists<false><<<grid, PT_WARPS * 32, 0, c.stream>>>(ngroups, m, xt, yt, vo, theta,
-                                                                  tnode, c.nnodes, counts, nullptr, nullptr,
-                                                                  err, nullptr);
-    TC_KERNEL_CHECK();
-    if ((rc = exclusive_scan(c, counts, offs, 3 * ngroups))) return rc;
-    for (int k = 0; k < 3; ++k)
-        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + k, offs + (k + 1) * ngroups, sizeof(int),
-                                    cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    const int n_e2p = (int)c.h_pinned[0], total = (int)c.h_pinned[1];
-    const int ntasks = (int)c.h_pinned[2] - total;
+    int *ko, *vo;
+    TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
+    {
+        AuxScope on_aux(c);
+        TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_fork, 0));
+        if ((rc = target_keys(c, xt, yt, m, tkeys, nullptr))) return rc;
+        if ((rc = radix_sort_pairs(c, tkeys, nullptr, m, 2 * LMAX, tkeys2, tperm2, tkeys, tperm,
+                                   &ko, &vo)))
+            return rc;
+        k_potential_lists<false><<<grid, PT_WARPS * 32, 0, c.stream>>>(
+            ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, counts, nullptr, nullptr, err, nullptr);
+        TC_KERNEL_CHECK();
+        if ((rc = exclusive_scan(c, counts, offs, 3 * ngroups))) return rc;
+        for (int k = 0; k < 3; ++k)
+            TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 32 + k, offs + (k + 1) * ngroups, sizeof(int),
+                                        cudaMemcpyDeviceToHost, c.stream));
+        TC_CUDA_TRY(cudaEventRecord(c.ev_totals, c.stream));
+    }
+    if (between && (rc = between(c))) {
+        cudaStreamSynchronize(c.aux);   // leave nothing of this solve in flight
+        return rc;
+    }
+    TC_CUDA_TRY(cudaEventSynchronize(c.ev_totals));
+    const int n_e2p = (int)c.h_pinned[32], total = (int)c.h_pinned[33];
+    const int ntasks = (int)c.h_pinned[34] - total;
     c.counts.n_e2p = n_e2p;
     c.counts.n_p2p = total - n_e2p;
     c.counts.n_e2l = 0;
     c.counts.e2l_pairs = 0;
     c.counts.l2p_targets = 0;
     int2 *lists;
-    if ((rc = ensure(c, S_PE2P, (size_t)total + 1, &lists))) return rc;
-    k_potential_lists<true><<<grid, PT_WARPS * 32, 0, c.stream>>>(ngroups, m, xt, yt, vo, theta,
-                                                                 tnode, c.nnodes, nullptr, offs, lists, err,
-                                                                 slot_ptr<unsigned long long>(c, S_STATS));
-    TC_KERNEL_CHECK();
+    {
+        AuxScope on_aux(c);
+        if ((rc = ensure(c, S_PE2P, (size_t)total + 1, &lists))) return rc;
+        k_potential_lists<true><<<grid, PT_WARPS * 32, 0, c.stream>>>(
+            ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, nullptr, offs, lists, err,
+            slot_ptr<unsigned long long>(c, S_STATS));
+        TC_KERNEL_CHECK();
+        TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
+    }
+    TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
     phase_mark(c, 4);
     int *task_ctr, *task_group;
     double *partial;

@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <utility>
 
 #include "tc_common.cuh"
 
@@ -67,6 +68,10 @@ struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // auxiliary stream: interaction lists are built on it while the expansions are formed on
+    // `stream`; ordered against `stream` with the events below
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_totals = nullptr, ev_join = nullptr;
     DevBuf buf[S_NUM_SLOTS];
     unsigned *h_pinned = nullptr;         // small pinned staging area for readbacks
     int precision = 0;                    // 0 = plain FP64, 1 = mixed
@@ -137,14 +142,29 @@ int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys
 int build_topology(Context &c, int leafcap);
 
 // ---- upward.cu
-int upward_pass(Context &c, int order);
+int upward_prepare(Context &c, int order);   // buffers of the upward pass, c.order
+int upward_moments(Context &c);              // leaf setup + parent moments (what traversals read)
+int upward_expansions(Context &c);           // P2E + E2E
+int upward_pass(Context &c, int order);      // all three
+
+// Swaps the context's main and auxiliary streams for the lifetime of the object, so that the
+// helpers (which all launch on c.stream) run on the auxiliary stream.
+struct AuxScope {
+    Context &c;
+    explicit AuxScope(Context &ctx) : c(ctx) { std::swap(c.stream, c.aux); }
+    ~AuxScope() { std::swap(c.stream, c.aux); }
+};
+
+// Work launched on the main stream while the interaction lists are built on the auxiliary one.
+typedef int (*OverlapFn)(Context &c);
 
 // ---- force.cu
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
-               int nblocks, double *xout, double *yout);
+               int nblocks, double *xout, double *yout, OverlapFn between);
 
 // ---- potential.cu
-int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out);
+int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out,
+              OverlapFn between);
 
 // ---- capi.cu
 int check_device_errors(Context &c, const char *where);

@@ -1,15 +1,17 @@
-// upward.cu -- the upward pass: leaf setup + P2E, then E2E level by level.
+// upward.cu -- the upward pass, in two parts.
 //
-// k_leaf_setup: four threads per node run the leaf setup with the reference's four strided
-// accumulators (drivers/upward.cpp:61-93, kernels/upward-common.ispc:13-57).
-// k_leaf_p2e: one warp per leaf forms its multipole expansion, lanes over sources with the P
-// coefficients in registers (kernels/upward-kernels.m4:18-93); FP32 lane sums in the
-// mixed-precision form.
-// k_upward_level: one launch per deep tree level, deepest first, one warp per inner node; the
-// small top levels run in one single-block launch that walks them with a block barrier between
-// levels (upward.cpp:95-218, kernels/upward-kernels.m4:95-149).  Children were finished before
-// their parent's level starts, so no atomics or fences are needed; the reference does the same
-// merges in the order its OpenMP tasks happen to finish.
+// Moments (what the traversals read): k_leaf_setup (four threads per node) runs the leaf setup
+// with the reference's four strided accumulators (drivers/upward.cpp:61-93,
+// kernels/upward-common.ispc:13-57); k_moments_level / k_moments_top then form every inner
+// node's mass, weights, com and radius level by level, deepest first (upward.cpp:95-218).
+// Expansions: k_leaf_p2e (one warp per leaf, lanes over sources, FP32 lane sums in the
+// mixed-precision form; kernels/upward-kernels.m4:18-93), then E2E deepest level first
+// (upward-kernels.m4:95-149): k_upward_wide (thread per inner node, cp.async staging) on wide
+// levels, k_upward_level (warp per inner node) on narrow ones, k_upward_top (one block) on the
+// small top levels.  Inner node r of level l is addressed structurally (its children are
+// off[l+1] + 4r .. +3, its id is their cell's parent), so the E2E does not depend on the child
+// pointers that the moments pass may rewrite.  The two parts are separate so that the
+// interaction lists can be built on another stream while the expansions are formed.
 //
 // Bit-exact restatements (decisions of the traversals depend on these values):
 //  * leaf mass / |v| weights / weighted sums: four strided lane accumulators, reduced as
@@ -235,53 +237,17 @@ __global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 5 : 3) void k_leaf_p2e(
     }
 }
 
-// ------------------------------------------------------------------------------ merge (E2E)
-// b_l = sum_c z0^l [ -m_c/l + sum_{k=1..l} C(l-1,k-1) a_{c,k-1} z0^-k ],  z0 = child com - parent
-// com.  Lane l-1 (l = 1..P) owns coefficient l of the parent for all four children; the
-// binomials C(l-1, k-1) (zero for k > l) are read from a block-shared table, row k.
-template <int P>
-struct MergeShared {
-    cplx coef[4][P];   // a_{c,k-1} z0_c^-k, k = 1..P
-};
-
-template <int P>
-struct BinomRows {
-    double b[P][32];   // b[k][lane] = C(lane, k) for k <= lane < P, else 0
-};
-
-template <int P>
-__device__ __forceinline__ void fill_binom_rows(BinomRows<P> &t) {
-    for (int i = threadIdx.x; i < P * 32; i += blockDim.x) {
-        const int k = i / 32, l = i % 32;
-        t.b[k][l] = (l < P && k <= l) ? g_binom_up.c[l][k] : 0.0;
-    }
-}
-
-template <int P>
-__device__ __forceinline__ void merge_node(int parent, int nnodes, int leafcap, double ext,
-                                           const int2 *__restrict__ range,
-                                           const int4 *__restrict__ cell, TNode *tnode,
-                                           double *mass, double *wgt, double *wxs, double *wys,
-                                           double *exps, unsigned *err, const BinomRows<P> &bt,
-                                           MergeShared<P> &sh) {
-    const int lane = lane_id();
-    const int2 prg = range[parent];
-    const int4 pcl = cell[parent];
-    const int cb = tnode[parent].child;
-    if (is_leaf(prg, pcl, leafcap)) return;
-    if (cb <= parent || cb + 4 > nnodes) {
-        if (lane == 0) atomicOr(err, DEVERR_BOUNDS);
-        return;
-    }
-    // this lane's coefficient of each child, loaded together with the children's moments
-    double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
-    if (lane < P)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const double *ex = exps + (size_t)(cb + c) * 2 * P;
-            er[c] = ex[lane];
-            ei[c] = ex[P + lane];
-        }
+// ------------------------------------------------------------------------------ moments
+// Parent moments, bit-exact (upward.cpp:95-218): sums over the children as (c0 + c3) + (c1 + c2),
+// com = wx / w, radius min(max_c |com - com_c| + r_c over weighted children, (double)1.4143f ext
+// / 2^l); when all four children are negligible child 3 becomes an empty leaf.  These are what
+// the traversals read; they run level by level before any expansion work, so that the
+// interaction lists can be built while the expansions are still being formed.
+// Inner node r of level l owns the children off[l+1] + 4r .. +3 and is their common parent
+// cell[off[l+1] + 4r].w.
+__device__ __forceinline__ void parent_moments(int l, int cb, int parent, double ext,
+                                               TNode *tnode, double *mass, double *wgt,
+                                               double *wxs, double *wys) {
     double cm[4], cw[4], cwx[4], cwy[4], cxc[4], cyc[4], cr[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -306,9 +272,117 @@ __device__ __forceinline__ void merge_node(int parent, int nnodes, int leafcap, 
             const double cand = __dadd_rn(__dsqrt_rn(__fma_rn(rx, rx, __dmul_rn(ry, ry))), cr[c]);
             rr = cand > rr ? cand : rr;
         }
-    const double cap = __ddiv_rn(__dmul_rn((double)1.4143f, ext), (double)(1 << pcl.x));
-    const double prad = cap < rr ? cap : rr;
+    const double cap = __ddiv_rn(__dmul_rn((double)1.4143f, ext), (double)(1 << l));
+    int zcount = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) zcount += fabs(cw[c]) < 1.1e-16;
+    tnode[parent].xcom = px;
+    tnode[parent].ycom = py;
+    tnode[parent].r = cap < rr ? cap : rr;
+    mass[parent] = pm;
+    wgt[parent] = pw;
+    wxs[parent] = pwx;
+    wys[parent] = pwy;
+    if (zcount == 4) {
+        tnode[cb + 3].child = -1;
+        tnode[cb + 3].count = 0;
+    }
+}
 
+__device__ __forceinline__ bool inner_node(int l, int r, const LevelOffsets &lo, int nnodes,
+                                           const int4 *__restrict__ cell, int &cb, int &parent,
+                                           unsigned *err) {
+    cb = lo.off[l + 1] + 4 * r;
+    parent = cb + 4 <= nnodes ? cell[cb].w : -1;
+    if (parent < lo.off[l] || parent >= lo.off[l + 1]) {
+        atomicOr(err, DEVERR_TREE);
+        return false;
+    }
+    return true;
+}
+
+// one level, one thread per inner node
+__global__ __launch_bounds__(256) void k_moments_level(int l, LevelOffsets lo, int nnodes,
+                                                       const int4 *__restrict__ cell, TNode *tnode,
+                                                       double *mass, double *wgt, double *wxs,
+                                                       double *wys, const Frame *__restrict__ frame,
+                                                       unsigned *err) {
+    const int ninner = (lo.off[l + 2] - lo.off[l + 1]) / 4;
+    const double ext = frame->ext;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < ninner; r += gridDim.x * blockDim.x) {
+        int cb, parent;
+        if (inner_node(l, r, lo, nnodes, cell, cb, parent, err))
+            parent_moments(l, cb, parent, ext, tnode, mass, wgt, wxs, wys);
+    }
+}
+
+// levels ltop .. 0 in one block, a block barrier between levels
+__global__ __launch_bounds__(1024) void k_moments_top(int ltop, LevelOffsets lo, int nnodes,
+                                                      const int4 *__restrict__ cell, TNode *tnode,
+                                                      double *mass, double *wgt, double *wxs,
+                                                      double *wys, const Frame *__restrict__ frame,
+                                                      unsigned *err) {
+    const double ext = frame->ext;
+    for (int l = ltop; l >= 0; --l) {
+        const int ninner = (lo.off[l + 2] - lo.off[l + 1]) / 4;
+        for (int r = threadIdx.x; r < ninner; r += blockDim.x) {
+            int cb, parent;
+            if (inner_node(l, r, lo, nnodes, cell, cb, parent, err))
+                parent_moments(l, cb, parent, ext, tnode, mass, wgt, wxs, wys);
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------ merge (E2E)
+// b_l = sum_c z0^l [ -m_c/l + sum_{k=1..l} C(l-1,k-1) a_{c,k-1} z0^-k ],  z0 = child com - parent
+// com (upward-kernels.m4:95-149).  All four children are shifted unless three or four of them
+// are negligible: four -> the parent's expansion is zero; three -> the remaining child's
+// coefficients are copied unshifted (upward.cpp:173-188).
+// Narrow levels: a warp per inner node; lane l-1 (l = 1..P) owns coefficient l of the parent
+// for all four children, with the binomials C(l-1, k-1) (zero for k > l) from a block-shared
+// table, row k.
+template <int P>
+struct MergeShared {
+    cplx coef[4][P];   // a_{c,k-1} z0_c^-k, k = 1..P
+};
+
+template <int P>
+struct BinomRows {
+    double b[P][32];   // b[k][lane] = C(lane, k) for k <= lane < P, else 0
+};
+
+template <int P>
+__device__ __forceinline__ void fill_binom_rows(BinomRows<P> &t) {
+    for (int i = threadIdx.x; i < P * 32; i += blockDim.x) {
+        const int k = i / 32, l = i % 32;
+        t.b[k][l] = (l < P && k <= l) ? g_binom_up.c[l][k] : 0.0;
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void merge_node(int cb, int parent, const TNode *tnode,
+                                           const double *mass, const double *wgt, double *exps,
+                                           const BinomRows<P> &bt, MergeShared<P> &sh) {
+    const int lane = lane_id();
+    // this lane's coefficient of each child, loaded together with the children's moments
+    double er[4] = {0, 0, 0, 0}, ei[4] = {0, 0, 0, 0};
+    if (lane < P)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double *ex = exps + (size_t)(cb + c) * 2 * P;
+            er[c] = ex[lane];
+            ei[c] = ex[P + lane];
+        }
+    double cm[4], cw[4], cxc[4], cyc[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        cm[c] = mass[cb + c];
+        cw[c] = wgt[cb + c];
+        cxc[c] = tnode[cb + c].xcom;
+        cyc[c] = tnode[cb + c].ycom;
+    }
+    const double px = tnode[parent].xcom, py = tnode[parent].ycom;
     int zcount = 0, nz = 0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -319,10 +393,6 @@ __device__ __forceinline__ void merge_node(int parent, int nnodes, int leafcap, 
     double *dst = exps + (size_t)parent * 2 * P;
     if (zcount == 4) {
         for (int k = lane; k < 2 * P; k += 32) dst[k] = 0.0;
-        if (lane == 0) {
-            tnode[cb + 3].child = -1;
-            tnode[cb + 3].count = 0;
-        }
     } else if (zcount == 3) {
         double sr = 0, si = 0;
 #pragma unroll
@@ -381,33 +451,30 @@ __device__ __forceinline__ void merge_node(int parent, int nnodes, int leafcap, 
             dst[P + lane] = (si[0] + si[1]) + (si[2] + si[3]);
         }
     }
-    if (lane == 0) {
-        tnode[parent].xcom = px;
-        tnode[parent].ycom = py;
-        tnode[parent].r = prad;
-        mass[parent] = pm;
-        wgt[parent] = pw;
-        wxs[parent] = pwx;
-        wys[parent] = pwy;
-    }
+    __syncwarp();
 }
 
-// One level: inner nodes [lo, hi), one warp each.
+// One level, one warp per inner node.
 template <int P>
 __global__ __launch_bounds__(UP_WARPS * 32, 5) void k_upward_level(
-    int lo, int hi, int nnodes, int leafcap, const int2 *__restrict__ range,
-    const int4 *__restrict__ cell, TNode *tnode, double *mass, double *wgt, double *wxs,
-    double *wys, double *exps, const Frame *__restrict__ frame, unsigned *err) {
+    int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
+    const double *mass, const double *wgt, double *exps, unsigned *err) {
     __shared__ MergeShared<P> shared[UP_WARPS];
     __shared__ BinomRows<P> bt;
     fill_binom_rows<P>(bt);
     __syncthreads();
-    const double ext = frame->ext;
     MergeShared<P> &sh = shared[threadIdx.x >> 5];
-    for (int parent = lo + blockIdx.x * UP_WARPS + (threadIdx.x >> 5); parent < hi;
-         parent += gridDim.x * UP_WARPS)
-        merge_node<P>(parent, nnodes, leafcap, ext, range, cell, tnode, mass, wgt, wxs, wys, exps,
-                      err, bt, sh);
+    const int ninner = (lo.off[l + 2] - lo.off[l + 1]) / 4;
+    for (int r = blockIdx.x * UP_WARPS + (threadIdx.x >> 5); r < ninner;
+         r += gridDim.x * UP_WARPS) {
+        int cb, parent;
+        bool ok = true;
+        if (lane_id() == 0) ok = inner_node(l, r, lo, nnodes, cell, cb, parent, err);
+        ok = __shfl_sync(FULL_MASK, ok, 0);
+        cb = __shfl_sync(FULL_MASK, cb, 0);
+        parent = __shfl_sync(FULL_MASK, parent, 0);
+        if (ok) merge_node<P>(cb, parent, tnode, mass, wgt, exps, bt, sh);
+    }
 }
 
 // Wide levels: one thread per inner node.  Inner node r of level l owns the children
@@ -449,15 +516,13 @@ __device__ __forceinline__ void stage_children(double (*buf)[33], const double *
 
 template <int P>
 __global__ __launch_bounds__(UP_WIDE_WARPS * 32, 8) void k_upward_wide(
-    int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, TNode *tnode, double *mass,
-    double *wgt, double *wxs, double *wys, double *exps, const Frame *__restrict__ frame,
-    unsigned *err) {
+    int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
+    const double *mass, const double *wgt, double *exps, unsigned *err) {
     __shared__ WideShared<P> shared[UP_WIDE_WARPS];
     WideShared<P> &st = shared[threadIdx.x >> 5];
     const int lane = lane_id();
     const int cbase = lo.off[l + 1];
     const int ninner = (lo.off[l + 2] - cbase) / 4;
-    const double ext = frame->ext;
     for (int r0 = (blockIdx.x * UP_WIDE_WARPS + (threadIdx.x >> 5)) * 32; r0 < ninner;
          r0 += gridDim.x * UP_WIDE_WARPS * 32) {
         const int r = r0 + lane;
@@ -466,58 +531,29 @@ __global__ __launch_bounds__(UP_WIDE_WARPS * 32, 8) void k_upward_wide(
         int parent = -1;
         if (act) {
             parent = cell[cb].w;
-            if (parent < lo.off[l] || parent >= lo.off[l + 1] || tnode[parent].child != cb ||
-                cb + 4 > nnodes) {
+            if (parent < lo.off[l] || parent >= lo.off[l + 1] || cb + 4 > nnodes) {
                 atomicOr(err, DEVERR_TREE);
                 act = false;
             }
         }
         st.parent[lane] = act ? parent : -1;
-        double cm[4], cw[4], cwx[4], cwy[4], cxc[4], cyc[4], cr[4];
+        double cm[4], cw[4], cxc[4], cyc[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int id = act ? cb + c : 0;
             cm[c] = mass[id];
             cw[c] = wgt[id];
-            cwx[c] = wxs[id];
-            cwy[c] = wys[id];
             cxc[c] = tnode[id].xcom;
             cyc[c] = tnode[id].ycom;
-            cr[c] = tnode[id].r;
         }
-        const double pm = __dadd_rn(__dadd_rn(cm[0], cm[3]), __dadd_rn(cm[1], cm[2]));
-        const double pw = __dadd_rn(__dadd_rn(cw[0], cw[3]), __dadd_rn(cw[1], cw[2]));
-        const double pwx = __dadd_rn(__dadd_rn(cwx[0], cwx[3]), __dadd_rn(cwx[1], cwx[2]));
-        const double pwy = __dadd_rn(__dadd_rn(cwy[0], cwy[3]), __dadd_rn(cwy[1], cwy[2]));
-        const double px = __ddiv_rn(pwx, pw), py = __ddiv_rn(pwy, pw);
-        double rr = 0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            if (cw[c] != 0) {
-                const double rx = __dsub_rn(px, cxc[c]), ry = __dsub_rn(py, cyc[c]);
-                const double cand = __dadd_rn(__dsqrt_rn(__fma_rn(rx, rx, __dmul_rn(ry, ry))), cr[c]);
-                rr = cand > rr ? cand : rr;
-            }
+        // the parent's com comes from the moments pass
+        const double px = act ? tnode[parent].xcom : 0.0, py = act ? tnode[parent].ycom : 0.0;
         int zcount = 0, nz = 0;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const bool negl = fabs(cw[c]) < 1.1e-16;
             zcount += negl;
             if (!negl) nz = c;
-        }
-        if (act) {
-            const double cap = __ddiv_rn(__dmul_rn((double)1.4143f, ext), (double)(1 << l));
-            tnode[parent].xcom = px;
-            tnode[parent].ycom = py;
-            tnode[parent].r = cap < rr ? cap : rr;
-            mass[parent] = pm;
-            wgt[parent] = pw;
-            wxs[parent] = pwx;
-            wys[parent] = pwy;
-            if (zcount == 4) {
-                tnode[cb + 3].child = -1;
-                tnode[cb + 3].count = 0;
-            }
         }
         const bool shift = act && zcount <= 2;
 #pragma unroll
@@ -586,43 +622,91 @@ __global__ __launch_bounds__(UP_WIDE_WARPS * 32, 8) void k_upward_wide(
 // level's writes before its parents' reads.
 template <int P>
 __global__ __launch_bounds__(UP_TOP_WARPS * 32) void k_upward_top(
-    int ltop, LevelOffsets level_off, int nnodes, int leafcap,
-    const int2 *__restrict__ range, const int4 *__restrict__ cell, TNode *tnode, double *mass,
-    double *wgt, double *wxs, double *wys, double *exps, const Frame *__restrict__ frame,
-    unsigned *err) {
+    int ltop, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
+    const double *mass, const double *wgt, double *exps, unsigned *err) {
     __shared__ MergeShared<P> shared[UP_TOP_WARPS];
     __shared__ BinomRows<P> bt;
     fill_binom_rows<P>(bt);
     __syncthreads();
-    const double ext = frame->ext;
     const int warp = threadIdx.x >> 5;
     MergeShared<P> &sh = shared[warp];
     for (int l = ltop; l >= 0; --l) {
-        const int lo = level_off.off[l], hi = level_off.off[l + 1];
-        for (int parent = lo + warp; parent < hi; parent += UP_TOP_WARPS)
-            merge_node<P>(parent, nnodes, leafcap, ext, range, cell, tnode, mass, wgt, wxs, wys,
-                          exps, err, bt, sh);
+        const int ninner = (lo.off[l + 2] - lo.off[l + 1]) / 4;
+        for (int r = warp; r < ninner; r += UP_TOP_WARPS) {
+            int cb = 0, parent = 0;
+            bool ok = true;
+            if (lane_id() == 0) ok = inner_node(l, r, lo, nnodes, cell, cb, parent, err);
+            ok = __shfl_sync(FULL_MASK, ok, 0);
+            cb = __shfl_sync(FULL_MASK, cb, 0);
+            parent = __shfl_sync(FULL_MASK, parent, 0);
+            if (ok) merge_node<P>(cb, parent, tnode, mass, wgt, exps, bt, sh);
+        }
         __syncthreads();
     }
 }
 
 static int sm_count_up() { return device_sm_count(); }
 
-template <int P>
-static int run_upward(Context &c, double *mass, double *w, double *wx, double *wy, double *exps) {
+// Largest level ltop such that levels 0 .. ltop all have at most `limit` inner nodes (-1: none).
+static int small_top(const Context &c, int limit) {
+    int ltop = -1;
+    while (ltop + 1 < LMAX && (c.level_off[ltop + 3] - c.level_off[ltop + 2]) / 4 <= limit) ++ltop;
+    return ltop;
+}
+
+static LevelOffsets level_offsets(const Context &c) {
+    LevelOffsets offs;
+    for (int l = 0; l < LMAX + 3; ++l) offs.off[l] = c.level_off[l];
+    return offs;
+}
+
+constexpr int MOM_TOP_MAX = 1024;   // levels with at most this many inner nodes: one block
+
+int upward_moments(Context &c) {
     const int nn = c.nnodes;
-    const double *xs = slot_ptr<double>(c, S_XS), *ys = slot_ptr<double>(c, S_YS),
-                 *vs = slot_ptr<double>(c, S_VS);
     const int2 *range = slot_ptr<int2>(c, S_RANGE);
     const int4 *cell = slot_ptr<int4>(c, S_CELL);
     TNode *tnode = slot_ptr<TNode>(c, S_TNODE);
     const Frame *frame = slot_ptr<Frame>(c, S_FRAME);
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    double *mass = slot_ptr<double>(c, S_MASS), *w = slot_ptr<double>(c, S_W),
+           *wx = slot_ptr<double>(c, S_WX), *wy = slot_ptr<double>(c, S_WY);
+    k_leaf_setup<<<(int)(((long long)nn * 4 + 255) / 256), 256, 0, c.stream>>>(
+        nn, c.nsrc, c.leafcap, slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
+        slot_ptr<double>(c, S_VS), range, cell, tnode, mass, w, wx, wy, frame, err);
+    TC_KERNEL_CHECK();
+    // inner nodes exist on levels 0 .. LMAX-1, deepest first
+    const LevelOffsets offs = level_offsets(c);
+    const int ltop = small_top(c, MOM_TOP_MAX);
+    for (int l = LMAX - 1; l > ltop; --l) {
+        const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
+        if (ninner <= 0) continue;
+        k_moments_level<<<(ninner + 255) / 256, 256, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
+                                                                    wx, wy, frame, err);
+        TC_KERNEL_CHECK();
+    }
+    if (ltop >= 0) {
+        k_moments_top<<<1, MOM_TOP_MAX, 0, c.stream>>>(ltop, offs, nn, cell, tnode, mass, w, wx, wy,
+                                                       frame, err);
+        TC_KERNEL_CHECK();
+    }
+    return TC_OK;
+}
+
+template <int P>
+static int run_expansions(Context &c) {
+    const int nn = c.nnodes;
+    const double *xs = slot_ptr<double>(c, S_XS), *ys = slot_ptr<double>(c, S_YS),
+                 *vs = slot_ptr<double>(c, S_VS);
+    const int2 *range = slot_ptr<int2>(c, S_RANGE);
+    const int4 *cell = slot_ptr<int4>(c, S_CELL);
+    const TNode *tnode = slot_ptr<TNode>(c, S_TNODE);
+    const Frame *frame = slot_ptr<Frame>(c, S_FRAME);
+    unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    const double *mass = slot_ptr<double>(c, S_MASS), *w = slot_ptr<double>(c, S_W);
+    double *exps = slot_ptr<double>(c, S_EXPS);
     const int sms = sm_count_up();
 
-    k_leaf_setup<<<(int)(((long long)nn * 4 + 255) / 256), 256, 0, c.stream>>>(
-        nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell, tnode, mass, w, wx, wy, frame, err);
-    TC_KERNEL_CHECK();
     const bool mixed = c.precision == 1;
     const size_t smem64 = UP_WARPS * sizeof(LeafShared<P, double>);
     const size_t smem32 = UP_WARPS * sizeof(LeafShared<P, float>);
@@ -639,39 +723,38 @@ static int run_upward(Context &c, double *mass, double *w, double *wx, double *w
     p2e<<<grid, UP_WARPS * 32, smem, c.stream>>>(nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell,
                                                  tnode, exps, frame);
     TC_KERNEL_CHECK();
-    // Inner nodes exist on levels 0 .. LMAX-1; level l occupies [level_off[l], level_off[l+1]).
-    // Levels 0 .. ltop are all small: they run in one single-block launch after the others.
-    int ltop = -1;
-    while (ltop + 1 < LMAX && c.level_off[ltop + 2] - c.level_off[ltop + 1] <= UP_TOP_MAX_NODES)
-        ++ltop;
-    LevelOffsets offs;
-    for (int l = 0; l < LMAX + 3; ++l) offs.off[l] = c.level_off[l];
+    // E2E deepest level first: wide levels thread per node, narrow ones warp per node, the
+    // small top levels in one single-block launch
+    const LevelOffsets offs = level_offsets(c);
+    const int ltop = small_top(c, UP_TOP_MAX_NODES);
     for (int l = LMAX - 1; l > ltop; --l) {
-        const int lo = c.level_off[l], hi = c.level_off[l + 1];
         const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
-        if (hi <= lo || ninner <= 0) continue;
+        if (ninner <= 0) continue;
         if (ninner >= UP_WIDE_MIN_NODES) {
             const int g = (int)std::min<long long>(
                 (ninner + UP_WIDE_WARPS * 32 - 1) / (UP_WIDE_WARPS * 32), (long long)sms * 8);
-            k_upward_wide<P><<<g, UP_WIDE_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
-                                                                wx, wy, exps, frame, err);
+            k_upward_wide<P><<<g, UP_WIDE_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass,
+                                                                     w, exps, err);
         } else {
-            const int g = (int)std::min<long long>((hi - lo + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
-            k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(lo, hi, nn, c.leafcap, range,
-                                                                 cell, tnode, mass, w, wx, wy,
-                                                                 exps, frame, err);
+            const int g = (int)std::min<long long>((ninner + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
+            k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
+                                                                 exps, err);
         }
         TC_KERNEL_CHECK();
     }
     if (ltop >= 0) {
-        k_upward_top<P><<<1, UP_TOP_WARPS * 32, 0, c.stream>>>(
-            ltop, offs, nn, c.leafcap, range, cell, tnode, mass, w, wx, wy, exps, frame, err);
+        k_upward_top<P><<<1, UP_TOP_WARPS * 32, 0, c.stream>>>(ltop, offs, nn, cell, tnode, mass, w,
+                                                               exps, err);
         TC_KERNEL_CHECK();
     }
     return TC_OK;
 }
 
-int upward_pass(Context &c, int order) {
+int upward_prepare(Context &c, int order) {
+    if (order != ORDER_POTENTIAL && order != ORDER_FORCE) {
+        set_error(TC_ERR_INVALID, "unsupported expansion order %d", order);
+        return TC_ERR_INVALID;
+    }
     const int nn = c.nnodes;
     int rc;
     double *mass, *w, *wx, *wy, *exps;
@@ -679,16 +762,19 @@ int upward_pass(Context &c, int order) {
         (rc = ensure(c, S_WX, nn, &wx)) || (rc = ensure(c, S_WY, nn, &wy)) ||
         (rc = ensure(c, S_EXPS, (size_t)nn * 2 * order, &exps)))
         return rc;
-    if (order == ORDER_POTENTIAL)
-        rc = run_upward<ORDER_POTENTIAL>(c, mass, w, wx, wy, exps);
-    else if (order == ORDER_FORCE)
-        rc = run_upward<ORDER_FORCE>(c, mass, w, wx, wy, exps);
-    else {
-        set_error(TC_ERR_INVALID, "unsupported expansion order %d", order);
-        return TC_ERR_INVALID;
-    }
-    if (rc) return rc;
     c.order = order;
+    return TC_OK;
+}
+
+int upward_expansions(Context &c) {
+    return c.order == ORDER_POTENTIAL ? run_expansions<ORDER_POTENTIAL>(c)
+                                      : run_expansions<ORDER_FORCE>(c);
+}
+
+int upward_pass(Context &c, int order) {
+    int rc;
+    if ((rc = upward_prepare(c, order)) || (rc = upward_moments(c)) || (rc = upward_expansions(c)))
+        return rc;
     return TC_OK;
 }
 
