@@ -101,6 +101,16 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
         TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
     }
+    // freed pool blocks stay cached in the process for the next allocation (the default release
+    // threshold of 0 would hand them back to the driver at every synchronisation)
+    static const cudaError_t pool_rc = [device] {
+        cudaMemPool_t pool;
+        cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, device);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = UINT64_MAX;
+        return cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }();
+    TC_CUDA_TRY(pool_rc);
     TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_totals, cudaEventDisableTiming));
@@ -117,12 +127,19 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     return TC_OK;
 }
 
+// Hands the pool blocks that no context holds back to the driver.
+static void release_pool_cache(int device) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+}
+
 static void context_free(Context &c) {
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
+    if (c.aux) cudaStreamSynchronize(c.aux);
     for (auto &b : c.buf)
         if (b.p) cudaFree(b.p);
-    if (c.aux) cudaStreamSynchronize(c.aux);
+    release_pool_cache(c.device);
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join})
@@ -415,6 +432,7 @@ TC_API int tc_context_trim(tc_context *ctx) {
     Context &c = ctx->c;
     cudaSetDevice(c.device);
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    TC_CUDA_TRY(cudaStreamSynchronize(c.aux));
     for (int s = 0; s < S_NUM_SLOTS; ++s) {
         if (s == S_ERR || s == S_STATS) continue;   // created with the context, tiny
         DevBuf &b = c.buf[s];
@@ -422,6 +440,7 @@ TC_API int tc_context_trim(tc_context *ctx) {
         b.p = nullptr;
         b.bytes = 0;
     }
+    release_pool_cache(c.device);
     c.nnodes = c.nsrc = 0;
     return TC_OK;
 }

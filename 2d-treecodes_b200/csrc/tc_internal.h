@@ -87,6 +87,11 @@ struct Context {
     Frame frame_h = {};
 };
 
+// Buffers come from the device's stream-ordered pool (cudaMallocAsync on the context's current
+// stream): growing one frees the old block in stream order instead of synchronising the device,
+// and a context created or grown while other contexts compute does not stall them.  Work on the
+// auxiliary stream is ordered against the main stream by events, so a block freed on either
+// stream is no longer in use on the other.
 template <class T>
 int ensure(Context &c, Slot s, size_t count, T **out) {
     size_t need = count * sizeof(T);
@@ -94,16 +99,16 @@ int ensure(Context &c, Slot s, size_t count, T **out) {
     DevBuf &b = c.buf[s];
     if (b.bytes < need) {
         if (b.p) {
-            cudaError_t e = cudaStreamSynchronize(c.stream);
-            if (e != cudaSuccess) { set_error(TC_ERR_CUDA, "sync before realloc: %s", cudaGetErrorString(e)); return TC_ERR_CUDA; }
-            cudaFree(b.p);
+            cudaFreeAsync(b.p, c.stream);
             b.p = nullptr;
             b.bytes = 0;
         }
         size_t alloc = need + need / 8;   // headroom for the next call
-        cudaError_t e = cudaMalloc(&b.p, alloc);
+        cudaError_t e = cudaMallocAsync(&b.p, alloc, c.stream);
         if (e != cudaSuccess) {
-            set_error(TC_ERR_ALLOC, "cudaMalloc(%zu bytes) failed: %s", alloc, cudaGetErrorString(e));
+            b.p = nullptr;
+            set_error(TC_ERR_ALLOC, "cudaMallocAsync(%zu bytes) failed: %s", alloc,
+                      cudaGetErrorString(e));
             return TC_ERR_ALLOC;
         }
         b.bytes = alloc;

@@ -31,8 +31,24 @@ DISTRIBUTIONS = ("uniform", "gaussian_mixture", "lamb_oseen", "vortex_sheet")
 THETAS = (0.3, 0.5, 0.7)
 
 
+def pinned_empty(n):
+    """A float64 host array in page-locked memory (torch's pinned allocator), so that the
+    library's host-to-device copies of it are direct DMA; plain memory without torch."""
+    try:
+        import torch
+        return torch.empty(int(n), dtype=torch.float64, pin_memory=True).numpy()
+    except Exception:   # no CUDA driver: pageable memory works too, only slower
+        return np.empty(int(n))
+
+
+def pinned_copy(a):
+    out = pinned_empty(len(a))
+    out[:] = a
+    return out
+
+
 def _masters(log2_max, seed):
-    """Per distribution: x, y and an unnormalised value array of 2^log2_max points."""
+    """Per distribution: x, y and an unnormalised value array of 2^log2_max points (pinned)."""
     n = 1 << log2_max
     r = np.random.Generator(np.random.PCG64(seed))
     out = {}
@@ -44,6 +60,7 @@ def _masters(log2_max, seed):
     out["lamb_oseen"] = (lo["xs"], lo["ys"], lo["vs"] * n, True)      # value * N
     vs = W.vortex_sheet_force(n=n, blocks_per_side=1, seed=seed + 4)
     out["vortex_sheet"] = (vs["xs"], vs["ys"], vs["vs"] * n, True)
+    out = {k: (pinned_copy(a), pinned_copy(b), pinned_copy(c), sc) for k, (a, b, c, sc) in out.items()}
     noise = r.standard_normal(2 * n)
     return out, noise
 

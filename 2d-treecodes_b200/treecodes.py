@@ -321,13 +321,16 @@ class Server:
     request's queue / service / latency times.  Host arrays are kept alive here until waited.
     """
 
-    def __init__(self, slots=4, hbm_budget_bytes=32 << 30, device=-1):
+    def __init__(self, slots=4, hbm_budget_bytes=32 << 30, device=-1, host_alloc=None):
+        """host_alloc(n) -> float64 array for the outputs (e.g. page-locked memory, so that the
+        results come back by direct DMA); numpy's allocator by default."""
         self.lib = load()
         h = _vp()
         _check(self.lib.tc_server_create(ctypes.byref(h), int(device), int(slots),
                                          int(hbm_budget_bytes)))
         self.h = h
         self._live = {}
+        self._alloc = host_alloc or np.empty
 
     def _submit(self, req, keep, outs):
         t = ctypes.c_longlong()
@@ -337,7 +340,7 @@ class Server:
 
     def submit_potential(self, theta, xs, ys, vs, xt, yt, precision=0, client=0):
         xs, ys, vs, xt, yt = map(_f64, (xs, ys, vs, xt, yt))
-        out = np.empty(len(xt))
+        out = self._alloc(len(xt))
         req = Request(kind=REQUEST_POTENTIAL, precision=int(precision), theta=float(theta),
                       client=int(client), nsources=len(xs), xsources=_p(xs), ysources=_p(ys),
                       sourcevalues=_p(vs), ntargets=len(xt), xtargets=_p(xt), ytargets=_p(yt),
@@ -347,7 +350,7 @@ class Server:
     def submit_force(self, theta, xs, ys, vs, x0s, y0s, hs, precision=0, client=0):
         xs, ys, vs, x0, y0, h = map(_f64, (xs, ys, vs, x0s, y0s, hs))
         nt = len(x0) * BLOCKSIZE * BLOCKSIZE
-        xo, yo = np.empty(nt), np.empty(nt)
+        xo, yo = self._alloc(nt), self._alloc(nt)
         req = Request(kind=REQUEST_FORCE_MRAG, precision=int(precision), theta=float(theta),
                       client=int(client), nsources=len(xs), xsources=_p(xs), ysources=_p(ys),
                       sourcevalues=_p(vs), nblocks=len(x0), x0s=_p(x0), y0s=_p(y0), hs=_p(h),
