@@ -238,32 +238,6 @@ __global__ __launch_bounds__(256) void k_keys_hist(const double *__restrict__ x,
     }
 }
 
-// Block-wide exclusive scan of one int per thread (blockDim.x a multiple of 32, <= 1024).
-__device__ int block_exclusive_scan(int v, int *total) {
-    __shared__ int warp_sums[32];
-    const int lane = lane_id(), w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    int inc = v;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(FULL_MASK, inc, o);
-        if (lane >= o) inc += t;
-    }
-    __syncthreads();
-    if (lane == 31) warp_sums[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        int s = lane < nw ? warp_sums[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(FULL_MASK, s, o);
-            if (lane >= o) s += t;
-        }
-        if (lane < nw) warp_sums[lane] = s;
-    }
-    __syncthreads();
-    const int base = w ? warp_sums[w - 1] : 0;
-    if (total) *total = warp_sums[nw - 1];
-    return base + inc - v;
-}
-
 __global__ __launch_bounds__(RS_RADIX) void k_hist_scan(const int *__restrict__ hist,
                                                         int *__restrict__ offsets) {
     const int p = blockIdx.x;

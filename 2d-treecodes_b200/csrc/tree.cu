@@ -39,47 +39,100 @@ __device__ __forceinline__ int lower_bound_dev(const int *__restrict__ keys, int
     return lo;
 }
 
-__global__ void k_tree_mask(const int *__restrict__ keys, int n, int leafcap,
-                            unsigned short *__restrict__ mask, int *__restrict__ flag) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int k = keys[i];
-        const int cprev = i == 0 ? -1 : common_level(keys[i - 1], k);
-        const int cnext = i + leafcap < n ? common_level(k, keys[i + leafcap]) : -1;
-        const int hi = min(cnext, LMAX - 1);
-        unsigned m = 0;
-        for (int l = cprev + 1; l <= hi; ++l) m |= 1u << l;
-        mask[i] = (unsigned short)m;
-        flag[i] = m != 0;
-    }
-}
+// The split list: per tile of TL_TILE sources, each source's level mask (bit l: it starts an
+// inner cell of level l), a block scan
+// of the flags and the tile's global offset by a decoupled look-back over the tiles before it
+// (tile ids from an atomic counter, so a tile only waits on tiles already running; the wait is
+// bounded and raises DEVERR_SPIN_LIMIT).  The tile that holds the last source writes the list
+// length to *nlist_out.
+constexpr int TL_THREADS = 256;
+constexpr int TL_ITEMS = 16;
+constexpr int TL_TILE = TL_THREADS * TL_ITEMS;
+constexpr unsigned TL_AGG = 1u << 30, TL_INC = 2u << 30, TL_VAL = (1u << 30) - 1;
+constexpr int TL_SPIN_LIMIT = 1 << 22;
 
-__global__ void k_tree_compact(const unsigned short *__restrict__ mask,
-                               const int *__restrict__ off, int n, int cap,
-                               int *__restrict__ lpos, unsigned short *__restrict__ lmask,
-                               unsigned *err) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const unsigned m = mask[i];
-        if (m) {
-            const int j = off[i];
-            if (j >= cap) {
-                atomicOr(err, DEVERR_TREE);
-                continue;
-            }
-            lpos[j] = i;
-            lmask[j] = (unsigned short)m;
+__global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict__ keys, int n,
+                                                          int leafcap, int cap, unsigned *status,
+                                                          int *tile_counter, int *__restrict__ lpos,
+                                                          unsigned short *__restrict__ lmask,
+                                                          int *nlist_out, unsigned *err) {
+    __shared__ int s_tile, s_excl;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1);
+    __syncthreads();
+    const int tile = s_tile;
+    const int i0 = tile * TL_TILE + threadIdx.x * TL_ITEMS;   // this thread's 16 sources
+    unsigned short m[TL_ITEMS];
+    int cnt = 0;
+    int prev = i0 > 0 && i0 <= n ? keys[i0 - 1] : 0;
+#pragma unroll
+    for (int k = 0; k < TL_ITEMS; ++k) {
+        const int i = i0 + k;
+        unsigned mk = 0;
+        if (i < n) {
+            const int key = keys[i];
+            const int cprev = i == 0 ? -1 : common_level(prev, key);
+            const int cnext = i + leafcap < n ? common_level(key, keys[i + leafcap]) : -1;
+            const int hi = min(cnext, LMAX - 1);
+            for (int l = cprev + 1; l <= hi; ++l) mk |= 1u << l;
+            prev = key;
         }
+        m[k] = (unsigned short)mk;
+        cnt += mk != 0;
     }
+    int total;
+    const int toff = block_exclusive_scan(cnt, &total);
+    if (threadIdx.x == 0) {
+        unsigned *mine = status + tile;
+        int excl = 0;
+        if (tile == 0) {
+            atomicExch(mine, TL_INC | (unsigned)total);
+        } else {
+            atomicExch(mine, TL_AGG | (unsigned)total);
+            int spins = 0;
+            for (int j = tile - 1; j >= 0;) {
+                const unsigned st = *(const volatile unsigned *)(status + j);
+                const unsigned flag = st & ~TL_VAL;
+                if (flag == 0) {
+                    if (++spins > TL_SPIN_LIMIT) {
+                        atomicOr(err, DEVERR_SPIN_LIMIT);
+                        break;
+                    }
+                    continue;
+                }
+                excl += (int)(st & TL_VAL);
+                if (flag == TL_INC) break;
+                --j;
+            }
+            atomicExch(mine, TL_INC | (unsigned)(excl + total));
+        }
+        s_excl = excl;
+        if ((long long)(tile + 1) * TL_TILE >= n) *nlist_out = excl + total;
+    }
+    __syncthreads();
+    int j = s_excl + toff;
+#pragma unroll
+    for (int k = 0; k < TL_ITEMS; ++k)
+        if (m[k]) {
+            if (j < cap) {
+                lpos[j] = i0 + k;
+                lmask[j] = m[k];
+            } else {
+                atomicOr(err, DEVERR_TREE);
+            }
+            ++j;
+        }
 }
 
 constexpr int RANK_THREADS = 1024;
 
 // Per block of 1024 list entries: how many have bit l, for every level l.
 __global__ __launch_bounds__(RANK_THREADS) void k_rank_count(const unsigned short *__restrict__ lmask,
-                                                             int nlist, int *__restrict__ blk,
-                                                             int nblk) {
+                                                             const int *__restrict__ d_nlist,
+                                                             int *__restrict__ blk, int nblk) {
     __shared__ int s_cnt[LMAX];
     if (threadIdx.x < LMAX) s_cnt[threadIdx.x] = 0;
     __syncthreads();
+    const int nlist = *d_nlist;
     const int j = blockIdx.x * RANK_THREADS + threadIdx.x;
     const unsigned m = j < nlist ? lmask[j] : 0u;
     for (int l = 0; l < LMAX; ++l) {
@@ -122,12 +175,13 @@ __global__ __launch_bounds__(1024) void k_rank_scan(int *__restrict__ blk, int n
         }
 }
 
-// rank[l * nlist + j] = number of list entries before j that have bit l.
+// rank[l * stride + j] = number of list entries before j that have bit l.
 __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned short *__restrict__ lmask,
-                                                             int nlist,
+                                                             const int *__restrict__ d_nlist,
                                                              const int *__restrict__ blk, int nblk,
-                                                             int *__restrict__ rank) {
+                                                             int *__restrict__ rank, int stride) {
     __shared__ int s_w[LMAX][RANK_THREADS / 32];
+    const int nlist = *d_nlist;
     const int j = blockIdx.x * RANK_THREADS + threadIdx.x;
     const int w = threadIdx.x >> 5;
     const unsigned m = j < nlist ? lmask[j] : 0u;
@@ -152,7 +206,7 @@ __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned shor
 #pragma unroll
         for (int l = 0; l < LMAX; ++l)
             if ((m >> l) & 1u)
-                rank[(size_t)l * nlist + j] =
+                rank[(size_t)l * stride + j] =
                     blk[(size_t)l * nblk + blockIdx.x] + s_w[l][w] + __popc(bal[l] & lt);
     }
 }
@@ -168,7 +222,8 @@ __global__ void k_tree_root(int n, int leafcap, TNode *tnode, int2 *range, int4 
 __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap,
                                 const int *__restrict__ lpos,
                                 const unsigned short *__restrict__ lmask, int nlist,
-                                const int *__restrict__ rank, LevelOffsets lo, int nnodes,
+                                const int *__restrict__ rank, int stride, LevelOffsets lo,
+                                int nnodes,
                                 TNode *__restrict__ tnode, int2 *__restrict__ range,
                                 int4 *__restrict__ cell, unsigned *err) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nlist; j += gridDim.x * blockDim.x) {
@@ -191,9 +246,9 @@ __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap
                     atomicOr(err, DEVERR_TREE);
                     continue;
                 }
-                id = lo.off[l] + 4 * rank[(size_t)(l - 1) * nlist + jp] + (P & 3);
+                id = lo.off[l] + 4 * rank[(size_t)(l - 1) * stride + jp] + (P & 3);
             }
-            const int base = lo.off[l + 1] + 4 * rank[(size_t)l * nlist + j];
+            const int base = lo.off[l + 1] + 4 * rank[(size_t)l * stride + j];
             if (id < 0 || id >= nnodes || base < 0 || base + 4 > nnodes) {
                 atomicOr(err, DEVERR_BOUNDS);
                 continue;
@@ -229,51 +284,46 @@ int build_topology(Context &c, int leafcap) {
     const int n = c.nsrc;
     int rc;
     const int *keys = slot_ptr<int>(c, S_KEYS);
-    unsigned short *mask;
-    int *flag, *off;
-    if ((rc = ensure(c, S_TMASK, n, &mask)) || (rc = ensure(c, S_TFLAG, n, &flag)) ||
-        (rc = ensure(c, S_TOFF, (size_t)n + 1, &off)))
-        return rc;
-    k_tree_mask<<<grid_for_tree(n, 256), 256, 0, c.stream>>>(keys, n, leafcap, mask, flag);
-    TC_KERNEL_CHECK();
-    if ((rc = exclusive_scan(c, flag, off, n))) return rc;
-    // The list length is needed to size the rank pass: read it back with the level totals.
-    // Upper bound first (every inner cell has > leafcap sources in one level): n/(L+1) per level.
+    // Upper bound of the list length (every inner cell has > leafcap sources in one level):
+    // n/(L+1) per level.  The rank arrays are laid out with this stride, so nothing waits for
+    // the actual length before the level totals are read back.
     const long long bound = (long long)LMAX * (n / (leafcap + 1) + 1);
     const int cap = (int)(bound < n ? bound : n);
-    int *lpos, *rank, *blkc, *totals;
+    const int ntl = (n + TL_TILE - 1) / TL_TILE;
+    const int nblk = (cap + RANK_THREADS - 1) / RANK_THREADS;
+    int *lpos, *rank, *blkc, *totals, *tl_counter;
+    unsigned *tl_status;
     unsigned short *lmask;
     if ((rc = ensure(c, S_LPOS, (size_t)cap + 1, &lpos)) ||
-        (rc = ensure(c, S_LMASK, (size_t)cap + 1, &lmask)))
+        (rc = ensure(c, S_LMASK, (size_t)cap + 1, &lmask)) ||
+        (rc = ensure(c, S_TFLAG, (size_t)ntl + 8, &tl_status)) ||
+        (rc = ensure(c, S_LRANK, (size_t)LMAX * (cap + 1), &rank)) ||
+        (rc = ensure(c, S_LBLK, (size_t)LMAX * (nblk + 1), &blkc)) ||
+        (rc = ensure(c, S_LEVEL_TOTALS, LMAX + 4, &totals)))
         return rc;
-    k_tree_compact<<<grid_for_tree(n, 256), 256, 0, c.stream>>>(mask, off, n, cap, lpos, lmask,
-                                                                slot_ptr<unsigned>(c, S_ERR));
+    int *d_nlist = totals + LMAX;
+    tl_counter = totals + LMAX + 1;
+    TC_CUDA_TRY(cudaMemsetAsync(totals, 0, sizeof(int) * (LMAX + 4), c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(tl_status, 0, sizeof(unsigned) * ntl, c.stream));
+    unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    k_tree_list<<<ntl, TL_THREADS, 0, c.stream>>>(keys, n, leafcap, cap, tl_status, tl_counter,
+                                                   lpos, lmask, d_nlist, err);
     TC_KERNEL_CHECK();
-    // read back the list length
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, off + n, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    k_rank_count<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk);
+    TC_KERNEL_CHECK();
+    k_rank_scan<<<LMAX, 1024, 0, c.stream>>>(blkc, nblk, totals);
+    TC_KERNEL_CHECK();
+    k_rank_apply<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk, rank, cap);
+    TC_KERNEL_CHECK();
+    // the level totals and the list length, in one read-back
+    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, totals, sizeof(int) * (LMAX + 1),
+                                cudaMemcpyDeviceToHost, c.stream));
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    const int nlist = (int)c.h_pinned[0];
+    const int nlist = (int)c.h_pinned[LMAX];
     if (nlist > cap) {
         set_error(TC_ERR_INVALID, "tree list length %d exceeds its bound %d", nlist, cap);
         return TC_ERR_INVALID;
     }
-    const int nblk = (nlist + RANK_THREADS - 1) / RANK_THREADS;
-    if ((rc = ensure(c, S_LRANK, (size_t)LMAX * (nlist + 1), &rank)) ||
-        (rc = ensure(c, S_LBLK, (size_t)LMAX * (nblk + 1), &blkc)) ||
-        (rc = ensure(c, S_LEVEL_TOTALS, LMAX + 1, &totals)))
-        return rc;
-    TC_CUDA_TRY(cudaMemsetAsync(totals, 0, sizeof(int) * (LMAX + 1), c.stream));
-    if (nlist > 0) {
-        k_rank_count<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, nlist, blkc, nblk);
-        TC_KERNEL_CHECK();
-        k_rank_scan<<<LMAX, 1024, 0, c.stream>>>(blkc, nblk, totals);
-        TC_KERNEL_CHECK();
-        k_rank_apply<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, nlist, blkc, nblk, rank);
-        TC_KERNEL_CHECK();
-    }
-    TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, totals, sizeof(int) * LMAX, cudaMemcpyDeviceToHost,
-                                c.stream));
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
     LevelOffsets lo;
     lo.off[0] = 0;
     lo.off[1] = 1;
@@ -309,7 +359,7 @@ int build_topology(Context &c, int leafcap) {
     TC_KERNEL_CHECK();
     if (nlist > 0) {
         k_tree_children<<<grid_for_tree(nlist, 128), 128, 0, c.stream>>>(
-            keys, n, leafcap, lpos, lmask, nlist, rank, lo, c.nnodes, tnode, range, cell,
+            keys, n, leafcap, lpos, lmask, nlist, rank, cap, lo, c.nnodes, tnode, range, cell,
             slot_ptr<unsigned>(c, S_ERR));
         TC_KERNEL_CHECK();
     }
