@@ -29,7 +29,7 @@ enum Slot {
     // scan scratch
     S_SCAN_BLOCKS,
     // tree build
-    S_TMASK, S_TFLAG, S_TOFF, S_LPOS, S_LMASK, S_LRANK, S_LBLK, S_LEVEL_TOTALS,
+    S_TMASK, S_TFLAG, S_TOFF, S_LPOS, S_LMASK, S_LRANK, S_LINV, S_LBLK, S_LEVEL_TOTALS,
     // nodes
     S_TNODE, S_RANGE, S_CELL, S_MASS, S_W, S_WX, S_WY, S_EXPS, S_UPCNT,
     // force traversal / lists

@@ -39,6 +39,19 @@ __device__ __forceinline__ int lower_bound_dev(const int *__restrict__ keys, int
     return lo;
 }
 
+// The same bound, found by doubling steps from lo first: O(log(answer - lo)) reads, which is
+// what pays for the many small cells of the deep levels.
+__device__ __forceinline__ int gallop_lower_bound(const int *__restrict__ keys, int lo, int hi,
+                                                  int val) {
+    if (lo >= hi || keys[lo] >= val) return lo;
+    int a = lo, step = 1;   // keys[a] < val
+    while (a + step < hi && keys[a + step] < val) {
+        a += step;
+        step <<= 1;
+    }
+    return lower_bound_dev(keys, a + 1, min(a + step, hi), val);
+}
+
 // The split list: per tile of TL_TILE sources, each source's level mask (bit l: it starts an
 // inner cell of level l), a block scan
 // of the flags and the tile's global offset by a decoupled look-back over the tiles before it
@@ -175,11 +188,14 @@ __global__ __launch_bounds__(1024) void k_rank_scan(int *__restrict__ blk, int n
         }
 }
 
-// rank[l * stride + j] = number of list entries before j that have bit l.
+// rank[l * stride + j] = number of list entries before j that have bit l (for every entry j,
+// with or without bit l).
+// inv[l * stride + r] = the entry whose level-l inner cell has rank r.
 __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned short *__restrict__ lmask,
                                                              const int *__restrict__ d_nlist,
                                                              const int *__restrict__ blk, int nblk,
-                                                             int *__restrict__ rank, int stride) {
+                                                             int *__restrict__ rank,
+                                                             int *__restrict__ inv, int stride) {
     __shared__ int s_w[LMAX][RANK_THREADS / 32];
     const int nlist = *d_nlist;
     const int j = blockIdx.x * RANK_THREADS + threadIdx.x;
@@ -204,10 +220,11 @@ __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned shor
     if (j < nlist) {
         const unsigned lt = lanemask_lt();
 #pragma unroll
-        for (int l = 0; l < LMAX; ++l)
-            if ((m >> l) & 1u)
-                rank[(size_t)l * stride + j] =
-                    blk[(size_t)l * nblk + blockIdx.x] + s_w[l][w] + __popc(bal[l] & lt);
+        for (int l = 0; l < LMAX; ++l) {
+            const int r = blk[(size_t)l * nblk + blockIdx.x] + s_w[l][w] + __popc(bal[l] & lt);
+            rank[(size_t)l * stride + j] = r;
+            if ((m >> l) & 1u) inv[(size_t)l * stride + r] = j;
+        }
     }
 }
 
@@ -219,56 +236,66 @@ __global__ void k_tree_root(int n, int leafcap, TNode *tnode, int2 *range, int4 
     if (n <= leafcap) tnode[0].child = -1;
 }
 
+// One thread per inner cell: the r-th inner cell of level l is started by list entry
+// inv[l][r] (source s = lpos[j]).  Its children's ranges come from searches for the child key
+// boundaries inside [s, e), e the first key past the cell; its own id from its parent's rank.
 __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap,
                                 const int *__restrict__ lpos,
-                                const unsigned short *__restrict__ lmask, int nlist,
-                                const int *__restrict__ rank, int stride, LevelOffsets lo,
-                                int nnodes,
+                                const unsigned short *__restrict__ lmask,
+                                const int *__restrict__ rank, const int *__restrict__ inv,
+                                int stride, int ninner, LevelOffsets lo, int nnodes,
                                 TNode *__restrict__ tnode, int2 *__restrict__ range,
                                 int4 *__restrict__ cell, unsigned *err) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nlist; j += gridDim.x * blockDim.x) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ninner; t += gridDim.x * blockDim.x) {
+        // level of inner cell t: the inner cells are numbered level by level
+        int l = 0, r = t;
+        while (l < LMAX - 1 && r >= (lo.off[l + 2] - lo.off[l + 1]) / 4) {
+            r -= (lo.off[l + 2] - lo.off[l + 1]) / 4;
+            ++l;
+        }
+        const int j = inv[(size_t)l * stride + r];
         const int s = lpos[j];
-        unsigned m = lmask[j];
+        const unsigned mj = lmask[j];
+        if (!((mj >> l) & 1u)) {
+            atomicOr(err, DEVERR_TREE);
+            continue;
+        }
         const int key = keys[s];
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const int shift = 2 * (LMAX - l);
-            const int P = l == 0 ? 0 : (key >> shift);
-            const int e = l == 0 ? n : lower_bound_dev(keys, s, n, (P + 1) << shift);
-            int id = 0;
-            if (l > 0) {
-                // the parent run starts at the first key with the level-(l-1) prefix P >> 2
-                const int pshift = shift + 2;
-                const int sp = lower_bound_dev(keys, 0, s + 1, (P >> 2) << pshift);
-                const int jp = lower_bound_dev(lpos, 0, nlist, sp);
-                if (jp >= nlist || lpos[jp] != sp || !((lmask[jp] >> (l - 1)) & 1u)) {
-                    atomicOr(err, DEVERR_TREE);
-                    continue;
-                }
-                id = lo.off[l] + 4 * rank[(size_t)(l - 1) * stride + jp] + (P & 3);
-            }
-            const int base = lo.off[l + 1] + 4 * rank[(size_t)l * stride + j];
-            if (id < 0 || id >= nnodes || base < 0 || base + 4 > nnodes) {
-                atomicOr(err, DEVERR_BOUNDS);
+        const int shift = 2 * (LMAX - l);
+        const int P = l == 0 ? 0 : (key >> shift);
+        const int e = l == 0 ? n : gallop_lower_bound(keys, s, n, (P + 1) << shift);
+        int id = 0;
+        if (l > 0) {
+            // The parent is the inner cell of level l-1 that holds source s: the last list
+            // entry up to j with bit l-1 (a later one would start a new level-(l-1) cell
+            // before s).  Its rank is the count of such entries up to j, minus one.
+            const int prank = rank[(size_t)(l - 1) * stride + j] + (int)((mj >> (l - 1)) & 1u) - 1;
+            if (prank < 0) {
+                atomicOr(err, DEVERR_TREE);
                 continue;
             }
-            tnode[id].child = base;
-            const int cshift = shift - 2;
-            int b[5];
-            b[0] = s;
-            b[4] = e;
-            for (int c = 1; c < 4; ++c) b[c] = lower_bound_dev(keys, b[c - 1], e, ((P << 2) | c) << cshift);
-            const int cx = compact_bits(P), cy = compact_bits(P >> 1);
-            for (int c = 0; c < 4; ++c) {
-                const int cid = base + c;
-                const int cnt = b[c + 1] - b[c];
-                range[cid] = make_int2(b[c], b[c + 1]);
-                cell[cid] = make_int4(l + 1, 2 * cx + (c & 1), 2 * cy + (c >> 1), id);
-                tnode[cid].count = cnt;
-                const bool inner = cnt > leafcap && l + 1 < LMAX;
-                if (!inner) tnode[cid].child = -1;
-            }
+            id = lo.off[l] + 4 * prank + (P & 3);
+        }
+        const int base = lo.off[l + 1] + 4 * r;
+        if (id < 0 || id >= nnodes || base < 0 || base + 4 > nnodes) {
+            atomicOr(err, DEVERR_BOUNDS);
+            continue;
+        }
+        tnode[id].child = base;
+        const int cshift = shift - 2;
+        int b[5];
+        b[0] = s;
+        b[4] = e;
+        for (int c = 1; c < 4; ++c) b[c] = gallop_lower_bound(keys, b[c - 1], e, ((P << 2) | c) << cshift);
+        const int cx = compact_bits(P), cy = compact_bits(P >> 1);
+        for (int c = 0; c < 4; ++c) {
+            const int cid = base + c;
+            const int cnt = b[c + 1] - b[c];
+            range[cid] = make_int2(b[c], b[c + 1]);
+            cell[cid] = make_int4(l + 1, 2 * cx + (c & 1), 2 * cy + (c >> 1), id);
+            tnode[cid].count = cnt;
+            const bool inner = cnt > leafcap && l + 1 < LMAX;
+            if (!inner) tnode[cid].child = -1;
         }
     }
 }
@@ -291,13 +318,14 @@ int build_topology(Context &c, int leafcap) {
     const int cap = (int)(bound < n ? bound : n);
     const int ntl = (n + TL_TILE - 1) / TL_TILE;
     const int nblk = (cap + RANK_THREADS - 1) / RANK_THREADS;
-    int *lpos, *rank, *blkc, *totals, *tl_counter;
+    int *lpos, *rank, *rinv, *blkc, *totals, *tl_counter;
     unsigned *tl_status;
     unsigned short *lmask;
     if ((rc = ensure(c, S_LPOS, (size_t)cap + 1, &lpos)) ||
         (rc = ensure(c, S_LMASK, (size_t)cap + 1, &lmask)) ||
         (rc = ensure(c, S_TFLAG, (size_t)ntl + 8, &tl_status)) ||
         (rc = ensure(c, S_LRANK, (size_t)LMAX * (cap + 1), &rank)) ||
+        (rc = ensure(c, S_LINV, (size_t)LMAX * (cap + 1), &rinv)) ||
         (rc = ensure(c, S_LBLK, (size_t)LMAX * (nblk + 1), &blkc)) ||
         (rc = ensure(c, S_LEVEL_TOTALS, LMAX + 4, &totals)))
         return rc;
@@ -313,7 +341,7 @@ int build_topology(Context &c, int leafcap) {
     TC_KERNEL_CHECK();
     k_rank_scan<<<LMAX, 1024, 0, c.stream>>>(blkc, nblk, totals);
     TC_KERNEL_CHECK();
-    k_rank_apply<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk, rank, cap);
+    k_rank_apply<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk, rank, rinv, cap);
     TC_KERNEL_CHECK();
     // the level totals and the list length, in one read-back
     TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, totals, sizeof(int) * (LMAX + 1),
@@ -357,10 +385,10 @@ int build_topology(Context &c, int leafcap) {
         return rc;
     k_tree_root<<<1, 1, 0, c.stream>>>(n, leafcap, tnode, range, cell);
     TC_KERNEL_CHECK();
-    if (nlist > 0) {
-        k_tree_children<<<grid_for_tree(nlist, 128), 128, 0, c.stream>>>(
-            keys, n, leafcap, lpos, lmask, nlist, rank, cap, lo, c.nnodes, tnode, range, cell,
-            slot_ptr<unsigned>(c, S_ERR));
+    if (ninner > 0) {
+        k_tree_children<<<grid_for_tree((int)ninner, 128), 128, 0, c.stream>>>(
+            keys, n, leafcap, lpos, lmask, rank, rinv, cap, (int)ninner, lo, c.nnodes, tnode, range,
+            cell, slot_ptr<unsigned>(c, S_ERR));
         TC_KERNEL_CHECK();
     }
     return TC_OK;
