@@ -101,10 +101,10 @@ size_t footprint_estimate(int kind, long long n, long long ntargets, long long n
     const bool force = kind == TC_REQUEST_FORCE_MRAG;
     const long long leaf = force ? tc::LEAF_FORCE : tc::LEAF_POTENTIAL;
     const long long p = force ? tc::ORDER_FORCE : tc::ORDER_POTENTIAL;
-    // per source: staged x/y/v, sorted x/y/v, sort ping-pong copies, keys and permutations,
-    // tree-build masks, flags and offsets, per-level ranks of the split list
+    // per source: staged x/y/v, sorted x/y/v, keys and permutation, the sort's two item arrays
+    // and packed records, tree-build flags; per-level ranks of the split list
     const long long nodes = 4 * (n / leaf + 1) + 64;
-    size_t b = (size_t)n * 112 + (size_t)std::min(n, nodes) * 4 * tc::LMAX;
+    size_t b = (size_t)n * 128 + (size_t)std::min(n, nodes) * 8 * tc::LMAX;
     // per node: traversal record, range, cell, moments, expansion (+ scaled FP32 copy)
     b += (size_t)nodes * (88 + 16 * p + (precision ? 8 * p + 4 : 0));
     if (force) {

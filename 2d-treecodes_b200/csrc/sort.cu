@@ -1,17 +1,21 @@
 // sort.cu -- bounding square, Morton keys, LSD radix sort with a stable permutation, and the
-// source gather.  Restates drivers/sort-sources.cpp:23-132 of the reference.
+// sorted source arrays.  Restates drivers/sort-sources.cpp:23-132 of the reference.
 //
 // Data flow per solve (N sources, all FP64 SoA in HBM):
-//   k_bbox          x, y           -> Frame (xmin, ymin, ext, scale)       2 x 8 B/src read
-//   k_keys          x, y, Frame    -> keys (30-bit Morton)                 16 B read, 4 B write
-//   radix sort      keys (+ index) -> sorted keys, permutation             4 onesweep passes
-//   k_gather        x, y, v, perm  -> sorted x, y, v                       24 B gathered, 24 B written
+//   k_bbox            x, y        -> Frame (xmin, ymin, ext, scale)          16 B/src read
+//   k_keys_pack       x, y, v     -> items (key << 32 | index), records      24 B read, 40 B written
+//                                    (x, y, v, 0), digit histograms
+//   k_onesweep_items  items       -> items sorted by one 8-bit key digit     8 B read, 8 B written
+//                                    (4 passes)
+//   k_gather_sources  items, recs -> sorted keys, permutation, x, y, v       8 B + one 32-byte
+//                                                                            record read, 32 B written
 //
-// The radix sort is a one-pass-per-digit ("onesweep") LSD sort: every CTA ranks a tile of
-// 4096 keys in shared memory with warp-level match_any, publishes its per-digit counts, and
-// finds its global offsets by a decoupled look-back over the tiles before it.  Tiles take
-// their ids from an atomic counter, so each waits only on tiles that already run; the waits
-// are bounded and raise DEVERR_SPIN_LIMIT instead of hanging.
+// The radix sort is a one-pass-per-digit ("onesweep") LSD sort: every CTA counts the digits of
+// a tile of items, finds its global digit offsets by a decoupled look-back over the tiles
+// before it, ranks the tile in shared memory with warp digit ballots and writes it out in
+// runs of equal digits.  Tiles take their ids from an atomic counter, so each waits only on
+// tiles that already run; the waits are bounded and raise DEVERR_SPIN_LIMIT instead of
+// hanging.  Ties keep input order, so the order is the reference's (key, index) order.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -199,45 +203,6 @@ __global__ __launch_bounds__(256) void k_hist(const int *__restrict__ keys, int 
     }
 }
 
-// Morton keys of the sources and the histograms of every 8-bit digit of them, in one pass
-// (k_keys followed by k_hist, without reading the keys back).
-__global__ __launch_bounds__(256) void k_keys_hist(const double *__restrict__ x,
-                                                   const double *__restrict__ y, int n,
-                                                   const Frame *__restrict__ frame,
-                                                   int *__restrict__ keys, int npasses,
-                                                   int *__restrict__ hist) {
-    __shared__ int s[RS_MAX_PASSES][RS_RADIX];
-    for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
-    __syncthreads();
-    const Frame f = *frame;
-    auto key_of = [&](double xv, double yv) {
-        const int k = spread_bits(quantize(xv, f.xmin, f.scale)) |
-                      (spread_bits(quantize(yv, f.ymin, f.scale)) << 1);
-        for (int p = 0; p < npasses; ++p) atomicAdd(&s[p][((unsigned)k >> (8 * p)) & 0xFF], 1);
-        return k;
-    };
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-    if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0 &&
-        (reinterpret_cast<uintptr_t>(keys) & 7) == 0) {
-        // 16-byte loads and 8-byte stores: two sources per thread and step
-        const double2 *x2 = reinterpret_cast<const double2 *>(x);
-        const double2 *y2 = reinterpret_cast<const double2 *>(y);
-        int2 *k2 = reinterpret_cast<int2 *>(keys);
-        for (int i = gid; i < n / 2; i += stride) {
-            const double2 a = x2[i], b = y2[i];
-            k2[i] = make_int2(key_of(a.x, b.x), key_of(a.y, b.y));
-        }
-        if ((n & 1) && gid == 0) keys[n - 1] = key_of(x[n - 1], y[n - 1]);
-    } else {
-        for (int i = gid; i < n; i += stride) keys[i] = key_of(x[i], y[i]);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < npasses * RS_RADIX; i += blockDim.x) {
-        const int c = (&s[0][0])[i];
-        if (c) atomicAdd(&hist[i], c);
-    }
-}
-
 __global__ __launch_bounds__(RS_RADIX) void k_hist_scan(const int *__restrict__ hist,
                                                         int *__restrict__ offsets) {
     const int p = blockIdx.x;
@@ -249,26 +214,55 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned *p) {
     return *(const volatile unsigned *)p;
 }
 
+// The lanes of `vmask` whose 8-bit digit equals this lane's: one ballot per digit bit
+// (eight cheap votes instead of one match.any, which has a much lower issue rate).
+__device__ __forceinline__ unsigned digit_peers(unsigned vmask, int d) {
+    unsigned peers = vmask;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (d >> b) & 1;
+        const unsigned bal = __ballot_sync(FULL_MASK, bit);
+        peers &= bit ? bal : ~bal;
+    }
+    return peers;
+}
+
 // Exclusive prefix of digit d over the tiles before `tile` (decoupled look-back): walk back
-// over the predecessors' statuses, adding aggregates, until the first inclusive prefix.  A
-// predecessor that has published nothing yet is read again; the number of such reads is
-// bounded (DEVERR_SPIN_LIMIT).  (Reading several predecessors per step measured slower.)
+// over the predecessors' statuses, adding aggregates, until the first inclusive prefix.  The
+// statuses of LB_WINDOW predecessors are read at once (independent loads, each coalesced over
+// the CTA's digit threads), which cuts the walk of ~17 dependent L2 round trips measured on
+// 16M keys to ~6.  A predecessor that has published nothing yet is read again from there; the
+// number of reads without progress is bounded (DEVERR_SPIN_LIMIT).
+constexpr int LB_WINDOW = 4;
+
 __device__ __forceinline__ int lookback(const unsigned *status, int tile, int d, unsigned *err) {
     int excl = 0;
     int spins = 0;
-    for (int j = tile - 1; j >= 0;) {
-        const unsigned s = ld_volatile(status + (size_t)j * RS_RADIX + d);
-        const unsigned flag = s & ~RS_VALMASK;
-        if (flag == 0) {
-            if (++spins > RS_SPIN_LIMIT) {
-                atomicOr(err, DEVERR_SPIN_LIMIT);
-                break;
+    int j = tile - 1;
+    while (j >= 0) {
+        unsigned s[LB_WINDOW];
+#pragma unroll
+        for (int q = 0; q < LB_WINDOW; ++q)
+            s[q] = j - q >= 0 ? ld_volatile(status + (size_t)(j - q) * RS_RADIX + d) : RS_FLAG_INC;
+        int used = 0;
+        bool stop = false;
+#pragma unroll
+        for (int q = 0; q < LB_WINDOW; ++q) {
+            if (stop) continue;
+            const unsigned flag = s[q] & ~RS_VALMASK;
+            if (flag == 0) {
+                stop = true;   // not published yet: read again from here
+                continue;
             }
-            continue;
+            excl += (int)(s[q] & RS_VALMASK);
+            ++used;
+            if (flag == RS_FLAG_INC) return excl;
         }
-        excl += (int)(s & RS_VALMASK);
-        if (flag == RS_FLAG_INC) break;
-        --j;
+        j -= used;
+        if (used == 0 && ++spins > RS_SPIN_LIMIT) {
+            atomicOr(err, DEVERR_SPIN_LIMIT);
+            break;
+        }
     }
     return excl;
 }
@@ -310,8 +304,8 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
         const bool valid = idx < n;
         const unsigned vmask = __ballot_sync(FULL_MASK, valid);
         const int d = (key[k] >> shift) & 0xFF;
-        unsigned peers = 0;
-        if (valid) peers = __match_any_sync(vmask, d);
+        unsigned peers = digit_peers(vmask, d);
+        if (!valid) peers = 0;
         const int old = valid ? hist[d] : 0;
         __syncwarp();
         if (valid && (peers & lt) == 0) hist[d] = old + __popc(peers);
@@ -375,100 +369,113 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
     }
 }
 
-// L2 prefetch of [p, p + bytes) rounded inwards to 16-byte bounds (a hint: no data moves to
-// the SM, nothing is written).
-__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
-    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
-    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
-    if (e > a)
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a))
-                     : "memory");
+// ---------------------------------------------------------------------------- source sort
+// The sources are sorted as 8-byte items (key << 32 | index) and gathered once at the end:
+//   * k_keys_pack reads x, y, v once and writes the Morton keys' digit histograms, the items
+//     in input order and a 32-byte record (x, y, v, 0) per source;
+//   * four onesweep passes over the items (8-bit digits of the key half; 16 B of traffic per
+//     item and pass);
+//   * k_gather_sources reads each sorted item's record (one 32-byte DRAM sector) and writes
+//     the sorted keys, permutation, x, y and v.
+// Ties keep input order, so the result is the (key, index) lexicographic order.
+__global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
+                                                   const double *__restrict__ y,
+                                                   const double *__restrict__ v, int n,
+                                                   const Frame *__restrict__ frame,
+                                                   unsigned long long *__restrict__ items,
+                                                   double2 *__restrict__ rec, int npasses,
+                                                   int *__restrict__ hist) {
+    __shared__ int s[RS_MAX_PASSES][RS_RADIX];
+    for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
+    __syncthreads();
+    const Frame f = *frame;
+    auto item_of = [&](double xv, double yv, int i) {
+        const int k = spread_bits(quantize(xv, f.xmin, f.scale)) |
+                      (spread_bits(quantize(yv, f.ymin, f.scale)) << 1);
+        for (int p = 0; p < npasses; ++p) atomicAdd(&s[p][((unsigned)k >> (8 * p)) & 0xFF], 1);
+        return ((unsigned long long)(unsigned)k << 32) | (unsigned)i;
+    };
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) |
+          reinterpret_cast<uintptr_t>(v)) & 15) == 0) {
+        // 16-byte loads and stores: two sources per thread and step
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        const double2 *y2 = reinterpret_cast<const double2 *>(y);
+        const double2 *v2 = reinterpret_cast<const double2 *>(v);
+        ulonglong2 *it2 = reinterpret_cast<ulonglong2 *>(items);
+        for (int i = gid; i < n / 2; i += stride) {
+            const double2 a = x2[i], b = y2[i], w = v2[i];
+            it2[i] = make_ulonglong2(item_of(a.x, b.x, 2 * i), item_of(a.y, b.y, 2 * i + 1));
+            rec[4 * i + 0] = make_double2(a.x, b.x);
+            rec[4 * i + 1] = make_double2(w.x, 0.0);
+            rec[4 * i + 2] = make_double2(a.y, b.y);
+            rec[4 * i + 3] = make_double2(w.y, 0.0);
+        }
+        if ((n & 1) && gid == 0) {
+            const int i = n - 1;
+            items[i] = item_of(x[i], y[i], i);
+            rec[2 * i] = make_double2(x[i], y[i]);
+            rec[2 * i + 1] = make_double2(v[i], 0.0);
+        }
+    } else {
+        for (int i = gid; i < n; i += stride) {
+            items[i] = item_of(x[i], y[i], i);
+            rec[2 * i] = make_double2(x[i], y[i]);
+            rec[2 * i + 1] = make_double2(v[i], 0.0);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npasses * RS_RADIX; i += blockDim.x) {
+        const int c = (&s[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
 }
 
-// The same pass for the sources, carrying the input index, coordinates and values along with
-// the key, so that the sorted x/y/v come out of the last pass without a random gather over the
-// whole array (~300 B of DRAM traffic per source on HBM, against 28 + 28 B here).
-//   * tiles of 2048 sources, 256 threads, 8 items per thread; three CTAs fit one SM;
-//   * at the start of a tile one thread asks for the tile's index/x/y/v ranges to be brought
-//     into L2 (cp.async.bulk.prefetch), so their DRAM latency overlaps ranking and look-back;
-//   * once the local positions are known every item's index, x, y and v are loaded together
-//     (32 loads in flight per thread, served by L2) and placed in sorted order in shared memory;
-//   * one output loop writes all five arrays, slot j going to s_global[digit] + j.
-constexpr int XYV_THREADS = 256;
-constexpr int XYV_WARPS = XYV_THREADS / 32;
-constexpr int XYV_ITEMS = 8;
-constexpr int XYV_TILE = XYV_THREADS * XYV_ITEMS;
-constexpr size_t XYV_SMEM = (size_t)XYV_TILE * (2 * sizeof(int) + 3 * sizeof(double)) +
-                            (size_t)XYV_WARPS * RS_RADIX * sizeof(int) + 2 * RS_RADIX * sizeof(int) +
-                            16;
+// One onesweep pass over 8-byte items, digit (item >> shift) & 0xFF: tiles of 3072 items
+// (256 threads x 12, four CTAs per SM); the tile's digit counts, then the global digit offsets
+// by decoupled look-back, then the stable rank within each warp from digit ballots; items are
+// placed in sorted order in shared memory and written out in runs of equal digits.
+constexpr int PS_THREADS = 256;
+constexpr int PS_WARPS = PS_THREADS / 32;
+constexpr int PS_ITEMS = 12;
+constexpr int PS_TILE = PS_THREADS * PS_ITEMS;
 
-__global__ __launch_bounds__(XYV_THREADS) void k_onesweep_xyv(
-    const int *__restrict__ keys_in, const int *__restrict__ idx_in,
-    const double *__restrict__ x_in, const double *__restrict__ y_in,
-    const double *__restrict__ v_in, int *__restrict__ keys_out, int *__restrict__ idx_out,
-    double *__restrict__ x_out, double *__restrict__ y_out, double *__restrict__ v_out, int n,
+__global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
+    const unsigned long long *__restrict__ in, unsigned long long *__restrict__ out, int n,
     int shift, const int *__restrict__ digit_offsets, unsigned *status, int *tile_counter,
     unsigned *err) {
-    extern __shared__ __align__(16) unsigned char xyv_smem[];
-    double *s_x = reinterpret_cast<double *>(xyv_smem);
-    double *s_y = s_x + XYV_TILE;
-    double *s_v = s_y + XYV_TILE;
-    int *s_keys = reinterpret_cast<int *>(s_v + XYV_TILE);
-    int *s_idx = s_keys + XYV_TILE;
-    int(*s_whist)[RS_RADIX] = reinterpret_cast<int(*)[RS_RADIX]>(s_idx + XYV_TILE);
-    int *s_tile_start = &s_whist[XYV_WARPS][0];
-    int *s_global = s_tile_start + RS_RADIX;
-    int *s_tile = s_global + RS_RADIX;
+    __shared__ unsigned long long s_items[PS_TILE];
+    __shared__ int s_whist[PS_WARPS][RS_RADIX];
+    __shared__ int s_count[RS_RADIX];
+    __shared__ int s_tile_start[RS_RADIX];
+    __shared__ int s_global[RS_RADIX];
+    __shared__ int s_tile;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) *s_tile = atomicAdd(tile_counter, 1);
-    for (int i = tid; i < XYV_WARPS * RS_RADIX; i += XYV_THREADS) (&s_whist[0][0])[i] = 0;
+    if (tid == 0) s_tile = atomicAdd(tile_counter, 1);
+    for (int i = tid; i < PS_WARPS * RS_RADIX; i += PS_THREADS) (&s_whist[0][0])[i] = 0;
+    s_count[tid] = 0;
     __syncthreads();
-    const int tile = *s_tile;
-    const int tile_base = tile * XYV_TILE;
-    const int tile_n = min(XYV_TILE, n - tile_base);
-    const int warp_base = tile_base + warp * (XYV_ITEMS * 32);
-    if (tid == 0) {
-        prefetch_l2(x_in + tile_base, sizeof(double) * tile_n);
-        prefetch_l2(y_in + tile_base, sizeof(double) * tile_n);
-        prefetch_l2(v_in + tile_base, sizeof(double) * tile_n);
-        if (idx_in) prefetch_l2(idx_in + tile_base, sizeof(int) * tile_n);
-    }
+    const int tile = s_tile;
+    const int tile_base = tile * PS_TILE;
+    const int tile_n = min(PS_TILE, n - tile_base);
+    const int warp_base = tile_base + warp * (PS_ITEMS * 32);
 
-    int key[XYV_ITEMS], pos[XYV_ITEMS];
+    unsigned long long item[PS_ITEMS];
+    int rank[PS_ITEMS];
 #pragma unroll
-    for (int k = 0; k < XYV_ITEMS; ++k) {
+    for (int k = 0; k < PS_ITEMS; ++k) {
         const int idx = warp_base + k * 32 + lane;
-        key[k] = idx < n ? keys_in[idx] : 0;
+        item[k] = idx < n ? in[idx] : 0ull;
     }
-
-    // stable rank within the warp, items visited in their original order (k, lane)
-    const unsigned lt = lanemask_lt();
-    int *hist = s_whist[warp];
-#pragma unroll
-    for (int k = 0; k < XYV_ITEMS; ++k) {
-        const int idx = warp_base + k * 32 + lane;
-        const bool valid = idx < n;
-        const unsigned vmask = __ballot_sync(FULL_MASK, valid);
-        const int d = (key[k] >> shift) & 0xFF;
-        unsigned peers = 0;
-        if (valid) peers = __match_any_sync(vmask, d);
-        const int old = valid ? hist[d] : 0;
-        __syncwarp();
-        if (valid && (peers & lt) == 0) hist[d] = old + __popc(peers);
-        __syncwarp();
-        pos[k] = old + __popc(peers & lt);
-    }
-    __syncthreads();
-
+    // Early counts: the tile's digit totals first (shared atomics), so that its aggregate is
+    // published and the look-back done before the ranking, not after it.
     const int d = tid;   // one digit per thread
-    int total = 0;
 #pragma unroll
-    for (int w = 0; w < XYV_WARPS; ++w) {
-        const int c = s_whist[w][d];
-        s_whist[w][d] = total;
-        total += c;
-    }
+    for (int k = 0; k < PS_ITEMS; ++k)
+        if (warp_base + k * 32 + lane < n) atomicAdd(&s_count[(int)(item[k] >> shift) & 0xFF], 1);
+    __syncthreads();
+    const int total = s_count[d];
     unsigned *mine = status + (size_t)tile * RS_RADIX + d;
     int excl = 0;
     if (tile == 0) {
@@ -478,45 +485,105 @@ __global__ __launch_bounds__(XYV_THREADS) void k_onesweep_xyv(
         excl = lookback(status, tile, d, err);
         atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
     }
+
+    const unsigned lt = lanemask_lt();
+    int *hist = s_whist[warp];
+#pragma unroll
+    for (int k = 0; k < PS_ITEMS; ++k) {
+        const int idx = warp_base + k * 32 + lane;
+        const bool valid = idx < n;
+        const unsigned vmask = __ballot_sync(FULL_MASK, valid);
+        const int dk = (int)(item[k] >> shift) & 0xFF;
+        unsigned peers = digit_peers(vmask, dk);
+        if (!valid) peers = 0;
+        const int old = valid ? hist[dk] : 0;
+        __syncwarp();
+        if (valid && (peers & lt) == 0) hist[dk] = old + __popc(peers);
+        __syncwarp();
+        rank[k] = old + __popc(peers & lt);
+    }
+    __syncthreads();
+    int run = 0;
+#pragma unroll
+    for (int w = 0; w < PS_WARPS; ++w) {
+        const int c = s_whist[w][d];
+        s_whist[w][d] = run;
+        run += c;
+    }
     const int start = block_exclusive_scan(total, nullptr);
     s_tile_start[d] = start;
     s_global[d] = digit_offsets[d] + excl - start;
     __syncthreads();
 
-    // every item to its sorted slot in shared memory, with its index, x, y and v
 #pragma unroll
-    for (int k = 0; k < XYV_ITEMS; ++k) {
+    for (int k = 0; k < PS_ITEMS; ++k) {
         const int idx = warp_base + k * 32 + lane;
         if (idx < n) {
-            const int dk = (key[k] >> shift) & 0xFF;
-            const int p = s_tile_start[dk] + s_whist[warp][dk] + pos[k];
+            const int dk = (int)(item[k] >> shift) & 0xFF;
+            const int p = s_tile_start[dk] + s_whist[warp][dk] + rank[k];
             if ((unsigned)p >= (unsigned)tile_n) {
                 atomicOr(err, DEVERR_BOUNDS);
-            } else {
-                s_keys[p] = key[k];
-                s_idx[p] = idx_in ? __ldg(idx_in + idx) : idx;
-                s_x[p] = __ldg(x_in + idx);
-                s_y[p] = __ldg(y_in + idx);
-                s_v[p] = __ldg(v_in + idx);
+                continue;
             }
+            s_items[p] = item[k];
         }
     }
     __syncthreads();
 
-    // slot j goes to s_global[digit] + j: runs of equal digits are consecutive in memory
 #pragma unroll 4
-    for (int j = tid; j < tile_n; j += XYV_THREADS) {
-        const int kj = s_keys[j];
-        const int g = s_global[(kj >> shift) & 0xFF] + j;
+    for (int j = tid; j < tile_n; j += PS_THREADS) {
+        const unsigned long long it = s_items[j];
+        const int g = s_global[(int)(it >> shift) & 0xFF] + j;
         if ((unsigned)g >= (unsigned)n) {
             atomicOr(err, DEVERR_BOUNDS);
             continue;
         }
-        keys_out[g] = kj;
-        idx_out[g] = s_idx[j];
-        x_out[g] = s_x[j];
-        y_out[g] = s_y[j];
-        v_out[g] = s_v[j];
+        out[g] = it;
+    }
+}
+
+// Sorted keys, permutation, x, y and v from the sorted items and the input-order records.
+constexpr int GS_THREADS = 256;
+constexpr int GS_ITEMS = 8;
+
+__global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
+    const unsigned long long *__restrict__ items, const double2 *__restrict__ rec, int n,
+    int *__restrict__ keys, int *__restrict__ perm, double *__restrict__ xs,
+    double *__restrict__ ys, double *__restrict__ vs, unsigned *err) {
+    const int stride = gridDim.x * GS_THREADS * GS_ITEMS;
+    for (int base = blockIdx.x * GS_THREADS * GS_ITEMS + threadIdx.x; base < n; base += stride) {
+        unsigned long long it[GS_ITEMS];
+        double2 a[GS_ITEMS];
+        double w[GS_ITEMS];
+#pragma unroll
+        for (int k = 0; k < GS_ITEMS; ++k) {
+            const int i = base + k * GS_THREADS;
+            it[k] = i < n ? items[i] : 0ull;
+        }
+#pragma unroll
+        for (int k = 0; k < GS_ITEMS; ++k) {
+            const int i = base + k * GS_THREADS;
+            const unsigned id = (unsigned)it[k];
+            if (i < n && id < (unsigned)n) {
+                a[k] = __ldg(rec + 2 * (size_t)id);
+                w[k] = __ldg(reinterpret_cast<const double *>(rec + 2 * (size_t)id + 1));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < GS_ITEMS; ++k) {
+            const int i = base + k * GS_THREADS;
+            if (i >= n) continue;
+            const unsigned id = (unsigned)it[k];
+            if (id >= (unsigned)n) {
+                atomicOr(err, DEVERR_BOUNDS);
+                continue;
+            }
+            keys[i] = (int)(it[k] >> 32);
+            perm[i] = (int)id;
+            xs[i] = a[k].x;
+            ys[i] = a[k].y;
+            vs[i] = w[k];
+        }
     }
 }
 
@@ -653,13 +720,12 @@ int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
 int sort_sources(Context &c, const double *x, const double *y, const double *v, int n) {
     int rc;
     double *xs, *ys, *vs;
-    int *keys, *perm, *keys2, *perm2;
+    int *keys, *perm;
     Frame *frame;
     double4 *partials;
     if ((rc = ensure(c, S_XS, n, &xs)) || (rc = ensure(c, S_YS, n, &ys)) ||
         (rc = ensure(c, S_VS, n, &vs)) || (rc = ensure(c, S_KEYS, n, &keys)) ||
-        (rc = ensure(c, S_PERM, n, &perm)) || (rc = ensure(c, S_KEYS2, n, &keys2)) ||
-        (rc = ensure(c, S_PERM2, n, &perm2)))
+        (rc = ensure(c, S_PERM, n, &perm)))
         return rc;
     // frame + bbox partials + completion counter share one small buffer
     const int gb = grid_for(n, BBOX_THREADS, 8);
@@ -671,19 +737,19 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     k_bbox<<<gb, BBOX_THREADS, 0, c.stream>>>(x, y, n, partials, done, frame);
     TC_KERNEL_CHECK();
 
-    // four 8-bit passes carrying (index, x, y, v); the ping-pong
-    // input -> tmp -> sorted -> tmp -> sorted ends in keys/perm/xs/ys/vs
+    // four 8-bit passes over the (key, index) items, then one gather of the records
     if (n >= (1 << 30)) {
         set_error(TC_ERR_INVALID, "too many sources for the radix sort (%d)", n);
         return TC_ERR_INVALID;
     }
-    double *x2, *y2, *v2;
+    unsigned long long *items_a, *items_b;
+    double2 *rec;
     int *hist, *counter;
     unsigned *status;
     const int npasses = (2 * LMAX + 7) / 8;
-    const int ntiles = (n + XYV_TILE - 1) / XYV_TILE;
-    if ((rc = ensure(c, S_X2, n, &x2)) || (rc = ensure(c, S_Y2, n, &y2)) ||
-        (rc = ensure(c, S_V2, n, &v2)) ||
+    const int ntiles = (n + PS_TILE - 1) / PS_TILE;
+    if ((rc = ensure(c, S_ITEMS_A, n, &items_a)) || (rc = ensure(c, S_ITEMS_B, n, &items_b)) ||
+        (rc = ensure(c, S_REC, 2 * (size_t)n, &rec)) ||
         (rc = ensure(c, S_RS_HIST, 2 * RS_MAX_PASSES * RS_RADIX, &hist)) ||
         (rc = ensure(c, S_RS_COUNTER, RS_MAX_PASSES, &counter)) ||
         (rc = ensure(c, S_RS_STATUS, (size_t)RS_MAX_PASSES * ntiles * RS_RADIX, &status)))
@@ -693,29 +759,23 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
                                 c.stream));
-    k_keys_hist<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, keys, npasses, hist);
+    k_keys_pack<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, v, n, frame, items_a, rec,
+                                                            npasses, hist);
     TC_KERNEL_CHECK();
     k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
     TC_KERNEL_CHECK();
-    static const cudaError_t attr_rc = cudaFuncSetAttribute(
-        k_onesweep_xyv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XYV_SMEM);
-    TC_CUDA_TRY(attr_rc);
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
-    static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in the sorted arrays");
+    static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in items_a");
     for (int p = 0; p < npasses; ++p) {
         const bool odd = p & 1;
-        const int *ki = odd ? keys2 : keys;
-        const int *ii = p == 0 ? nullptr : (odd ? perm2 : perm);
-        const double *xi = p == 0 ? x : (odd ? x2 : xs);
-        const double *yi = p == 0 ? y : (odd ? y2 : ys);
-        const double *vi = p == 0 ? v : (odd ? v2 : vs);
-        int *ko = odd ? keys : keys2, *io = odd ? perm : perm2;
-        double *xo = odd ? xs : x2, *yo = odd ? ys : y2, *vo = odd ? vs : v2;
-        k_onesweep_xyv<<<ntiles, XYV_THREADS, XYV_SMEM, c.stream>>>(
-            ki, ii, xi, yi, vi, ko, io, xo, yo, vo, n, 8 * p, offsets + p * RS_RADIX,
-            status + (size_t)p * ntiles * RS_RADIX, counter + p, err);
+        k_onesweep_items<<<ntiles, PS_THREADS, 0, c.stream>>>(
+            odd ? items_b : items_a, odd ? items_a : items_b, n, 32 + 8 * p,
+            offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err);
         TC_KERNEL_CHECK();
     }
+    k_gather_sources<<<grid_for(n, GS_THREADS * GS_ITEMS, 8), GS_THREADS, 0, c.stream>>>(
+        items_a, rec, n, keys, perm, xs, ys, vs, err);
+    TC_KERNEL_CHECK();
     c.nsrc = n;
     return TC_OK;
 }

@@ -23,7 +23,7 @@ enum Slot {
     // inputs staged from host memory
     S_XIN, S_YIN, S_VIN, S_XT, S_YT, S_X0, S_Y0, S_H, S_OUTX, S_OUTY,
     // sorted sources
-    S_XS, S_YS, S_VS, S_KEYS, S_PERM, S_KEYS2, S_PERM2, S_FRAME, S_X2, S_Y2, S_V2,
+    S_XS, S_YS, S_VS, S_KEYS, S_PERM, S_FRAME, S_ITEMS_A, S_ITEMS_B, S_REC,
     // radix sort scratch
     S_RS_STATUS, S_RS_HIST, S_RS_COUNTER,
     // scan scratch
