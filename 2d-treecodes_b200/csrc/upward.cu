@@ -145,7 +145,7 @@ struct LeafShared {
 // the com, so |z / R| <= 1 and no power under- or overflows).  Each lane sums at most
 // leafcap/32 terms in FP32; the 32 lane sums are added in FP64 and rescaled by R^(n+1) exactly.
 template <int P, bool MIXED>
-__global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 5 : 3) void k_leaf_p2e(
+__global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 4 : 3) void k_leaf_p2e(
     int nnodes, int nsrc, int leafcap, const double *__restrict__ xs, const double *__restrict__ ys,
     const double *__restrict__ vs, const int2 *__restrict__ range, const int4 *__restrict__ cell,
     const TNode *__restrict__ tnode, double *exps, const Frame *__restrict__ frame) {
@@ -186,6 +186,13 @@ __global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 5 : 3) void k_leaf_p2e(
         acc_t ar[P], ai[P];
 #pragma unroll
         for (int n = 0; n < P; ++n) ar[n] = ai[n] = acc_t(0);
+        // mixed form: the powers in consecutive pairs (v z^(n+1), v z^(n+2)) held in f32x2
+        // lanes and advanced by z^2, so one paired instruction does the work of two
+        float2 ar2[P / 2], ai2[P / 2];
+        if constexpr (MIXED) {
+#pragma unroll
+            for (int n = 0; n < P / 2; ++n) ar2[n] = ai2[n] = make_float2(0.f, 0.f);
+        }
         for (int base = rg.x; base < rg.y; base += 32 * U) {
             const int nu = min(U, (rg.y - base + 31) >> 5);   // warp-uniform
             acc_t zr[U], zi[U], v[U];
@@ -200,15 +207,45 @@ __global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 5 : 3) void k_leaf_p2e(
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (u >= nu) break;
-                acc_t pr = v[u] * zr[u], pim = v[u] * zi[u];
+                if constexpr (MIXED) {
+                    const float p1r = v[u] * zr[u], p1i = v[u] * zi[u];
+                    const float p2r = fmaf(p1r, zr[u], -p1i * zi[u]);
+                    const float p2i = fmaf(p1r, zi[u], p1i * zr[u]);
+                    const float z2r = fmaf(zr[u], zr[u], -zi[u] * zi[u]);
+                    const float z2i = 2.f * zr[u] * zi[u];
+                    const float2 z2r2 = make_float2(z2r, z2r), z2i2 = make_float2(z2i, z2i);
+                    const float2 nz2i2 = make_float2(-z2i, -z2i);
+                    float2 re2 = make_float2(p1r, p2r), im2 = make_float2(p1i, p2i);
 #pragma unroll
-                for (int n = 0; n < P; ++n) {
-                    ar[n] += pr;
-                    ai[n] += pim;
-                    const acc_t tr = fma(pr, zr[u], -pim * zi[u]);
-                    pim = fma(pr, zi[u], pim * zr[u]);
-                    pr = tr;
+                    for (int n = 0; n < P / 2; ++n) {
+                        ar2[n] = __fadd2_rn(ar2[n], re2);
+                        ai2[n] = __fadd2_rn(ai2[n], im2);
+                        if (n + 1 < P / 2) {
+                            const float2 nre = __ffma2_rn(re2, z2r2, __fmul2_rn(im2, nz2i2));
+                            im2 = __ffma2_rn(re2, z2i2, __fmul2_rn(im2, z2r2));
+                            re2 = nre;
+                        }
+                    }
+                } else {
+                    acc_t pr = v[u] * zr[u], pim = v[u] * zi[u];
+#pragma unroll
+                    for (int n = 0; n < P; ++n) {
+                        ar[n] += pr;
+                        ai[n] += pim;
+                        const acc_t tr = fma(pr, zr[u], -pim * zi[u]);
+                        pim = fma(pr, zi[u], pim * zr[u]);
+                        pr = tr;
+                    }
                 }
+            }
+        }
+        if constexpr (MIXED) {
+#pragma unroll
+            for (int n = 0; n < P / 2; ++n) {
+                ar[2 * n] = ar2[n].x;
+                ar[2 * n + 1] = ar2[n].y;
+                ai[2 * n] = ai2[n].x;
+                ai[2 * n + 1] = ai2[n].y;
             }
         }
         __syncwarp();
