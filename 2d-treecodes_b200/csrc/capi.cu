@@ -10,6 +10,8 @@
 #include <mutex>
 
 #include "treecodes_b200.h"
+#include <initializer_list>
+
 #include "tc_internal.h"
 
 namespace tc {
@@ -115,6 +117,7 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_totals, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_inputs, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaMallocHost(&c.h_pinned, 4096));
     for (auto &ev : c.ev) TC_CUDA_TRY(cudaEventCreate(&ev));
     unsigned *err;
@@ -142,7 +145,7 @@ static void context_free(Context &c) {
     release_pool_cache(c.device);
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
-    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join})
+    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs})
         if (ev) cudaEventDestroy(ev);
     if (c.aux) cudaStreamDestroy(c.aux);
     if (c.h_pinned) cudaFreeHost(c.h_pinned);
@@ -172,15 +175,16 @@ static void finish_timing(Context &c) {
 // traversals read.  The expansions follow separately (upward_expansions), so that they can be
 // formed while the interaction lists are built.
 static int build_tree_moments(Context &c, int kind, const double *x, const double *y,
-                              const double *v, int n) {
+                              const double *v, int n, cudaEvent_t values_ready = nullptr) {
     int rc;
     g_launches = 0;
     TC_CUDA_TRY(cudaMemsetAsync(slot_ptr<unsigned>(c, S_ERR), 0, sizeof(unsigned), c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(c.buf[S_STATS].p, 0, STAT_SLOTS * sizeof(unsigned long long),
                                 c.stream));
-    if ((rc = sort_sources(c, x, y, v, n))) return rc;
+    if ((rc = sort_sources(c, x, y, v, n, values_ready))) return rc;
     phase_mark(c, 1);
     if ((rc = build_topology(c, kind ? LEAF_FORCE : LEAF_POTENTIAL))) return rc;
+    if ((rc = finish_sources(c))) return rc;
     phase_mark(c, 2);
     if ((rc = upward_prepare(c, kind ? ORDER_FORCE : ORDER_POTENTIAL)) || (rc = upward_moments(c)))
         return rc;
@@ -205,7 +209,7 @@ static int expansions_then_mark(Context &c) {
 
 static int potential_device(Context &c, double theta, const double *xs, const double *ys,
                             const double *vs, int n, const double *xt, const double *yt, int m,
-                            double *out) {
+                            double *out, cudaEvent_t values_ready = nullptr) {
     if (n < 0 || m < 0) {
         set_error(TC_ERR_INVALID, "negative size (nsources %d, ntargets %d)", n, m);
         return TC_ERR_INVALID;
@@ -218,7 +222,7 @@ static int potential_device(Context &c, double theta, const double *xs, const do
     }
     int rc;
     phase_mark(c, 0);
-    if ((rc = build_tree_moments(c, 0, xs, ys, vs, n))) return rc;
+    if ((rc = build_tree_moments(c, 0, xs, ys, vs, n, values_ready))) return rc;
     if ((rc = potential(c, theta, xt, yt, m, out, expansions_then_mark))) return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_potential"))) return rc;
@@ -230,7 +234,8 @@ static int potential_device(Context &c, double theta, const double *xs, const do
 
 static int force_device(Context &c, double theta, const double *xs, const double *ys,
                         const double *vs, int n, const double *x0s, const double *y0s,
-                        const double *hs, int nb, double *xo, double *yo) {
+                        const double *hs, int nb, double *xo, double *yo,
+                        cudaEvent_t values_ready = nullptr) {
     if (n < 0 || nb < 0) {
         set_error(TC_ERR_INVALID, "negative size (nsources %d, nblocks %d)", n, nb);
         return TC_ERR_INVALID;
@@ -249,7 +254,7 @@ static int force_device(Context &c, double theta, const double *xs, const double
     }
     int rc;
     phase_mark(c, 0);
-    if ((rc = build_tree_moments(c, 1, xs, ys, vs, n))) return rc;
+    if ((rc = build_tree_moments(c, 1, xs, ys, vs, n, values_ready))) return rc;
     if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo, expansions_then_mark))) return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_force_mrag"))) return rc;
@@ -266,6 +271,38 @@ static int stage(Context &c, Slot s, const T *host, size_t n, T **dev) {
     return TC_OK;
 }
 
+// Host inputs in two parts: what the key sort needs first (x, y and anything `first` names)
+// on the main stream, then the source values and `later` arrays on the auxiliary stream once
+// the first part has been copied (one link, so the copies do not share it).  The solve's key
+// sort and tree build run while the later part is still in flight; c.ev_inputs marks the
+// values' arrival.  The buffers are allocated on the main stream before either copy.
+struct StagedArray {
+    Slot slot;
+    const double *host;
+    size_t n;
+    double **dev;
+};
+
+static int stage_split(Context &c, std::initializer_list<StagedArray> first,
+                       std::initializer_list<StagedArray> later) {
+    int rc;
+    for (const StagedArray &a : first)
+        if ((rc = stage(c, a.slot, a.host, a.n, a.dev))) return rc;
+    for (const StagedArray &a : later)
+        if ((rc = ensure(c, a.slot, a.n, a.dev))) return rc;
+    TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
+    TC_CUDA_TRY(cudaStreamWaitEvent(c.aux, c.ev_fork, 0));
+    bool values = true;
+    for (const StagedArray &a : later) {
+        if (a.n)
+            TC_CUDA_TRY(cudaMemcpyAsync(*a.dev, a.host, sizeof(double) * a.n,
+                                        cudaMemcpyHostToDevice, c.aux));
+        if (values) TC_CUDA_TRY(cudaEventRecord(c.ev_inputs, c.aux));   // after the values
+        values = false;
+    }
+    return TC_OK;
+}
+
 static int potential_host(Context &c, double theta, const double *xs, const double *ys,
                           const double *vs, int n, const double *xt, const double *yt, int m,
                           double *out) {
@@ -276,11 +313,17 @@ static int potential_host(Context &c, double theta, const double *xs, const doub
     if (m == 0) return TC_OK;
     int rc;
     double *dx, *dy, *dv, *dxt, *dyt, *dout;
-    if ((rc = stage(c, S_XIN, xs, n, &dx)) || (rc = stage(c, S_YIN, ys, n, &dy)) ||
-        (rc = stage(c, S_VIN, vs, n, &dv)) || (rc = stage(c, S_XT, xt, m, &dxt)) ||
-        (rc = stage(c, S_YT, yt, m, &dyt)) || (rc = ensure(c, S_OUTX, m, &dout)))
+    // the targets follow the values on the auxiliary stream, where the target sort runs
+    if ((rc = stage_split(c, {{S_XIN, xs, (size_t)n, &dx}, {S_YIN, ys, (size_t)n, &dy}},
+                          {{S_VIN, vs, (size_t)n, &dv}, {S_XT, xt, (size_t)m, &dxt},
+                           {S_YT, yt, (size_t)m, &dyt}})) ||
+        (rc = ensure(c, S_OUTX, m, &dout)))
         return rc;
-    if ((rc = potential_device(c, theta, dx, dy, dv, n, dxt, dyt, m, dout))) return rc;
+    rc = potential_device(c, theta, dx, dy, dv, n, dxt, dyt, m, dout, c.ev_inputs);
+    // the copies on the auxiliary stream read the caller's memory: done before returning
+    const cudaError_t e = cudaStreamSynchronize(c.aux);
+    if (rc) return rc;
+    TC_CUDA_TRY(e);
     TC_CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
     return TC_OK;
@@ -298,12 +341,16 @@ static int force_host(Context &c, double theta, const double *xs, const double *
     int rc;
     const size_t nt = (size_t)nb * BLOCKSIZE * BLOCKSIZE;
     double *dx, *dy, *dv, *d0x, *d0y, *dh, *dox, *doy;
-    if ((rc = stage(c, S_XIN, xs, n, &dx)) || (rc = stage(c, S_YIN, ys, n, &dy)) ||
-        (rc = stage(c, S_VIN, vs, n, &dv)) || (rc = stage(c, S_X0, x0s, nb, &d0x)) ||
-        (rc = stage(c, S_Y0, y0s, nb, &d0y)) || (rc = stage(c, S_H, hs, nb, &dh)) ||
+    if ((rc = stage_split(c, {{S_XIN, xs, (size_t)n, &dx}, {S_YIN, ys, (size_t)n, &dy},
+                              {S_X0, x0s, (size_t)nb, &d0x}, {S_Y0, y0s, (size_t)nb, &d0y},
+                              {S_H, hs, (size_t)nb, &dh}},
+                          {{S_VIN, vs, (size_t)n, &dv}})) ||
         (rc = ensure(c, S_OUTX, nt, &dox)) || (rc = ensure(c, S_OUTY, nt, &doy)))
         return rc;
-    if ((rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy))) return rc;
+    rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy, c.ev_inputs);
+    const cudaError_t e = cudaStreamSynchronize(c.aux);
+    if (rc) return rc;
+    TC_CUDA_TRY(e);
     TC_CUDA_TRY(cudaMemcpyAsync(xo, dox, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
     TC_CUDA_TRY(cudaMemcpyAsync(yo, doy, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));

@@ -372,12 +372,14 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
 // ---------------------------------------------------------------------------- source sort
 // The sources are sorted as 8-byte items (key << 32 | index) and gathered once at the end:
 //   * k_keys_pack reads x, y, v once and writes the Morton keys' digit histograms, the items
-//     in input order and a 32-byte record (x, y, v, 0) per source;
+//     in input order and a 32-byte record (x, y, v, 0) per source (k_keys_pack<false> and
+//     k_pack_rec split this in two when the values arrive later, see sort_sources);
 //   * four onesweep passes over the items (8-bit digits of the key half; 16 B of traffic per
 //     item and pass);
 //   * k_gather_sources reads each sorted item's record (one 32-byte DRAM sector) and writes
 //     the sorted keys, permutation, x, y and v.
 // Ties keep input order, so the result is the (key, index) lexicographic order.
+template <bool PACK>
 __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
                                                    const double *__restrict__ y,
                                                    const double *__restrict__ v, int n,
@@ -397,31 +399,38 @@ __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
     };
     const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) |
-          reinterpret_cast<uintptr_t>(v)) & 15) == 0) {
+          (PACK ? reinterpret_cast<uintptr_t>(v) : 0)) & 15) == 0) {
         // 16-byte loads and stores: two sources per thread and step
         const double2 *x2 = reinterpret_cast<const double2 *>(x);
         const double2 *y2 = reinterpret_cast<const double2 *>(y);
         const double2 *v2 = reinterpret_cast<const double2 *>(v);
         ulonglong2 *it2 = reinterpret_cast<ulonglong2 *>(items);
         for (int i = gid; i < n / 2; i += stride) {
-            const double2 a = x2[i], b = y2[i], w = v2[i];
+            const double2 a = x2[i], b = y2[i];
             it2[i] = make_ulonglong2(item_of(a.x, b.x, 2 * i), item_of(a.y, b.y, 2 * i + 1));
-            rec[4 * i + 0] = make_double2(a.x, b.x);
-            rec[4 * i + 1] = make_double2(w.x, 0.0);
-            rec[4 * i + 2] = make_double2(a.y, b.y);
-            rec[4 * i + 3] = make_double2(w.y, 0.0);
+            if (PACK) {
+                const double2 w = v2[i];
+                rec[4 * i + 0] = make_double2(a.x, b.x);
+                rec[4 * i + 1] = make_double2(w.x, 0.0);
+                rec[4 * i + 2] = make_double2(a.y, b.y);
+                rec[4 * i + 3] = make_double2(w.y, 0.0);
+            }
         }
         if ((n & 1) && gid == 0) {
             const int i = n - 1;
             items[i] = item_of(x[i], y[i], i);
-            rec[2 * i] = make_double2(x[i], y[i]);
-            rec[2 * i + 1] = make_double2(v[i], 0.0);
+            if (PACK) {
+                rec[2 * i] = make_double2(x[i], y[i]);
+                rec[2 * i + 1] = make_double2(v[i], 0.0);
+            }
         }
     } else {
         for (int i = gid; i < n; i += stride) {
             items[i] = item_of(x[i], y[i], i);
-            rec[2 * i] = make_double2(x[i], y[i]);
-            rec[2 * i + 1] = make_double2(v[i], 0.0);
+            if (PACK) {
+                rec[2 * i] = make_double2(x[i], y[i]);
+                rec[2 * i + 1] = make_double2(v[i], 0.0);
+            }
         }
     }
     __syncthreads();
@@ -546,6 +555,7 @@ __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
 constexpr int GS_THREADS = 256;
 constexpr int GS_ITEMS = 8;
 
+template <bool KEYS>
 __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
     const unsigned long long *__restrict__ items, const double2 *__restrict__ rec, int n,
     int *__restrict__ keys, int *__restrict__ perm, double *__restrict__ xs,
@@ -578,12 +588,36 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
                 atomicOr(err, DEVERR_BOUNDS);
                 continue;
             }
-            keys[i] = (int)(it[k] >> 32);
-            perm[i] = (int)id;
+            if (KEYS) {
+                keys[i] = (int)(it[k] >> 32);
+                perm[i] = (int)id;
+            }
             xs[i] = a[k].x;
             ys[i] = a[k].y;
             vs[i] = w[k];
         }
+    }
+}
+
+// The records (x, y, v, 0) in input order, when the values arrive after the sort has started.
+__global__ __launch_bounds__(256) void k_pack_rec(const double *__restrict__ x,
+                                                  const double *__restrict__ y,
+                                                  const double *__restrict__ v, int n,
+                                                  double2 *__restrict__ rec) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        rec[2 * i] = make_double2(x[i], y[i]);
+        rec[2 * i + 1] = make_double2(v[i], 0.0);
+    }
+}
+
+// Sorted keys and permutation from the sorted items.
+__global__ __launch_bounds__(256) void k_items_split(const unsigned long long *__restrict__ items,
+                                                     int n, int *__restrict__ keys,
+                                                     int *__restrict__ perm) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long it = items[i];
+        keys[i] = (int)(it >> 32);
+        perm[i] = (int)(unsigned)it;
     }
 }
 
@@ -717,8 +751,10 @@ int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
 }
 
 // ---------------------------------------------------------------------------- drivers
-int sort_sources(Context &c, const double *x, const double *y, const double *v, int n) {
+int sort_sources(Context &c, const double *x, const double *y, const double *v, int n,
+                 cudaEvent_t values_ready) {
     int rc;
+    c.late_ready = nullptr;   // a late-value sort of an earlier call that failed midway
     double *xs, *ys, *vs;
     int *keys, *perm;
     Frame *frame;
@@ -759,8 +795,13 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
                                 c.stream));
-    k_keys_pack<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, v, n, frame, items_a, rec,
-                                                            npasses, hist);
+    if (values_ready)
+        k_keys_pack<false><<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, nullptr, n, frame,
+                                                                      items_a, nullptr, npasses,
+                                                                      hist);
+    else
+        k_keys_pack<true><<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, v, n, frame, items_a,
+                                                                     rec, npasses, hist);
     TC_KERNEL_CHECK();
     k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
     TC_KERNEL_CHECK();
@@ -773,12 +814,40 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
             offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err);
         TC_KERNEL_CHECK();
     }
-    k_gather_sources<<<grid_for(n, GS_THREADS * GS_ITEMS, 8), GS_THREADS, 0, c.stream>>>(
+    c.nsrc = n;
+    if (values_ready) {
+        // the keys now (the tree needs nothing else); x/y/v in finish_sources
+        k_items_split<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(items_a, n, keys, perm);
+        TC_KERNEL_CHECK();
+        c.late_x = x;
+        c.late_y = y;
+        c.late_v = v;
+        c.late_ready = values_ready;
+        return TC_OK;
+    }
+    k_gather_sources<true><<<grid_for(n, GS_THREADS * GS_ITEMS, 8), GS_THREADS, 0, c.stream>>>(
         items_a, rec, n, keys, perm, xs, ys, vs, err);
     TC_KERNEL_CHECK();
-    c.nsrc = n;
     return TC_OK;
 }
+
+int finish_sources(Context &c) {
+    if (!c.late_ready) return TC_OK;
+    const int n = c.nsrc;
+    TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.late_ready, 0));
+    c.late_ready = nullptr;
+    double2 *rec = slot_ptr<double2>(c, S_REC);
+    k_pack_rec<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(c.late_x, c.late_y, c.late_v, n, rec);
+    TC_KERNEL_CHECK();
+    k_gather_sources<false><<<grid_for(n, GS_THREADS * GS_ITEMS, 8), GS_THREADS, 0, c.stream>>>(
+        slot_ptr<unsigned long long>(c, S_ITEMS_A), rec, n, nullptr, nullptr,
+        slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS), slot_ptr<double>(c, S_VS),
+        slot_ptr<unsigned>(c, S_ERR));
+    TC_KERNEL_CHECK();
+    return TC_OK;
+}
+
+
 
 int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys, int *idx) {
     (void)idx;

@@ -72,6 +72,12 @@ struct Context {
     // `stream`; ordered against `stream` with the events below
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_totals = nullptr, ev_join = nullptr;
+    // host entry points: x/y are copied on `stream`, v (and targets) on `aux` after them;
+    // ev_inputs marks v's arrival
+    cudaEvent_t ev_inputs = nullptr;
+    // a source sort whose values arrive late (sort_sources / finish_sources)
+    const double *late_x = nullptr, *late_y = nullptr, *late_v = nullptr;
+    cudaEvent_t late_ready = nullptr;
     DevBuf buf[S_NUM_SLOTS];
     unsigned *h_pinned = nullptr;         // small pinned staging area for readbacks
     int precision = 0;                    // 0 = plain FP64, 1 = mixed
@@ -140,7 +146,13 @@ int exclusive_scan(Context &c, const int *d_in, int *d_out, int n);   // d_out h
 int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, int nbits,
                      int *keys_a, int *vals_a, int *keys_b, int *vals_b, int **keys_out,
                      int **vals_out);
-int sort_sources(Context &c, const double *x, const double *y, const double *v, int n);
+// Sorts the sources.  With `values_ready`, an event that completes once v is in device memory,
+// v is read only by finish_sources() after a wait on that event, so that the key sort and the
+// tree build run while v is still being copied in; without it x/y/v are all sorted here and
+// finish_sources() does nothing.
+int sort_sources(Context &c, const double *x, const double *y, const double *v, int n,
+                 cudaEvent_t values_ready = nullptr);
+int finish_sources(Context &c);
 int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys, int *idx);
 
 // ---- tree.cu
