@@ -55,9 +55,9 @@ __device__ __forceinline__ int gallop_lower_bound(const int *__restrict__ keys, 
 // The split list: per tile of TL_TILE sources, each source's level mask (bit l: it starts an
 // inner cell of level l), a block scan
 // of the flags and the tile's global offset by a decoupled look-back over the tiles before it
-// (tile ids from an atomic counter, so a tile only waits on tiles already running; the wait is
-// bounded and raises DEVERR_SPIN_LIMIT).  The tile that holds the last source writes the list
-// length to *nlist_out.
+// (tile ids from an atomic counter, so a tile only waits on tiles already running; one warp
+// reads 32 predecessors per step; the wait is bounded and raises DEVERR_SPIN_LIMIT).  The tile
+// that holds the last source writes the list length to *nlist_out.
 constexpr int TL_THREADS = 256;
 constexpr int TL_ITEMS = 16;
 constexpr int TL_TILE = TL_THREADS * TL_ITEMS;
@@ -94,32 +94,47 @@ __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict_
     }
     int total;
     const int toff = block_exclusive_scan(cnt, &total);
-    if (threadIdx.x == 0) {
+    // Look-back by warp 0: 32 predecessors per step, lane q reading tile - 1 - q - (consumed)
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
         unsigned *mine = status + tile;
         int excl = 0;
         if (tile == 0) {
-            atomicExch(mine, TL_INC | (unsigned)total);
+            if (lane == 0) atomicExch(mine, TL_INC | (unsigned)total);
         } else {
-            atomicExch(mine, TL_AGG | (unsigned)total);
-            int spins = 0;
-            for (int j = tile - 1; j >= 0;) {
-                const unsigned st = *(const volatile unsigned *)(status + j);
+            if (lane == 0) atomicExch(mine, TL_AGG | (unsigned)total);
+            int j = tile - 1, spins = 0;
+            for (;;) {
+                const int jj = j - lane;
+                // before tile 0 reads as an inclusive prefix of 0
+                const unsigned st = jj >= 0 ? *(const volatile unsigned *)(status + jj) : TL_INC;
                 const unsigned flag = st & ~TL_VAL;
-                if (flag == 0) {
-                    if (++spins > TL_SPIN_LIMIT) {
-                        atomicOr(err, DEVERR_SPIN_LIMIT);
+                const unsigned inc = __ballot_sync(FULL_MASK, flag == TL_INC);
+                const unsigned none = __ballot_sync(FULL_MASK, flag == 0);
+                const int first_inc = inc ? __ffs(inc) - 1 : 31;
+                const unsigned upto = (2u << first_inc) - 1u;   // lanes 0 .. first_inc
+                if (none & upto) {
+                    // add what is published before the first unpublished predecessor, then
+                    // read again from it
+                    const int first_none = __ffs(none & upto) - 1;
+                    excl += __reduce_add_sync(FULL_MASK, lane < first_none ? st & TL_VAL : 0u);
+                    j -= first_none;
+                    if (first_none == 0 && ++spins > TL_SPIN_LIMIT) {
+                        if (lane == 0) atomicOr(err, DEVERR_SPIN_LIMIT);
                         break;
                     }
                     continue;
                 }
-                excl += (int)(st & TL_VAL);
-                if (flag == TL_INC) break;
-                --j;
+                excl += __reduce_add_sync(FULL_MASK, lane <= first_inc ? st & TL_VAL : 0u);
+                if (inc) break;
+                j -= 32;
             }
-            atomicExch(mine, TL_INC | (unsigned)(excl + total));
+            if (lane == 0) atomicExch(mine, TL_INC | (unsigned)(excl + total));
         }
-        s_excl = excl;
-        if ((long long)(tile + 1) * TL_TILE >= n) *nlist_out = excl + total;
+        if (lane == 0) {
+            s_excl = excl;
+            if ((long long)(tile + 1) * TL_TILE >= n) *nlist_out = excl + total;
+        }
     }
     __syncthreads();
     int j = s_excl + toff;
