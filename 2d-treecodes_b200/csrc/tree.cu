@@ -61,6 +61,8 @@ __device__ __forceinline__ int gallop_lower_bound(const int *__restrict__ keys, 
 constexpr int TL_THREADS = 256;
 constexpr int TL_ITEMS = 16;
 constexpr int TL_TILE = TL_THREADS * TL_ITEMS;
+constexpr int TL_HALO = LEAF_POTENTIAL;           // the largest leaf capacity
+constexpr int TL_STAGE = TL_TILE + 1 + TL_HALO;   // staged keys per tile
 constexpr unsigned TL_AGG = 1u << 30, TL_INC = 2u << 30, TL_VAL = (1u << 30) - 1;
 constexpr int TL_SPIN_LIMIT = 1 << 22;
 
@@ -70,21 +72,39 @@ __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict_
                                                           unsigned short *__restrict__ lmask,
                                                           int *nlist_out, unsigned *err) {
     __shared__ int s_tile, s_excl;
+    // the tile's keys with one before and leafcap after, staged by coalesced loads; word q is
+    // kept at q + q / 32 so that the 16-source runs of a warp's threads hit distinct banks
+    __shared__ int s_keys[TL_STAGE + TL_STAGE / 32 + 1];
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1);
     __syncthreads();
     const int tile = s_tile;
+    const int base = tile * TL_TILE - 1;   // key index of staged word 0
+    if (leafcap > TL_HALO) {
+        if (threadIdx.x == 0) atomicOr(err, DEVERR_BOUNDS);
+        return;   // every thread of every tile takes this branch: nothing waits on it
+    }
+    const int span = min(TL_TILE + 1 + leafcap, n - base);
+    for (int q = threadIdx.x; q < span; q += TL_THREADS) {
+        const int i = base + q;
+        s_keys[q + (q >> 5)] = i >= 0 ? keys[i] : 0;
+    }
+    __syncthreads();
+    auto staged = [&](int i) {
+        const int q = i - base;
+        return s_keys[q + (q >> 5)];
+    };
     const int i0 = tile * TL_TILE + threadIdx.x * TL_ITEMS;   // this thread's 16 sources
     unsigned short m[TL_ITEMS];
     int cnt = 0;
-    int prev = i0 > 0 && i0 <= n ? keys[i0 - 1] : 0;
+    int prev = i0 > 0 && i0 <= n ? staged(i0 - 1) : 0;
 #pragma unroll
     for (int k = 0; k < TL_ITEMS; ++k) {
         const int i = i0 + k;
         unsigned mk = 0;
         if (i < n) {
-            const int key = keys[i];
+            const int key = staged(i);
             const int cprev = i == 0 ? -1 : common_level(prev, key);
-            const int cnext = i + leafcap < n ? common_level(key, keys[i + leafcap]) : -1;
+            const int cnext = i + leafcap < n ? common_level(key, staged(i + leafcap)) : -1;
             const int hi = min(cnext, LMAX - 1);
             for (int l = cprev + 1; l <= hi; ++l) mk |= 1u << l;
             prev = key;
