@@ -186,7 +186,8 @@ static int build_tree_moments(Context &c, int kind, const double *x, const doubl
     if ((rc = build_topology(c, kind ? LEAF_FORCE : LEAF_POTENTIAL))) return rc;
     if ((rc = finish_sources(c))) return rc;
     phase_mark(c, 2);
-    if ((rc = upward_prepare(c, kind ? ORDER_FORCE : ORDER_POTENTIAL)) || (rc = upward_moments(c)))
+    if ((rc = upward_prepare(c, kind ? c.order_force : c.order_potential)) ||
+        (rc = upward_moments(c)))
         return rc;
     return TC_OK;
 }
@@ -241,11 +242,11 @@ static int force_device(Context &c, double theta, const double *xs, const double
         return TC_ERR_INVALID;
     }
     if (nb == 0) return TC_OK;
-    if (nb > (1 << 30) / (BLOCKSIZE * BLOCKSIZE)) {
+    if (nb > (1 << 30) / (c.blocksize * c.blocksize)) {
         set_error(TC_ERR_INVALID, "too many blocks (%d)", nb);
         return TC_ERR_INVALID;
     }
-    const size_t nt = (size_t)nb * BLOCKSIZE * BLOCKSIZE;
+    const size_t nt = (size_t)nb * c.blocksize * c.blocksize;
     if (n == 0) {
         TC_CUDA_TRY(cudaMemsetAsync(xo, 0, sizeof(double) * nt, c.stream));
         TC_CUDA_TRY(cudaMemsetAsync(yo, 0, sizeof(double) * nt, c.stream));
@@ -339,7 +340,7 @@ static int force_host(Context &c, double theta, const double *xs, const double *
     }
     if (nb == 0) return TC_OK;
     int rc;
-    const size_t nt = (size_t)nb * BLOCKSIZE * BLOCKSIZE;
+    const size_t nt = (size_t)nb * c.blocksize * c.blocksize;
     double *dx, *dy, *dv, *d0x, *d0y, *dh, *dox, *doy;
     if ((rc = stage_split(c, {{S_XIN, xs, (size_t)n, &dx}, {S_YIN, ys, (size_t)n, &dy},
                               {S_X0, x0s, (size_t)nb, &d0x}, {S_Y0, y0s, (size_t)nb, &d0y},
@@ -457,6 +458,43 @@ TC_API int tc_set_precision(tc_context *ctx, int precision) {
     }
     ctx->c.precision = precision;
     return TC_OK;
+}
+
+TC_API int tc_set_orders(tc_context *ctx, int potential_order, int force_order) {
+    clear_error();
+    if (!ctx) {
+        set_error(TC_ERR_INVALID, "no context");
+        return TC_ERR_INVALID;
+    }
+    int rc;
+    if ((rc = dispatch_order(potential_order, [](auto) -> int { return TC_OK; })) ||
+        (rc = dispatch_order(force_order, [](auto) -> int { return TC_OK; })))
+        return rc;
+    ctx->c.order_potential = potential_order;
+    ctx->c.order_force = force_order;
+    return TC_OK;
+}
+
+TC_API int tc_set_blocksize(tc_context *ctx, int blocksize) {
+    clear_error();
+    if (!ctx || (blocksize != 8 && blocksize != 16 && blocksize != 32 && blocksize != 64)) {
+        set_error(TC_ERR_INVALID, "unsupported MRAG block size %d (8, 16, 32 or 64)", blocksize);
+        return TC_ERR_INVALID;
+    }
+    ctx->c.blocksize = blocksize;
+    return TC_OK;
+}
+
+TC_API int tc_supported_orders(int *orders, int capacity) {
+    static const int list[] = {
+#define TC_ORDER_ITEM(P) P,
+        TC_FOR_EACH_ORDER(TC_ORDER_ITEM)
+#undef TC_ORDER_ITEM
+    };
+    const int n = (int)(sizeof(list) / sizeof(list[0]));
+    for (int i = 0; i < n && i < capacity; ++i)
+        if (orders) orders[i] = list[i];
+    return n;
 }
 
 TC_API int tc_set_timing(tc_context *ctx, int enabled) {

@@ -40,8 +40,23 @@ struct Brick {
     double h;
 };
 
-__device__ __forceinline__ Brick brick_geometry(double x0, double y0, double h, int q) {
-    const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
+// MRAG block layout: bs x bs targets per block (the reference's build-time BLOCKSIZE, 32 by
+// default), cut into 8 x 8 bricks, bps = bs / 8 per side; brick q of a block sits at column
+// q % bps, row q / bps (rows of bricks, treecode-force.cpp:110-111), and target (ix, iy) of
+// block b at ix + bs (iy + bs b).
+struct BlockLayout {
+    int bs, bps, bpb;   // targets per side, bricks per side, bricks per block
+};
+
+__device__ __forceinline__ void brick_of(const BlockLayout &L, int brick, int &blk, int &bx,
+                                         int &by) {
+    blk = brick / L.bpb;
+    const int q = brick - blk * L.bpb;
+    bx = (q % L.bps) * TILE;
+    by = (q / L.bps) * TILE;
+}
+
+__device__ __forceinline__ Brick brick_geometry(double x0, double y0, double h, int bx, int by) {
     Brick b;
     b.h = h;
     b.x0b = __fma_rn((double)bx + 3.5, h, x0);
@@ -78,7 +93,7 @@ constexpr int P2P_SEG = 2048;
 
 template <bool FILL>
 __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
-    int nbricks, const double *__restrict__ x0s, const double *__restrict__ y0s,
+    int nbricks, BlockLayout L, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int *__restrict__ lists,
     unsigned *err, unsigned long long *stats) {
@@ -91,8 +106,9 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
 
     for (int brick = blockIdx.x * TR_WARPS + warp; brick < nbricks;
          brick += gridDim.x * TR_WARPS) {
-        const int blk = brick >> 4;
-        const Brick b = brick_geometry(x0s[blk], y0s[blk], hs[blk], brick & 15);
+        int blk, bx, by;
+        brick_of(L, brick, blk, bx, by);
+        const Brick b = brick_geometry(x0s[blk], y0s[blk], hs[blk], bx, by);
         int o[3] = {0, 0, 0}, lim[3] = {0, 0, 0};
         if (FILL) {
 #pragma unroll
@@ -212,7 +228,7 @@ __device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
 // sums); the local expansion (E2L, L2P) stays FP64.
 template <int P, bool MIXED>
 __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
-    int nbricks, const double *__restrict__ x0s, const double *__restrict__ y0s,
+    int nbricks, BlockLayout L, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, const TNode *__restrict__ tnode,
     const double *__restrict__ mass, const double *__restrict__ exps,
     const int2 *__restrict__ range, const double *__restrict__ xs,
@@ -251,9 +267,10 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         const int brick = task_brick[task];
         const int part = task - (toff[brick] - tbase);
         const int nparts = toff[brick + 1] - toff[brick];
-        const int blk = brick >> 4, q = brick & 15;
+        int blk, bx, by;
+        brick_of(L, brick, blk, bx, by);
         const double h = hs[blk];
-        const Brick b = brick_geometry(x0s[blk], y0s[blk], h, q);
+        const Brick b = brick_geometry(x0s[blk], y0s[blk], h, bx, by);
         double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
 
         // ---------------- E2L: local expansion about the brick centre (force-kernels.m4:102-155)
@@ -548,9 +565,8 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         }
 
         if (nparts == 1) {
-            const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
-            const size_t o0 = (size_t)blk * BLOCKSIZE * BLOCKSIZE + (by + ty) * BLOCKSIZE + bx + tx;
-            const size_t o1 = o0 + 4 * BLOCKSIZE;
+            const size_t o0 = (size_t)blk * L.bs * L.bs + (size_t)(by + ty) * L.bs + bx + tx;
+            const size_t o1 = o0 + 4 * L.bs;
             xout[o0] = ax0;
             yout[o0] = ay0;
             xout[o1] = ax1;
@@ -598,7 +614,7 @@ __global__ void k_scale_coeffs(int nnodes, const TNode *__restrict__ tnode,
 }
 
 // Sum of the parts of every multi-task brick, in task order (deterministic).
-__global__ void k_force_gather_parts(int nbricks, const int *__restrict__ offs,
+__global__ void k_force_gather_parts(int nbricks, BlockLayout L, const int *__restrict__ offs,
                                      const double *__restrict__ partial, double *__restrict__ xout,
                                      double *__restrict__ yout) {
     const int lane = lane_id();
@@ -617,10 +633,10 @@ __global__ void k_force_gather_parts(int nbricks, const int *__restrict__ offs,
             ay1 += pp[96 + lane];
         }
         const int tx = lane & 7, ty = lane >> 3;
-        const int blk = brick >> 4, q = brick & 15;
-        const int bx = (q & 3) * TILE, by = (q >> 2) * TILE;
-        const size_t o0 = (size_t)blk * BLOCKSIZE * BLOCKSIZE + (by + ty) * BLOCKSIZE + bx + tx;
-        const size_t o1 = o0 + 4 * BLOCKSIZE;
+        int blk, bx, by;
+        brick_of(L, brick, blk, bx, by);
+        const size_t o0 = (size_t)blk * L.bs * L.bs + (size_t)(by + ty) * L.bs + bx + tx;
+        const size_t o1 = o0 + 4 * L.bs;
         xout[o0] = ax0;
         yout[o0] = ay0;
         xout[o1] = ax1;
@@ -635,11 +651,9 @@ static int sm_count() { return device_sm_count(); }
 // evaluation waits for both.
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
                int nblocks, double *xout, double *yout, OverlapFn between) {
-    if (c.order != ORDER_FORCE) {
-        set_error(TC_ERR_INVALID, "force evaluation needs an order-%d tree", ORDER_FORCE);
-        return TC_ERR_INVALID;
-    }
-    const int nbricks = nblocks * 16;
+    const int bps = c.blocksize / TILE;
+    const BlockLayout L = {c.blocksize, bps, bps * bps};
+    const int nbricks = nblocks * L.bpb;
     if (nbricks == 0) return TC_OK;
     int rc;
     // counts / offsets: E2L | E2P | P2P list lengths and evaluation tasks, nbricks each
@@ -656,7 +670,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         AuxScope on_aux(c);
         TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_fork, 0));
         k_force_lists<false><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
-            nbricks, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, err, nullptr);
+            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, err, nullptr);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
         for (int k = 0; k < 4; ++k)
@@ -683,7 +697,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         AuxScope on_aux(c);
         if ((rc = ensure(c, S_E2L, (size_t)tot[2] + 1, &lists))) return rc;
         k_force_lists<true><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
-            nbricks, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, err,
+            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, err,
             slot_ptr<unsigned long long>(c, S_STATS));
         TC_KERNEL_CHECK();
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
@@ -700,35 +714,42 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     k_task_map<<<(int)std::min<long long>((nbricks + 255) / 256, (long long)sm_count() * 8), 256, 0,
                  c.stream>>>(nbricks, offs, task_brick);
     TC_KERNEL_CHECK();
-    const bool mixed = c.precision == 1;
-    float2 *sexp = nullptr;
-    float *sscale = nullptr;
-    if (mixed) {
-        if ((rc = ensure(c, S_SEXP, (size_t)c.nnodes * ORDER_FORCE, &sexp)) ||
-            (rc = ensure(c, S_SSCALE, (size_t)c.nnodes, &sscale)))
-            return rc;
-        const long long items = (long long)c.nnodes * ORDER_FORCE;
-        k_scale_coeffs<ORDER_FORCE, true>
-            <<<(int)std::min<long long>((items + 255) / 256, (long long)sm_count() * 8), 256, 0,
-               c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
+    // the evaluation for the tree's expansion order
+    rc = dispatch_order(c.order, [&](auto order) -> int {
+        constexpr int P = decltype(order)::value;
+        int rc2;
+        const bool mixed = c.precision == 1;
+        float2 *sexp = nullptr;
+        float *sscale = nullptr;
+        if (mixed) {
+            if ((rc2 = ensure(c, S_SEXP, (size_t)c.nnodes * P, &sexp)) ||
+                (rc2 = ensure(c, S_SSCALE, (size_t)c.nnodes, &sscale)))
+                return rc2;
+            const long long items = (long long)c.nnodes * P;
+            k_scale_coeffs<P, true>
+                <<<(int)std::min<long long>((items + 255) / 256, (long long)sm_count() * 8), 256, 0,
+                   c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
+            TC_KERNEL_CHECK();
+        }
+        const int occ = mixed ? blocks_per_sm<k_force_eval<P, true>>(EV_WARPS * 32, 0)
+                              : blocks_per_sm<k_force_eval<P, false>>(EV_WARPS * 32, 0);
+        const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
+                                                    (long long)sm_count() * occ);
+        auto eval = mixed ? k_force_eval<P, true> : k_force_eval<P, false>;
+        phase_mark(c, 6);
+        eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
+            nbricks, L, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
+            slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
+            slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr, sexp, sscale,
+            task_brick);
         TC_KERNEL_CHECK();
-    }
-    const int occ = mixed ? blocks_per_sm<k_force_eval<ORDER_FORCE, true>>(EV_WARPS * 32, 0)
-                          : blocks_per_sm<k_force_eval<ORDER_FORCE, false>>(EV_WARPS * 32, 0);
-    const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
-                                                (long long)sm_count() * occ);
-    auto eval = mixed ? k_force_eval<ORDER_FORCE, true> : k_force_eval<ORDER_FORCE, false>;
-    phase_mark(c, 6);
-    eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
-        nbricks, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
-        slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-        slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr, sexp, sscale,
-        task_brick);
-    TC_KERNEL_CHECK();
+        return TC_OK;
+    });
+    if (rc) return rc;
     phase_mark(c, 7);
     if (ntasks > nbricks) {
         k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8, (long long)sm_count() * 16),
-                               256, 0, c.stream>>>(nbricks, offs, partial, xout, yout);
+                               256, 0, c.stream>>>(nbricks, L, offs, partial, xout, yout);
         TC_KERNEL_CHECK();
     }
     return TC_OK;

@@ -531,10 +531,6 @@ static int sm_count_p() { return device_sm_count(); }
 // main stream meanwhile, and the evaluation waits for both.
 int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out,
               OverlapFn between) {
-    if (c.order != ORDER_POTENTIAL) {
-        set_error(TC_ERR_INVALID, "potential evaluation needs an order-%d tree", ORDER_POTENTIAL);
-        return TC_ERR_INVALID;
-    }
     if (m == 0) return between ? between(c) : TC_OK;
     int rc;
     int *tkeys, *tperm, *tkeys2, *tperm2;
@@ -603,30 +599,37 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     k_task_map_groups<<<(int)std::min<long long>((ngroups + 255) / 256, (long long)sm_count_p() * 8),
                         256, 0, c.stream>>>(ngroups, offs, task_group);
     TC_KERNEL_CHECK();
-    const bool mixed = c.precision == 1;
-    float2 *sexp = nullptr;
-    float *sscale = nullptr;
-    if (mixed) {
-        if ((rc = ensure(c, S_SEXP, (size_t)c.nnodes * ORDER_POTENTIAL, &sexp)) ||
-            (rc = ensure(c, S_SSCALE, (size_t)c.nnodes, &sscale)))
-            return rc;
-        const long long items = (long long)c.nnodes * ORDER_POTENTIAL;
-        k_scale_coeffs_pot<ORDER_POTENTIAL>
-            <<<(int)std::min<long long>((items + 255) / 256, (long long)sm_count_p() * 8), 256, 0,
-               c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
+    // the evaluation for the tree's expansion order
+    rc = dispatch_order(c.order, [&](auto order) -> int {
+        constexpr int P = decltype(order)::value;
+        int rc2;
+        const bool mixed = c.precision == 1;
+        float2 *sexp = nullptr;
+        float *sscale = nullptr;
+        if (mixed) {
+            if ((rc2 = ensure(c, S_SEXP, (size_t)c.nnodes * P, &sexp)) ||
+                (rc2 = ensure(c, S_SSCALE, (size_t)c.nnodes, &sscale)))
+                return rc2;
+            const long long items = (long long)c.nnodes * P;
+            k_scale_coeffs_pot<P>
+                <<<(int)std::min<long long>((items + 255) / 256, (long long)sm_count_p() * 8), 256, 0,
+                   c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
+            TC_KERNEL_CHECK();
+        }
+        auto eval = mixed ? k_potential_eval<P, true> : k_potential_eval<P, false>;
+        const int occ = mixed ? blocks_per_sm<k_potential_eval<P, true>>(PE_WARPS * 32, 0)
+                              : blocks_per_sm<k_potential_eval<P, false>>(PE_WARPS * 32, 0);
+        const int egrid = (int)std::min<long long>((ntasks + PE_WARPS - 1) / PE_WARPS,
+                                                   (long long)sm_count_p() * occ);
+        phase_mark(c, 6);
+        eval<<<egrid, PE_WARPS * 32, 0, c.stream>>>(
+            ngroups, m, xt, yt, vo, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
+            slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
+            slot_ptr<double>(c, S_VS), offs, lists, out, partial, task_ctr, task_group, sexp, sscale);
         TC_KERNEL_CHECK();
-    }
-    auto eval = mixed ? k_potential_eval<ORDER_POTENTIAL, true> : k_potential_eval<ORDER_POTENTIAL, false>;
-    const int occ = mixed ? blocks_per_sm<k_potential_eval<ORDER_POTENTIAL, true>>(PE_WARPS * 32, 0)
-                          : blocks_per_sm<k_potential_eval<ORDER_POTENTIAL, false>>(PE_WARPS * 32, 0);
-    const int egrid = (int)std::min<long long>((ntasks + PE_WARPS - 1) / PE_WARPS,
-                                               (long long)sm_count_p() * occ);
-    phase_mark(c, 6);
-    eval<<<egrid, PE_WARPS * 32, 0, c.stream>>>(
-        ngroups, m, xt, yt, vo, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
-        slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-        slot_ptr<double>(c, S_VS), offs, lists, out, partial, task_ctr, task_group, sexp, sscale);
-    TC_KERNEL_CHECK();
+        return TC_OK;
+    });
+    if (rc) return rc;
     phase_mark(c, 7);
     if (ntasks > ngroups) {
         k_potential_gather_parts<<<(int)std::min<long long>((ngroups + 7) / 8, (long long)sm_count_p() * 16),

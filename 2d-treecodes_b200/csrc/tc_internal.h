@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <type_traits>
 #include <utility>
 
 #include "tc_common.cuh"
@@ -64,6 +65,27 @@ struct Counts {
 // Device-side work counters (unsigned long long each) in the S_STATS slot.
 enum { STAT_P2P_SOURCES = 0, STAT_E2P_PAIRS = 1, STAT_P2P_PAIRS = 2, STAT_SLOTS = 8 };
 
+// Expansion orders a context can be set to (tc_set_orders).  The reference fixes its orders at
+// build time (Makefile:13-14 of the reference: 12 for the potential, 24 for the force); here
+// every order-dependent kernel is instantiated for each order of this list.  28 is the
+// largest order whose E2L binomials C(2p - 1, p - 1) are exact in FP64.
+#define TC_FOR_EACH_ORDER(X) X(4) X(8) X(12) X(16) X(20) X(24) X(28)
+
+// f(std::integral_constant<int, p>) for a supported order p; TC_ERR_INVALID otherwise.
+template <class F>
+int dispatch_order(int p, F &&f) {
+    switch (p) {
+#define TC_ORDER_CASE(P) \
+    case P:              \
+        return f(std::integral_constant<int, P>{});
+        TC_FOR_EACH_ORDER(TC_ORDER_CASE)
+#undef TC_ORDER_CASE
+    default:
+        set_error(TC_ERR_INVALID, "unsupported expansion order %d", p);
+        return TC_ERR_INVALID;
+    }
+}
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -81,6 +103,9 @@ struct Context {
     DevBuf buf[S_NUM_SLOTS];
     unsigned *h_pinned = nullptr;         // small pinned staging area for readbacks
     int precision = 0;                    // 0 = plain FP64, 1 = mixed
+    int order_potential = ORDER_POTENTIAL;  // expansion orders of the next solves
+    int order_force = ORDER_FORCE;
+    int blocksize = BLOCKSIZE;            // MRAG block side of the force entry points
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};

@@ -788,12 +788,10 @@ static int run_expansions(Context &c) {
 }
 
 int upward_prepare(Context &c, int order) {
-    if (order != ORDER_POTENTIAL && order != ORDER_FORCE) {
-        set_error(TC_ERR_INVALID, "unsupported expansion order %d", order);
-        return TC_ERR_INVALID;
-    }
+    // an order without kernel instances is refused here, before any work
+    int rc = dispatch_order(order, [](auto) -> int { return TC_OK; });
+    if (rc) return rc;
     const int nn = c.nnodes;
-    int rc;
     double *mass, *w, *wx, *wy, *exps;
     if ((rc = ensure(c, S_MASS, nn, &mass)) || (rc = ensure(c, S_W, nn, &w)) ||
         (rc = ensure(c, S_WX, nn, &wx)) || (rc = ensure(c, S_WY, nn, &wy)) ||
@@ -804,8 +802,8 @@ int upward_prepare(Context &c, int order) {
 }
 
 int upward_expansions(Context &c) {
-    return c.order == ORDER_POTENTIAL ? run_expansions<ORDER_POTENTIAL>(c)
-                                      : run_expansions<ORDER_FORCE>(c);
+    return dispatch_order(c.order,
+                          [&](auto p) -> int { return run_expansions<decltype(p)::value>(c); });
 }
 
 int upward_pass(Context &c, int order) {

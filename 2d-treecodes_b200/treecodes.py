@@ -22,6 +22,8 @@ LIB_PATH = os.path.join(HERE, "lib", "lib2d-treecodes-b200.so")
 ORDER = {"potential": 12, "force": 24}
 LEAF = {"potential": 512, "force": 192}
 BLOCKSIZE = 32
+ORDER_POTENTIAL = 12   # the reference's default orders (its Makefile:13-14)
+ORDER_FORCE = 24
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -38,6 +40,9 @@ SIGNATURES = {
     "tc_context_create": (_i, [ctypes.POINTER(_vp), _i, _vp]),
     "tc_context_destroy": (None, [_vp]),
     "tc_set_precision": (_i, [_vp, _i]),
+    "tc_set_orders": (_i, [_vp, _i, _i]),
+    "tc_supported_orders": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
+    "tc_set_blocksize": (_i, [_vp, _i]),
     "tc_set_timing": (_i, [_vp, _i]),
     "tc_get_stats": (_i, [_vp, _vp]),
     "tc_get_stream": (_vp, [_vp]),
@@ -177,6 +182,14 @@ def treecode_force_mrag(theta, xsources, ysources, sourcevalues, x0s, y0s, hs):
     return xo, yo
 
 
+def supported_orders():
+    """The expansion orders Context.set_orders accepts."""
+    n = load().tc_supported_orders(None, 0)
+    buf = (ctypes.c_int * n)()
+    load().tc_supported_orders(buf, n)
+    return list(buf)
+
+
 def measure_fma_peak(fp64=True):
     t = ctypes.c_double()
     _check(load().tc_measure_fma_peak(1 if fp64 else 0, ctypes.byref(t)))
@@ -200,6 +213,7 @@ class Context:
         h = _vp()
         _check(self.lib.tc_context_create(ctypes.byref(h), int(device), stream))
         self.h = h
+        self.blocksize = BLOCKSIZE
         if precision:
             _check(self.lib.tc_set_precision(self.h, int(precision)))
         if timing:
@@ -223,6 +237,17 @@ class Context:
     def set_precision(self, mode):
         _check(self.lib.tc_set_precision(self.h, int(mode)))
 
+    def set_orders(self, potential_order=ORDER_POTENTIAL, force_order=ORDER_FORCE):
+        """Expansion orders of the next solves (the reference's build-time potential-order and
+        force-order); one of supported_orders() each."""
+        _check(self.lib.tc_set_orders(self.h, int(potential_order), int(force_order)))
+
+    def set_blocksize(self, blocksize=BLOCKSIZE):
+        """MRAG block side of the next force solves (8, 16, 32 or 64; the reference's
+        build-time mrag-blocksize): outputs of nblocks * blocksize**2 values."""
+        _check(self.lib.tc_set_blocksize(self.h, int(blocksize)))
+        self.blocksize = int(blocksize)
+
     def set_timing(self, on=True):
         self.lib.tc_set_timing(self.h, 1 if on else 0)
 
@@ -241,7 +266,7 @@ class Context:
 
     def force_mrag_host(self, theta, xs, ys, vs, x0s, y0s, hs, xo=None, yo=None):
         xs, ys, vs, x0, y0, h = map(_f64, (xs, ys, vs, x0s, y0s, hs))
-        nt = len(x0) * BLOCKSIZE * BLOCKSIZE
+        nt = len(x0) * self.blocksize * self.blocksize
         xo = np.empty(nt) if xo is None else xo
         yo = np.empty(nt) if yo is None else yo
         _check(self.lib.tc_force_mrag_host(self.h, float(theta), _p(xs), _p(ys), _p(vs), len(xs),

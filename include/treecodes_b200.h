@@ -96,6 +96,18 @@ typedef struct {
 TC_API int tc_context_create(tc_context **ctx, int device, void *cuda_stream);
 TC_API void tc_context_destroy(tc_context *ctx);
 TC_API int tc_set_precision(tc_context *ctx, int precision);
+/* Expansion orders of the context's next solves: the reference fixes them when it is built
+ * (Makefile:13-14 of the reference, potential-order = 12 and force-order = 24, which stay the
+ * defaults here).  Any order that tc_supported_orders lists may be chosen, independently for
+ * the two entry points; others are refused with TC_ERR_INVALID. */
+TC_API int tc_set_orders(tc_context *ctx, int potential_order, int force_order);
+/* Writes up to `capacity` supported orders (ascending) to `orders`; returns how many exist. */
+TC_API int tc_supported_orders(int *orders, int capacity);
+/* MRAG block side of the context's force solves (tc_force_mrag_host / _device): 8, 16, 32 or
+ * 64 targets, the reference's build-time mrag-blocksize (Makefile:15 of the reference, 32 by
+ * default and for treecode_force_mrag).  Outputs hold nblocks * blocksize^2 values, target
+ * (ix, iy) of block ib at ix + blocksize * (iy + blocksize * ib). */
+TC_API int tc_set_blocksize(tc_context *ctx, int blocksize);
 TC_API int tc_set_timing(tc_context *ctx, int enabled);
 TC_API int tc_get_stats(tc_context *ctx, tc_stats *out);
 TC_API void *tc_get_stream(tc_context *ctx);

@@ -44,7 +44,9 @@ def available() -> bool:
 
 
 def lib(kind: str, mode: str = "exact64"):
-    """kind: 'potential' | 'force' | 'direct'; mode: 'exact64' | 'faithful' | 'big'."""
+    """kind: 'potential' | 'force' | 'direct'; mode: 'exact64' | 'faithful' | 'big', or
+    'exact64_o8' / 'exact64_o16' / 'exact64_o28' (the EXACT64 build at that expansion order),
+    'exact64_b16' / 'exact64_b64' (force, the EXACT64 build with that MRAG block side)."""
     key = (kind, mode)
     if key not in _libs:
         name = "liboracle_direct.so" if kind == "direct" else f"libref_{kind}_{mode}.so"
@@ -89,12 +91,13 @@ def potential(theta, xs, ys, vs, xt, yt, mode="exact64"):
     return out
 
 
-def force_mrag(theta, xs, ys, vs, x0s, y0s, hs, mode="exact64"):
-    """drivers/treecode-force.cpp:203-236 run on the CPU; outputs ix + 32*(iy + 32*ib)."""
+def force_mrag(theta, xs, ys, vs, x0s, y0s, hs, mode="exact64", blocksize=32):
+    """drivers/treecode-force.cpp:203-236 run on the CPU; outputs ix + bs*(iy + bs*ib).  A block
+    side other than 32 needs the build of that BLOCKSIZE (mode 'exact64_b16' / 'exact64_b64')."""
     xs, ys, vs, x0s, y0s, hs = map(_f64, (xs, ys, vs, x0s, y0s, hs))
     nb = len(x0s)
-    xo = np.zeros(nb * 1024)
-    yo = np.zeros(nb * 1024)
+    xo = np.zeros(nb * blocksize * blocksize)
+    yo = np.zeros(nb * blocksize * blocksize)
     lib("force", mode).treecode_force_mrag(float(theta), _ptr(xs), _ptr(ys), _ptr(vs), len(xs),
                                           _ptr(x0s), _ptr(y0s), _ptr(hs), nb, _ptr(xo), _ptr(yo))
     return xo, yo

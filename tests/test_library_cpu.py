@@ -44,6 +44,14 @@ def test_python_binding_covers_header():
     assert sorted(T.SIGNATURES) == header_symbols()
 
 
+def test_supported_orders_list():
+    """tc_supported_orders needs no device: the orders with kernel instances, the reference's
+    defaults 12 and 24 among them."""
+    orders = T.supported_orders()
+    assert orders == sorted(orders) and {T.ORDER_POTENTIAL, T.ORDER_FORCE} <= set(orders)
+    assert max(orders) <= 28   # E2L binomials C(2p-1, p-1) exact in FP64
+
+
 def test_library_is_sm100a_build():
     out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", T.LIB_PATH],
                          capture_output=True, text=True)
