@@ -43,17 +43,23 @@ struct Brick {
 // MRAG block layout: bs x bs targets per block (the reference's build-time BLOCKSIZE, 32 by
 // default), cut into 8 x 8 bricks, bps = bs / 8 per side; brick q of a block sits at column
 // q % bps, row q / bps (rows of bricks, treecode-force.cpp:110-111), and target (ix, iy) of
-// block b at ix + bs (iy + bs b).
+// block b at ix + bs (iy + bs b).  The sides are powers of two, kept as their logarithms.
 struct BlockLayout {
-    int bs, bps, bpb;   // targets per side, bricks per side, bricks per block
+    int lbs, lbps;   // log2 of the targets and of the bricks per block side
 };
 
 __device__ __forceinline__ void brick_of(const BlockLayout &L, int brick, int &blk, int &bx,
                                          int &by) {
-    blk = brick / L.bpb;
-    const int q = brick - blk * L.bpb;
-    bx = (q % L.bps) * TILE;
-    by = (q / L.bps) * TILE;
+    blk = brick >> (2 * L.lbps);
+    const int q = brick & ((1 << (2 * L.lbps)) - 1);
+    bx = (q & ((1 << L.lbps) - 1)) * TILE;
+    by = (q >> L.lbps) * TILE;
+}
+
+// Output index of target (bx + tx, by + ty) of block blk.
+__device__ __forceinline__ size_t target_index(const BlockLayout &L, int blk, int bx, int by,
+                                               int tx, int ty) {
+    return ((size_t)blk << (2 * L.lbs)) + ((by + ty) << L.lbs) + bx + tx;
 }
 
 __device__ __forceinline__ Brick brick_geometry(double x0, double y0, double h, int bx, int by) {
@@ -226,9 +232,12 @@ __device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
 // MIXED = false: plain FP64.  MIXED = true: P2P and E2P in FP32 (float offsets from the brick
 // corner split into hi + lo parts, scaled multipole coefficients, compensated per-target
 // sums); the local expansion (E2L, L2P) stays FP64.
-template <int P, bool MIXED>
+// LBS > 0: the block layout of side 2^LBS fixed at compile time (the default side 32 has its
+// own instances: the layout arithmetic on kernel arguments measured 3% slower); LBS = 0: the
+// layout L given at run time.
+template <int P, bool MIXED, int LBS>
 __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
-    int nbricks, BlockLayout L, const double *__restrict__ x0s, const double *__restrict__ y0s,
+    int nbricks, BlockLayout L_arg, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, const TNode *__restrict__ tnode,
     const double *__restrict__ mass, const double *__restrict__ exps,
     const int2 *__restrict__ range, const double *__restrict__ xs,
@@ -237,6 +246,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     double *__restrict__ yout, double *__restrict__ partial, int *task_ctr,
     const float2 *__restrict__ sexp, const float *__restrict__ sscale,
     const int *__restrict__ task_brick) {
+    const BlockLayout L = LBS ? BlockLayout{LBS, LBS - 3} : L_arg;
     __shared__ EvalShared<P> shared[EV_WARPS];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     EvalShared<P> &sh = shared[warp];
@@ -565,8 +575,8 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         }
 
         if (nparts == 1) {
-            const size_t o0 = (size_t)blk * L.bs * L.bs + (size_t)(by + ty) * L.bs + bx + tx;
-            const size_t o1 = o0 + 4 * L.bs;
+            const size_t o0 = target_index(L, blk, bx, by, tx, ty);
+            const size_t o1 = o0 + ((size_t)4 << L.lbs);
             xout[o0] = ax0;
             yout[o0] = ay0;
             xout[o1] = ax1;
@@ -635,8 +645,8 @@ __global__ void k_force_gather_parts(int nbricks, BlockLayout L, const int *__re
         const int tx = lane & 7, ty = lane >> 3;
         int blk, bx, by;
         brick_of(L, brick, blk, bx, by);
-        const size_t o0 = (size_t)blk * L.bs * L.bs + (size_t)(by + ty) * L.bs + bx + tx;
-        const size_t o1 = o0 + 4 * L.bs;
+        const size_t o0 = target_index(L, blk, bx, by, tx, ty);
+        const size_t o1 = o0 + ((size_t)4 << L.lbs);
         xout[o0] = ax0;
         yout[o0] = ay0;
         xout[o1] = ax1;
@@ -651,9 +661,10 @@ static int sm_count() { return device_sm_count(); }
 // evaluation waits for both.
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
                int nblocks, double *xout, double *yout, OverlapFn between) {
-    const int bps = c.blocksize / TILE;
-    const BlockLayout L = {c.blocksize, bps, bps * bps};
-    const int nbricks = nblocks * L.bpb;
+    BlockLayout L = {0, 0};
+    while ((1 << L.lbs) < c.blocksize) ++L.lbs;   // 8, 16, 32 or 64 (tc_set_blocksize)
+    L.lbps = L.lbs - 3;
+    const int nbricks = nblocks << (2 * L.lbps);
     if (nbricks == 0) return TC_OK;
     int rc;
     // counts / offsets: E2L | E2P | P2P list lengths and evaluation tasks, nbricks each
@@ -731,11 +742,14 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                    c.stream>>>(c.nnodes, tnode, slot_ptr<double>(c, S_EXPS), sexp, sscale);
             TC_KERNEL_CHECK();
         }
-        const int occ = mixed ? blocks_per_sm<k_force_eval<P, true>>(EV_WARPS * 32, 0)
-                              : blocks_per_sm<k_force_eval<P, false>>(EV_WARPS * 32, 0);
+        constexpr int LBS32 = 5;   // the default block side, 32
+        const bool fixed = L.lbs == LBS32;
+        auto eval = mixed ? (fixed ? k_force_eval<P, true, LBS32> : k_force_eval<P, true, 0>)
+                          : (fixed ? k_force_eval<P, false, LBS32> : k_force_eval<P, false, 0>);
+        const int occ = mixed ? blocks_per_sm<k_force_eval<P, true, LBS32>>(EV_WARPS * 32, 0)
+                              : blocks_per_sm<k_force_eval<P, false, LBS32>>(EV_WARPS * 32, 0);
         const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
                                                     (long long)sm_count() * occ);
-        auto eval = mixed ? k_force_eval<P, true> : k_force_eval<P, false>;
         phase_mark(c, 6);
         eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
             nbricks, L, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
