@@ -230,8 +230,12 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
     __shared__ float2 s_coef32[PE_WARPS][P];
     __shared__ double2 s_xy[PE_WARPS][PE_CHUNK];
     __shared__ double s_v[PE_WARPS][PE_CHUNK];
-    __shared__ float4 s_off[PE_WARPS][PE_CHUNK];   // (x hi, x lo, y hi, y lo) from the reference
-    __shared__ float s_v32[PE_WARPS][PE_CHUNK];
+    // mixed form: the tile as negated float offsets (hi + lo) from the group's reference point,
+    // two sources per entry for paired-FP32 (f32x2) arithmetic: (-x hi, -x hi', -x lo, -x lo'),
+    // the same for y, and (v, v')
+    __shared__ float4 s_nx[PE_WARPS][PE_CHUNK / 2];
+    __shared__ float4 s_ny[PE_WARPS][PE_CHUNK / 2];
+    __shared__ float2 s_v2[PE_WARPS][PE_CHUNK / 2];
     __shared__ double s_part[PE_WARPS][32];        // P2P lane partials of a sparse mask
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     const double eps = 10 * DBL_EPSILON;
@@ -382,17 +386,26 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                 const unsigned cmask = msk;   // this tile's targets (msk moves on to the next tile)
                 const bool mine = (cmask >> lane) & 1;
                 __syncwarp();
-                if (lane < cnt) {
-                    if (MIXED) {
-                        float a, b2, c2, d2;
+                if (MIXED) {
+                    // source `lane` to entry lane / 2, half lane % 2; lanes past the tile add a
+                    // zero-valued source at the reference point (finite, contributes 0)
+                    float a = 0.f, b2 = 0.f, c2 = 0.f, d2 = 0.f, vv = 0.f;
+                    if (lane < cnt) {
                         split2(px - xref, a, b2);
                         split2(py - yref, c2, d2);
-                        s_off[warp][lane] = make_float4(a, b2, c2, d2);
-                        s_v32[warp][lane] = (float)pv;
-                    } else {
-                        s_xy[warp][lane] = make_double2(px, py);
-                        s_v[warp][lane] = pv;
+                        vv = (float)pv;
                     }
+                    float *nx = reinterpret_cast<float *>(s_nx[warp]);
+                    float *ny = reinterpret_cast<float *>(s_ny[warp]);
+                    const int e = 4 * (lane >> 1) + (lane & 1);
+                    nx[e] = -a;
+                    nx[e + 2] = -b2;
+                    ny[e] = -c2;
+                    ny[e + 2] = -d2;
+                    reinterpret_cast<float *>(s_v2[warp])[lane] = vv;
+                } else if (lane < cnt) {
+                    s_xy[warp][lane] = make_double2(px, py);
+                    s_v[warp][lane] = pv;
                 }
                 __syncwarp();
                 next_tile(t0, tn, msk);
@@ -410,15 +423,25 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                 if (k > (MIXED ? 8 : 16)) {
                     if (mine) {
                         if (MIXED) {
-                            float acc = 0;
+                            // two sources per step in f32x2 lanes; even and odd sources are
+                            // summed apart and added at the end of the tile
+                            const float2 txh2 = make_float2(txh, txh), txl2 = make_float2(txl, txl);
+                            const float2 tyh2 = make_float2(tyh, tyh), tyl2 = make_float2(tyl, tyl);
+                            const float2 eps2 = make_float2(epsf, epsf);
+                            float2 acc = make_float2(0.f, 0.f);
+                            const int npairs = (cnt + 1) >> 1;
 #pragma unroll 4
-                            for (int q = 0; q < cnt; ++q) {
-                                const float4 o = s_off[warp][q];
-                                const float dx = (txh - o.x) + (txl - o.y);
-                                const float dy = (tyh - o.z) + (tyl - o.w);
-                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), s_v32[warp][q], acc);
+                            for (int q = 0; q < npairs; ++q) {
+                                const float4 nx = s_nx[warp][q], ny = s_ny[warp][q];
+                                const float2 dx = __fadd2_rn(__fadd2_rn(txh2, make_float2(nx.x, nx.y)),
+                                                             __fadd2_rn(txl2, make_float2(nx.z, nx.w)));
+                                const float2 dy = __fadd2_rn(__fadd2_rn(tyh2, make_float2(ny.x, ny.y)),
+                                                             __fadd2_rn(tyl2, make_float2(ny.z, ny.w)));
+                                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, eps2));
+                                acc = __ffma2_rn(make_float2(lg2_approx(r2.x), lg2_approx(r2.y)),
+                                                 s_v2[warp][q], acc);
                             }
-                            two_sum_add(nh, nl, acc * ln2);
+                            two_sum_add(nh, nl, (acc.x + acc.y) * ln2);
                         } else {
 #pragma unroll 2
                             for (int q = 0; q < cnt; ++q) {
@@ -439,12 +462,15 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                         const float qyh = __shfl_sync(FULL_MASK, tyh, tl);
                         const float qyl = __shfl_sync(FULL_MASK, tyl, tl);
                         float acc = 0;
+                        const float *nx = reinterpret_cast<const float *>(s_nx[warp]);
+                        const float *ny = reinterpret_cast<const float *>(s_ny[warp]);
+                        const float *sv = reinterpret_cast<const float *>(s_v2[warp]);
                         if (lane < r * k)
                             for (int q = lane / k; q < cnt; q += r) {
-                                const float4 o = s_off[warp][q];
-                                const float dx = (qxh - o.x) + (qxl - o.y);
-                                const float dy = (qyh - o.z) + (qyl - o.w);
-                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), s_v32[warp][q], acc);
+                                const int e = 4 * (q >> 1) + (q & 1);
+                                const float dx = (qxh + nx[e]) + (qxl + nx[e + 2]);
+                                const float dy = (qyh + ny[e]) + (qyl + ny[e + 2]);
+                                acc = fmaf(lg2_approx(fmaf(dx, dx, fmaf(dy, dy, epsf))), sv[q], acc);
                             }
                         part = (double)acc;
                     } else {
