@@ -97,18 +97,28 @@ constexpr int TR_STACK = 2048;
 // does the far field), so that the few bricks on a dense region do not serialise the kernel.
 constexpr int P2P_SEG = 2048;
 
-template <bool FILL>
+// MODE 0: count the lists; MODE 1: write them at the scanned offsets (CSR); MODE 2: count
+// them and write each warp's entries into its own scratch region (kind k of warp w from
+// (k W + w) cap on), recording where each brick's run starts, so that a copy into CSR order
+// replaces the second walk.  A region that fills up sets meta[0] (the host then falls back to
+// MODE 1); meta[1] receives the largest run of entries any warp wrote, for sizing the regions.
+template <int MODE>
 __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
     int nbricks, BlockLayout L, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int *__restrict__ lists,
+    int *__restrict__ scratch, int cap, int *__restrict__ sstart, int *meta,
     unsigned *err, unsigned long long *stats) {
+    constexpr bool FILL = MODE == 1;
     __shared__ int stack_all[TR_WARPS][TR_STACK];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     int *stack = stack_all[warp];
     const double inv_theta = 1.0 / theta, theta2 = theta * theta;
     const unsigned lt = lanemask_lt();
     unsigned long long p2p_sources = 0;   // per lane: sources of the P2P leaves it listed
+    const int wglob = blockIdx.x * TR_WARPS + warp, nwarps = gridDim.x * TR_WARPS;
+    int cur[3] = {0, 0, 0};               // MODE 2: entries this warp has written, per kind
+    bool full = false;
 
     for (int brick = blockIdx.x * TR_WARPS + warp; brick < nbricks;
          brick += gridDim.x * TR_WARPS) {
@@ -139,7 +149,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                     kind = classify(nd, b, inv_theta, theta2);
                     child = nd.child;
                     if (kind == K_P2P) bsrc += nd.count;
-                    if (FILL && kind == K_P2P) p2p_sources += (unsigned)nd.count;
+                    if (MODE != 0 && kind == K_P2P && stats) p2p_sources += (unsigned)nd.count;
                     if (kind == K_DESCEND && (child <= node || child + 4 > nnodes)) {
                         atomicOr(err, DEVERR_BOUNDS);
                         kind = K_SKIP;
@@ -156,6 +166,11 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                     const int at = o[k] + n[k] + __popc(bal & lt);
                     if (at < lim[k]) lists[at] = node;
                     else atomicOr(err, DEVERR_BOUNDS);
+                }
+                if (MODE == 2 && kind == k) {
+                    const int at = cur[k] + n[k] + __popc(bal & lt);
+                    if (at < cap) scratch[(size_t)(k * nwarps + wglob) * cap + at] = node;
+                    else full = true;
                 }
                 n[k] += __popc(bal);
             }
@@ -181,14 +196,41 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                 counts[2 * nbricks + brick] = n[2];
                 // evaluation tasks: the brick's P2P sources in segments of at most P2P_SEG
                 counts[3 * nbricks + brick] = max(1, (total + P2P_SEG - 1) / P2P_SEG);
+                if (MODE == 2)
+                    for (int k = 0; k < 3; ++k)
+                        sstart[k * nbricks + brick] = (k * nwarps + wglob) * cap + cur[k];
             }
+            if (MODE == 2)
+                for (int k = 0; k < 3; ++k) cur[k] += n[k];
         }
         __syncwarp();
     }
-    if (FILL) {
+    if (MODE == 2) {
+        if (__any_sync(FULL_MASK, full) && lane == 0) atomicOr(&meta[0], 1);
+        if (lane == 0) atomicMax(&meta[1], max(cur[0], max(cur[1], cur[2])));
+    }
+    if (MODE != 0 && stats) {
         for (int m = 16; m; m >>= 1) p2p_sources += __shfl_xor_sync(FULL_MASK, p2p_sources, m);
         if (lane == 0 && p2p_sources) atomicAdd(&stats[STAT_P2P_SOURCES], p2p_sources);
     }
+}
+
+// The lists in CSR order from the scratch runs of k_force_lists<2>: warp per brick.
+__global__ __launch_bounds__(256) void k_force_lists_copy(int nbricks,
+                                                          const int *__restrict__ counts,
+                                                          const int *__restrict__ offs,
+                                                          const int *__restrict__ sstart,
+                                                          const int *__restrict__ scratch,
+                                                          int *__restrict__ lists) {
+    const int lane = lane_id();
+    for (int brick = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; brick < nbricks;
+         brick += (gridDim.x * blockDim.x) >> 5)
+        for (int k = 0; k < 3; ++k) {
+            const int n = counts[k * nbricks + brick];
+            const int *src = scratch + sstart[k * nbricks + brick];
+            int *dst = lists + offs[k * nbricks + brick];
+            for (int i = lane; i < n; i += 32) dst[i] = src[i];
+        }
 }
 
 // ------------------------------------------------------------------------------ evaluation
@@ -676,17 +718,36 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     const int trgrid = (int)std::min<long long>((nbricks + TR_WARPS - 1) / TR_WARPS,
                                                 (long long)sm_count() * 16);
+    // One walk counts the lists and writes them into per-warp scratch runs; after the scan a
+    // copy puts them in CSR order.  If a run outgrew its region the second walk (MODE 1) writes
+    // them instead, and the regions are sized up for the next solve.
+    const int nwarps = trgrid * TR_WARPS;
+    // regions of at most 512 MB in all (a longer run takes the second walk)
+    const int cap = (int)std::min<long long>(c.list_cap, (512ll << 20) / (12ll * nwarps));
+    int *scratch, *sstart, *meta;
+    {
+        AuxScope on_aux(c);
+        if ((rc = ensure(c, S_LSCRATCH, (size_t)3 * nwarps * cap, &scratch)) ||
+            (rc = ensure(c, S_LSTART, (size_t)3 * nbricks, &sstart)) ||
+            (rc = ensure(c, S_LMETA, 4, &meta)))
+            return rc;
+    }
+    unsigned long long *stats = slot_ptr<unsigned long long>(c, S_STATS);
     TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
     {
         AuxScope on_aux(c);
         TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_fork, 0));
-        k_force_lists<false><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
-            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, err, nullptr);
+        TC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(int) * 4, c.stream));
+        k_force_lists<2><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
+            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, scratch,
+            cap, sstart, meta, err, stats);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
         for (int k = 0; k < 4; ++k)
             TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 32 + k, offs + (k + 1) * nbricks, sizeof(int),
                                         cudaMemcpyDeviceToHost, c.stream));
+        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 36, meta, sizeof(int) * 2,
+                                    cudaMemcpyDeviceToHost, c.stream));
         TC_CUDA_TRY(cudaEventRecord(c.ev_totals, c.stream));
     }
     if (between && (rc = between(c))) {
@@ -696,6 +757,9 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     TC_CUDA_TRY(cudaEventSynchronize(c.ev_totals));
     int tot[4];
     for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[32 + k];
+    const bool overflow = c.h_pinned[36] != 0;
+    const int longest = (int)c.h_pinned[37];
+    if (longest > c.list_cap) c.list_cap = longest + longest / 4;   // for the next solve
     const int ntasks = tot[3] - tot[2];
     c.counts.n_e2l = tot[0];
     c.counts.n_e2p = tot[1] - tot[0];
@@ -707,9 +771,16 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     {
         AuxScope on_aux(c);
         if ((rc = ensure(c, S_E2L, (size_t)tot[2] + 1, &lists))) return rc;
-        k_force_lists<true><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
-            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, err,
-            slot_ptr<unsigned long long>(c, S_STATS));
+        if (!overflow) {
+            k_force_lists_copy<<<(int)std::min<long long>((nbricks + 7) / 8,
+                                                          (long long)sm_count() * 16),
+                                 256, 0, c.stream>>>(nbricks, counts, offs, sstart, scratch,
+                                                     lists);
+        } else {
+            k_force_lists<1><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
+                nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, nullptr,
+                0, nullptr, nullptr, err, nullptr);
+        }
         TC_KERNEL_CHECK();
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
     }

@@ -35,6 +35,7 @@ enum Slot {
     S_TNODE, S_RANGE, S_CELL, S_MASS, S_W, S_WX, S_WY, S_EXPS, S_UPCNT,
     // force traversal / lists
     S_FCOUNT, S_FOFF, S_E2L, S_E2P, S_P2P, S_BRICK_CTR, S_FPART, S_SEXP, S_SSCALE, S_TASKMAP,
+    S_LSCRATCH, S_LSTART, S_LMETA,
     // potential targets / lists
     S_TKEYS, S_TPERM, S_TKEYS2, S_TPERM2, S_PCOUNT, S_POFF, S_PE2P, S_PP2P,
     // misc
@@ -106,6 +107,7 @@ struct Context {
     int order_potential = ORDER_POTENTIAL;  // expansion orders of the next solves
     int order_force = ORDER_FORCE;
     int blocksize = BLOCKSIZE;            // MRAG block side of the force entry points
+    int list_cap = 1024;                  // per-warp scratch run of the one-walk list build
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};
