@@ -4,6 +4,7 @@
 // (drivers/treecode-potential.h:21-29, drivers/treecode-force.h:21-31).  Each calling thread
 // gets its own context (stream + grow-only device buffers), so the functions are reentrant,
 // unlike the reference whose Tree:: globals are shared (drivers/upward.cpp:51-59).
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -41,6 +42,28 @@ static void clear_error() {
 
 void phase_mark(Context &c, int idx) {
     if (c.timing) cudaEventRecord(c.ev[idx], c.stream);
+}
+
+long long scratch_layout(const Context &c, int nkinds, int nwarps, int nitems,
+                         long long max_entries, ScratchLayout &s) {
+    const long long per_warp = nwarps > 0 ? ((long long)nitems + nwarps - 1) / nwarps : 0;
+    long long total = 0;
+    for (int k = 0; k < 3; ++k) {
+        long long cap = k < nkinds ? c.list_per_item[k] * per_warp + 16 : 0;
+        if (k < nkinds && cap * nwarps * nkinds > max_entries) cap = max_entries / (nwarps * nkinds);
+        s.cap[k] = (int)cap;
+        s.koff[k] = (int)total;
+        total += cap * nwarps;
+    }
+    return total;
+}
+
+void scratch_learn(Context &c, int nkinds, int nwarps, int nitems, const unsigned *longest) {
+    const long long per_warp = nwarps > 0 ? ((long long)nitems + nwarps - 1) / nwarps : 1;
+    for (int k = 0; k < nkinds; ++k) {
+        const long long need = ((long long)longest[k] * 5 / 4 + per_warp - 1) / per_warp;
+        if (need > c.list_per_item[k]) c.list_per_item[k] = (int)std::min<long long>(need, 1 << 20);
+    }
 }
 
 // Reads back the device error word and the work counters (one sync).  The counters land in

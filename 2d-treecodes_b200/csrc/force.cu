@@ -97,17 +97,17 @@ constexpr int TR_STACK = 2048;
 // does the far field), so that the few bricks on a dense region do not serialise the kernel.
 constexpr int P2P_SEG = 2048;
 
-// MODE 0: count the lists; MODE 1: write them at the scanned offsets (CSR); MODE 2: count
-// them and write each warp's entries into its own scratch region (kind k of warp w from
-// (k W + w) cap on), recording where each brick's run starts, so that a copy into CSR order
-// replaces the second walk.  A region that fills up sets meta[0] (the host then falls back to
-// MODE 1); meta[1] receives the largest run of entries any warp wrote, for sizing the regions.
+// MODE 1: write the lists at the scanned offsets (CSR); MODE 2: count them and write each
+// warp's entries into its own scratch region (ScratchLayout), recording where each brick's run
+// starts, so that a copy into CSR order replaces a second walk.  A region that fills up sets
+// meta[0] (the host then falls back to MODE 1); meta[1 + k] receives the longest run of kind k
+// any warp wrote, for sizing the regions of the next build.
 template <int MODE>
 __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
     int nbricks, BlockLayout L, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int *__restrict__ lists,
-    int *__restrict__ scratch, int cap, int *__restrict__ sstart, int *meta,
+    int *__restrict__ scratch, ScratchLayout sl, int *__restrict__ sstart, int *meta,
     unsigned *err, unsigned long long *stats) {
     constexpr bool FILL = MODE == 1;
     __shared__ int stack_all[TR_WARPS][TR_STACK];
@@ -116,7 +116,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
     const double inv_theta = 1.0 / theta, theta2 = theta * theta;
     const unsigned lt = lanemask_lt();
     unsigned long long p2p_sources = 0;   // per lane: sources of the P2P leaves it listed
-    const int wglob = blockIdx.x * TR_WARPS + warp, nwarps = gridDim.x * TR_WARPS;
+    const int wglob = blockIdx.x * TR_WARPS + warp;
     int cur[3] = {0, 0, 0};               // MODE 2: entries this warp has written, per kind
     bool full = false;
 
@@ -169,7 +169,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                 }
                 if (MODE == 2 && kind == k) {
                     const int at = cur[k] + n[k] + __popc(bal & lt);
-                    if (at < cap) scratch[(size_t)(k * nwarps + wglob) * cap + at] = node;
+                    if (at < sl.cap[k]) scratch[sl.koff[k] + (size_t)wglob * sl.cap[k] + at] = node;
                     else full = true;
                 }
                 n[k] += __popc(bal);
@@ -198,7 +198,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
                 counts[3 * nbricks + brick] = max(1, (total + P2P_SEG - 1) / P2P_SEG);
                 if (MODE == 2)
                     for (int k = 0; k < 3; ++k)
-                        sstart[k * nbricks + brick] = (k * nwarps + wglob) * cap + cur[k];
+                        sstart[k * nbricks + brick] = sl.koff[k] + wglob * sl.cap[k] + cur[k];
             }
             if (MODE == 2)
                 for (int k = 0; k < 3; ++k) cur[k] += n[k];
@@ -207,7 +207,8 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
     }
     if (MODE == 2) {
         if (__any_sync(FULL_MASK, full) && lane == 0) atomicOr(&meta[0], 1);
-        if (lane == 0) atomicMax(&meta[1], max(cur[0], max(cur[1], cur[2])));
+        if (lane == 0)
+            for (int k = 0; k < 3; ++k) atomicMax(&meta[1 + k], cur[k]);
     }
     if (MODE != 0 && stats) {
         for (int m = 16; m; m >>= 1) p2p_sources += __shfl_xor_sync(FULL_MASK, p2p_sources, m);
@@ -722,12 +723,12 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     // copy puts them in CSR order.  If a run outgrew its region the second walk (MODE 1) writes
     // them instead, and the regions are sized up for the next solve.
     const int nwarps = trgrid * TR_WARPS;
-    // regions of at most 512 MB in all (a longer run takes the second walk)
-    const int cap = (int)std::min<long long>(c.list_cap, (512ll << 20) / (12ll * nwarps));
+    ScratchLayout sl;   // at most 512 MB in all (a longer run takes the second walk)
+    const long long nscratch = scratch_layout(c, 3, nwarps, nbricks, (512ll << 20) / 4, sl);
     int *scratch, *sstart, *meta;
     {
         AuxScope on_aux(c);
-        if ((rc = ensure(c, S_LSCRATCH, (size_t)3 * nwarps * cap, &scratch)) ||
+        if ((rc = ensure(c, S_LSCRATCH, (size_t)nscratch + 1, &scratch)) ||
             (rc = ensure(c, S_LSTART, (size_t)3 * nbricks, &sstart)) ||
             (rc = ensure(c, S_LMETA, 4, &meta)))
             return rc;
@@ -740,13 +741,13 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         TC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(int) * 4, c.stream));
         k_force_lists<2><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
             nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, scratch,
-            cap, sstart, meta, err, stats);
+            sl, sstart, meta, err, stats);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
         for (int k = 0; k < 4; ++k)
             TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 32 + k, offs + (k + 1) * nbricks, sizeof(int),
                                         cudaMemcpyDeviceToHost, c.stream));
-        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 36, meta, sizeof(int) * 2,
+        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 36, meta, sizeof(int) * 4,
                                     cudaMemcpyDeviceToHost, c.stream));
         TC_CUDA_TRY(cudaEventRecord(c.ev_totals, c.stream));
     }
@@ -758,8 +759,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     int tot[4];
     for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[32 + k];
     const bool overflow = c.h_pinned[36] != 0;
-    const int longest = (int)c.h_pinned[37];
-    if (longest > c.list_cap) c.list_cap = longest + longest / 4;   // for the next solve
+    scratch_learn(c, 3, nwarps, nbricks, c.h_pinned + 37);   // for the next solve
     const int ntasks = tot[3] - tot[2];
     c.counts.n_e2l = tot[0];
     c.counts.n_e2p = tot[1] - tot[0];
@@ -779,7 +779,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         } else {
             k_force_lists<1><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
                 nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, nullptr,
-                0, nullptr, nullptr, err, nullptr);
+                sl, nullptr, nullptr, err, nullptr);
         }
         TC_KERNEL_CHECK();
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));

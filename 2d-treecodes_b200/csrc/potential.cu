@@ -40,12 +40,23 @@ constexpr int PT_SEG = 4096;
 // never holds more than PL_STACK - 160 + 96 + 45 entries.
 constexpr int PL_STACK = 512;
 
-template <bool FILL>
+// MODE 1: write the lists at the scanned offsets (CSR); MODE 2: count them and write each
+// warp's entries into its own scratch region (ScratchLayout), recording where each group's run
+// starts, so that a copy into CSR order replaces a second walk.  A region that fills up sets
+// meta[0] (the host then falls back to MODE 1); meta[1 + k] receives the longest run of kind
+// k any warp wrote.  The work counters are added by the walk that runs last over every group
+// (MODE 2, or MODE 1 when it runs).
+template <int MODE>
 __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
     int ngroups, int m, const double *__restrict__ xt, const double *__restrict__ yt,
     const int *__restrict__ tperm, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int2 *__restrict__ lists,
+    int2 *__restrict__ scratch, ScratchLayout sl, int *__restrict__ sstart, int *meta,
     unsigned *err, unsigned long long *stats) {
+    constexpr bool FILL = MODE == 1;
+    const int wglob = blockIdx.x * PT_WARPS + (threadIdx.x >> 5);
+    int cur[2] = {0, 0};   // MODE 2: entries this warp has written, per kind
+    bool full = false;
     __shared__ int2 stack_all[PT_WARPS][PL_STACK];
     __shared__ double2 targ_all[PT_WARPS][32];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
@@ -149,6 +160,22 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
                     else atomicOr(err, DEVERR_BOUNDS);
                 }
             }
+            if (MODE == 2) {
+                if (f_far) {
+                    const int at = cur[0] + n0 + __popc(bf & lt);
+                    if (at < sl.cap[0])
+                        scratch[sl.koff[0] + (size_t)wglob * sl.cap[0] + at] =
+                            make_int2(ent.x, (int)far);
+                    else full = true;
+                }
+                if (f_near) {
+                    const int at = cur[1] + n1 + __popc(bn & lt);
+                    if (at < sl.cap[1])
+                        scratch[sl.koff[1] + (size_t)wglob * sl.cap[1] + at] =
+                            make_int2(ent.x, (int)rest);
+                    else full = true;
+                }
+            }
             n0 += __popc(bf);
             n1 += __popc(bn);
             e2p_pairs += (unsigned)__reduce_add_sync(FULL_MASK, f_far ? __popc(far) : 0);
@@ -175,13 +202,46 @@ __global__ __launch_bounds__(PT_WARPS * 32) void k_potential_lists(
             counts[ngroups + g] = n1;
             // evaluation tasks: the group's near-field sources in segments of at most PT_SEG
             counts[2 * ngroups + g] = max(1, (gsrc + PT_SEG - 1) / PT_SEG);
+            if (MODE == 2) {
+                sstart[g] = sl.koff[0] + wglob * sl.cap[0] + cur[0];
+                sstart[ngroups + g] = sl.koff[1] + wglob * sl.cap[1] + cur[1];
+            }
+        }
+        if (MODE == 2) {
+            cur[0] += n0;
+            cur[1] += n1;
         }
         __syncwarp();
     }
-    if (FILL && lane == 0) {
+    if (MODE == 2) {
+        if (__any_sync(FULL_MASK, full) && lane == 0) atomicOr(&meta[0], 1);
+        if (lane == 0) {
+            atomicMax(&meta[1], cur[0]);
+            atomicMax(&meta[2], cur[1]);
+        }
+    }
+    if (stats && lane == 0) {
         if (e2p_pairs) atomicAdd(&stats[STAT_E2P_PAIRS], e2p_pairs);
         if (p2p_pairs) atomicAdd(&stats[STAT_P2P_PAIRS], p2p_pairs);
     }
+}
+
+// The lists in CSR order from the scratch runs of k_potential_lists<2>: warp per group.
+__global__ __launch_bounds__(256) void k_potential_lists_copy(int ngroups,
+                                                              const int *__restrict__ counts,
+                                                              const int *__restrict__ offs,
+                                                              const int *__restrict__ sstart,
+                                                              const int2 *__restrict__ scratch,
+                                                              int2 *__restrict__ lists) {
+    const int lane = lane_id();
+    for (int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups;
+         g += (gridDim.x * blockDim.x) >> 5)
+        for (int k = 0; k < 2; ++k) {
+            const int n = counts[k * ngroups + g];
+            const int2 *src = scratch + sstart[k * ngroups + g];
+            int2 *dst = lists + offs[k * ngroups + g];
+            for (int i = lane; i < n; i += 32) dst[i] = src[i];
+        }
 }
 
 constexpr int PE_WARPS = 4;
@@ -574,6 +634,14 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     const int grid = (int)std::min<long long>((ngroups + PT_WARPS - 1) / PT_WARPS,
                                               (long long)sm_count_p() * 16);
     int *ko, *vo;
+    // One walk counts the lists and writes them into per-warp scratch runs; after the scan a
+    // copy puts them in CSR order.  If a run outgrew its region a second walk writes them
+    // instead, and the regions are sized up for the next solve (at most 512 MB in all).
+    const int nwarps = grid * PT_WARPS;
+    ScratchLayout sl;   // at most 512 MB in all (a longer run takes the second walk)
+    const long long nscratch = scratch_layout(c, 2, nwarps, ngroups, (512ll << 20) / 8, sl);
+    int *scratch, *sstart, *meta;
+    unsigned long long *stats = slot_ptr<unsigned long long>(c, S_STATS);
     TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
     {
         AuxScope on_aux(c);
@@ -582,13 +650,21 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
         if ((rc = radix_sort_pairs(c, tkeys, nullptr, m, 2 * LMAX, tkeys2, tperm2, tkeys, tperm,
                                    &ko, &vo)))
             return rc;
-        k_potential_lists<false><<<grid, PT_WARPS * 32, 0, c.stream>>>(
-            ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, counts, nullptr, nullptr, err, nullptr);
+        if ((rc = ensure(c, S_LSCRATCH, (size_t)2 * nscratch + 2, &scratch)) ||
+            (rc = ensure(c, S_LSTART, (size_t)2 * ngroups, &sstart)) ||
+            (rc = ensure(c, S_LMETA, 4, &meta)))
+            return rc;
+        TC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(int) * 4, c.stream));
+        k_potential_lists<2><<<grid, PT_WARPS * 32, 0, c.stream>>>(
+            ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, counts, nullptr, nullptr,
+            reinterpret_cast<int2 *>(scratch), sl, sstart, meta, err, stats);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 3 * ngroups))) return rc;
         for (int k = 0; k < 3; ++k)
             TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 32 + k, offs + (k + 1) * ngroups, sizeof(int),
                                         cudaMemcpyDeviceToHost, c.stream));
+        TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 36, meta, sizeof(int) * 4,
+                                    cudaMemcpyDeviceToHost, c.stream));
         TC_CUDA_TRY(cudaEventRecord(c.ev_totals, c.stream));
     }
     if (between && (rc = between(c))) {
@@ -598,6 +674,8 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     TC_CUDA_TRY(cudaEventSynchronize(c.ev_totals));
     const int n_e2p = (int)c.h_pinned[32], total = (int)c.h_pinned[33];
     const int ntasks = (int)c.h_pinned[34] - total;
+    const bool overflow = c.h_pinned[36] != 0;
+    scratch_learn(c, 2, nwarps, ngroups, c.h_pinned + 37);   // for the next solve
     c.counts.n_e2p = n_e2p;
     c.counts.n_p2p = total - n_e2p;
     c.counts.n_e2l = 0;
@@ -607,9 +685,19 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     {
         AuxScope on_aux(c);
         if ((rc = ensure(c, S_PE2P, (size_t)total + 1, &lists))) return rc;
-        k_potential_lists<true><<<grid, PT_WARPS * 32, 0, c.stream>>>(
-            ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, nullptr, offs, lists, err,
-            slot_ptr<unsigned long long>(c, S_STATS));
+        if (!overflow) {
+            k_potential_lists_copy<<<(int)std::min<long long>((ngroups + 7) / 8,
+                                                              (long long)sm_count_p() * 16),
+                                     256, 0, c.stream>>>(ngroups, counts, offs, sstart,
+                                                         reinterpret_cast<int2 *>(scratch), lists);
+        } else {
+            // the second walk adds the work counters again: clear the first walk's
+            TC_CUDA_TRY(cudaMemsetAsync(stats + STAT_E2P_PAIRS, 0, 2 * sizeof(unsigned long long),
+                                        c.stream));
+            k_potential_lists<1><<<grid, PT_WARPS * 32, 0, c.stream>>>(
+                ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, nullptr, offs, lists, nullptr,
+                sl, nullptr, nullptr, err, stats);
+        }
         TC_KERNEL_CHECK();
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
     }

@@ -87,6 +87,21 @@ int dispatch_order(int p, F &&f) {
     }
 }
 
+// Per-warp scratch regions of a one-walk list build: kind k of warp w holds cap[k] entries from
+// koff[k] + w cap[k] on.
+struct ScratchLayout {
+    int cap[3];
+    int koff[3];
+};
+
+struct Context;
+// Regions for `nkinds` kinds, `nwarps` warps and `nitems` bricks / groups, from the context's
+// learned sizes, at most `max_entries` entries in all; returns the entries needed.
+long long scratch_layout(const Context &c, int nkinds, int nwarps, int nitems,
+                         long long max_entries, ScratchLayout &s);
+// Raises the learned sizes from a build's per-kind longest runs (meta[1..nkinds]).
+void scratch_learn(Context &c, int nkinds, int nwarps, int nitems, const unsigned *longest);
+
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -107,7 +122,9 @@ struct Context {
     int order_potential = ORDER_POTENTIAL;  // expansion orders of the next solves
     int order_force = ORDER_FORCE;
     int blocksize = BLOCKSIZE;            // MRAG block side of the force entry points
-    int list_cap = 1024;                  // per-warp scratch run of the one-walk list build
+    // one-walk list builds: entries per brick / target group and list kind that a warp's
+    // scratch region is sized for, raised after every solve to what it needed
+    int list_per_item[3] = {32, 32, 32};
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};
