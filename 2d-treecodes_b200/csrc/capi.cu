@@ -575,6 +575,7 @@ TC_API int tc_get_stats(tc_context *ctx, tc_stats *out) {
     out->l2p_targets = c.counts.l2p_targets;
     out->launches = c.counts.launches;
     out->eval_kernel_ms = c.times.eval_kernel_ms;
+    out->list_walks = c.list_walks;
     return TC_OK;
 }
 

@@ -759,6 +759,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     int tot[4];
     for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[32 + k];
     const bool overflow = c.h_pinned[36] != 0;
+    c.list_walks = overflow ? 2 : 1;
     scratch_learn(c, 3, nwarps, nbricks, c.h_pinned + 37);   // for the next solve
     const int ntasks = tot[3] - tot[2];
     c.counts.n_e2l = tot[0];

@@ -675,6 +675,7 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     const int n_e2p = (int)c.h_pinned[32], total = (int)c.h_pinned[33];
     const int ntasks = (int)c.h_pinned[34] - total;
     const bool overflow = c.h_pinned[36] != 0;
+    c.list_walks = overflow ? 2 : 1;
     scratch_learn(c, 2, nwarps, ngroups, c.h_pinned + 37);   // for the next solve
     c.counts.n_e2p = n_e2p;
     c.counts.n_p2p = total - n_e2p;

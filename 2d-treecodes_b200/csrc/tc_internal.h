@@ -125,6 +125,7 @@ struct Context {
     // one-walk list builds: entries per brick / target group and list kind that a warp's
     // scratch region is sized for, raised after every solve to what it needed
     int list_per_item[3] = {32, 32, 32};
+    int list_walks = 0;                   // walks the last list build took (1 or 2)
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};

@@ -90,6 +90,8 @@ typedef struct {
     long long l2p_targets;           /* targets evaluated from local expansions */
     long long launches;              /* kernels launched by the last solve */
     float eval_kernel_ms;            /* the evaluation kernel alone (timing enabled) */
+    int list_walks;                  /* tree walks that built the lists: 1, or 2 when the
+                                        one-walk build outgrew its scratch (which then grows) */
 } tc_stats;
 
 /* device < 0 selects the current device; stream may be NULL (the context creates one). */
