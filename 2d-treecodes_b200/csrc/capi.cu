@@ -19,6 +19,7 @@ namespace tc {
 
 int direct_potential(Context &c, const double *xs, const double *ys, const double *vs, int n,
                      const double *xt, const double *yt, int m, double *out);
+int log_probe(Context &c, const double *x, int n, double *out);
 int direct_force(Context &c, const double *xs, const double *ys, const double *vs, int n,
                  const double *xt, const double *yt, int m, double *xo, double *yo);
 int measure_fma_peak(int fp64, double *tflops);
@@ -698,6 +699,14 @@ TC_API int tc_direct_potential_device(tc_context *ctx, const double *xs, const d
                                       const double *yt, int m, double *out) {
     CTX_GUARD();
     int rc = direct_potential(ctx->c, xs, ys, vs, n, xt, yt, m, out);
+    if (rc) return rc;
+    TC_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+    return TC_OK;
+}
+
+TC_API int tc_log_probe_device(tc_context *ctx, const double *x, int n, double *out) {
+    CTX_GUARD();
+    int rc = log_probe(ctx->c, x, n, out);
     if (rc) return rc;
     TC_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
     return TC_OK;

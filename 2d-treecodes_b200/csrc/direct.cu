@@ -1,9 +1,11 @@
 // direct.cu -- O(N M) FP64 direct sums on the GPU (accuracy reference at sizes where the CPU
 // direct sum of main.cpp:201-245 would take minutes) and an FMA-throughput probe used as the
 // FP64 / FP32 pipe peak of the roofline.
+#include <algorithm>
 #include <cfloat>
 
 #include "tc_internal.h"
+#include "tc_math.cuh"
 
 namespace tc {
 
@@ -82,6 +84,22 @@ int direct_force(Context &c, const double *xs, const double *ys, const double *v
     if (m == 0) return TC_OK;
     k_direct_force<<<(m + DS_THREADS - 1) / DS_THREADS, DS_THREADS, 0, c.stream>>>(
         xs, ys, vs, n, xt, yt, m, xo, yo);
+    TC_KERNEL_CHECK();
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------- log probe
+// out[2i] = log_pos(x[i]) (the potential kernels' logarithm), out[2i + 1] = the library log.
+__global__ void k_log_probe(const double *__restrict__ x, int n, double *__restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        out[2 * i] = log_pos(x[i]);
+        out[2 * i + 1] = log(x[i]);
+    }
+}
+
+int log_probe(Context &c, const double *x, int n, double *out) {
+    if (n <= 0) return TC_OK;
+    k_log_probe<<<(int)std::min<long long>((n + 255) / 256, 148 * 8), 256, 0, c.stream>>>(x, n, out);
     TC_KERNEL_CHECK();
     return TC_OK;
 }

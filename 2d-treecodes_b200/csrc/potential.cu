@@ -376,14 +376,14 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                                             fmaf(q.x, ui, fmaf(q.y, ur, d.y)));
                         }
                         two_sum_add(sh, sl, ur * q.x - ui * q.y);
-                        far += mm * log(r2) * 0.5;
+                        far += mm * log_pos(r2) * 0.5;
                     } else {
                         const double inv = 1.0 / r2;
                         const cplx u = {rz * inv, -iz * inv};
                         cplx q = s_coef[warp][P - 1];
 #pragma unroll
                         for (int k = P - 2; k >= 0; --k) q = cfma(q, u, s_coef[warp][k]);
-                        far += mm * log(r2) * 0.5 + (u.re * q.re - u.im * q.im);
+                        far += mm * log_pos(r2) * 0.5 + (u.re * q.re - u.im * q.im);
                     }
                 }
             }
@@ -507,7 +507,7 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                             for (int q = 0; q < cnt; ++q) {
                                 const double2 sp = s_xy[warp][q];
                                 const double xr = x - sp.x, yr = y - sp.y;
-                                near += log(xr * xr + yr * yr + eps) * s_v[warp][q];
+                                near += log_pos(xr * xr + yr * yr + eps) * s_v[warp][q];
                             }
                         }
                     }
@@ -540,7 +540,7 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                             for (int q = lane / k; q < cnt; q += r) {
                                 const double2 sp = s_xy[warp][q];
                                 const double xr = qx - sp.x, yr = qy - sp.y;
-                                part += log(xr * xr + yr * yr + eps) * s_v[warp][q];
+                                part += log_pos(xr * xr + yr * yr + eps) * s_v[warp][q];
                             }
                     }
                     s_part[warp][lane] = part;

@@ -22,6 +22,44 @@ constexpr BinomTable make_binom_table() {
     return t;
 }
 
+// Natural logarithm of a positive normal double, for the potential kernels' log r^2 terms
+// (arguments r^2 + 10 eps or |z|^2 of a far cell, never zero, subnormal or infinite).  From the
+// mathematics: x = 2^e m with m in [sqrt(1/2), sqrt(2)), s = (m - 1) / (m + 1), and
+// log m = 2 atanh s = 2 s (1 + s^2/3 + s^4/5 + ... + s^20/21), the atanh series cut where
+// |s| <= 0.1716 leaves a remainder below 2^-55 of it; log x = e ln 2 + log m, with ln 2 split
+// into a head of 21 bits (e * head exact) and a tail.  The division is a refined reciprocal
+// (rcp_nr).  About 30 instructions against the library log's ~100; within a few ulp of it
+// (tests/test_gpu_parity.py checks the bound on 2^20 arguments).
+__device__ __forceinline__ double log_pos(double x) {
+    const int lo = __double2loint(x);
+    int hi = __double2hiint(x);
+    int e = (hi >> 20) - 1023;
+    int mh = (hi & 0x000fffff) | 0x3ff00000;   // m in [1, 2)
+    if (mh > 0x3ff6a09e) {                     // m above sqrt(2) (to 20 bits): halve it
+        mh -= 0x00100000;
+        ++e;
+    }
+    const double m = __hiloint2double(mh, lo);
+    const double f = m - 1.0;
+    const double s = f * rcp_nr(2.0 + f);
+    const double z = s * s;
+    double q = 1.0 / 21.0;
+    q = fma(q, z, 1.0 / 19.0);
+    q = fma(q, z, 1.0 / 17.0);
+    q = fma(q, z, 1.0 / 15.0);
+    q = fma(q, z, 1.0 / 13.0);
+    q = fma(q, z, 1.0 / 11.0);
+    q = fma(q, z, 1.0 / 9.0);
+    q = fma(q, z, 1.0 / 7.0);
+    q = fma(q, z, 1.0 / 5.0);
+    q = fma(q, z, 1.0 / 3.0);
+    const double two_s = 2.0 * s;
+    const double logm = fma(two_s * z, q, two_s);
+    constexpr double LN2_HEAD = 0x1.62e42p-1, LN2_TAIL = 0x1.fdf473de6af28p-22;
+    const double de = (double)e;
+    return fma(de, LN2_HEAD, fma(de, LN2_TAIL, logm));
+}
+
 struct cplx {
     double re, im;
 };

@@ -43,6 +43,7 @@ SIGNATURES = {
     "tc_set_orders": (_i, [_vp, _i, _i]),
     "tc_supported_orders": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
     "tc_set_blocksize": (_i, [_vp, _i]),
+    "tc_log_probe_device": (_i, [_vp, _vp, _i, _vp]),
     "tc_set_timing": (_i, [_vp, _i]),
     "tc_get_stats": (_i, [_vp, _vp]),
     "tc_get_stream": (_vp, [_vp]),
@@ -297,6 +298,11 @@ class Context:
                                                int(xs.numel()), _ptr(xt), _ptr(yt),
                                                int(xt.numel()), _ptr(xo), _ptr(yo)))
         return xo, yo
+
+    def log_probe_device(self, x, out):
+        """out[2i] = the potential kernels' log of x[i], out[2i + 1] = the library log."""
+        _check(self.lib.tc_log_probe_device(self.h, _ptr(x), int(x.numel()), _ptr(out)))
+        return out
 
     # ---- tree inspection
     def tree(self, kind, xs, ys, vs):

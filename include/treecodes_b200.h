@@ -159,6 +159,9 @@ TC_API int tc_direct_force_device(tc_context *ctx, const double *xsources,
                                   const double *ysources, const double *sourcevalues,
                                   int nsources, const double *xtargets, const double *ytargets,
                                   int ntargets, double *xout, double *yout);
+/* Diagnostic: out[2i] = the logarithm the potential kernels use (a positive normal x only),
+ * out[2i + 1] = the CUDA library's log, both on the device (device pointers, n values). */
+TC_API int tc_log_probe_device(tc_context *ctx, const double *x, int n, double *out);
 
 /* Allocation-free source sort.  No counterpart in the reference.
  *

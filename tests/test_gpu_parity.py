@@ -227,3 +227,25 @@ def test_gpu_direct_sum_matches_cpu_direct_sum(gpu_ctx):
     gp = dev_empty(64)
     gpu_ctx.direct_potential_device(dev(w["xs"]), dev(w["ys"]), dev(w["vs"]), dev(xt), dev(yt), gp)
     assert rel_l2(host(gp), cp) < 1e-12
+
+
+def test_potential_log_within_a_few_ulp_of_the_library(gpu_ctx):
+    """The potential kernels' own logarithm (log_pos: atanh series on the reduced mantissa)
+    against CUDA's log on 2^20 arguments spanning the range the kernels feed it (r^2 + 10 eps
+    from ~2e-15 up, far-cell |z|^2), plus arguments next to 1, to powers of two and to the
+    sqrt(2) split of the reduction."""
+    r = np.random.default_rng(5)
+    x = np.exp(r.uniform(np.log(2e-15), np.log(1e6), 1 << 20))
+    edges = []
+    for b in [1.0, 2.0, 0.5, 2.0 ** -40, 2.0 ** 19, np.sqrt(2.0), np.sqrt(0.5)]:
+        edges += [b, np.nextafter(b, 0), np.nextafter(b, 4 * b)]
+        edges += list(b * (1 + np.linspace(-1e-6, 1e-6, 101)))
+    x = np.r_[x, np.array(edges)]
+    xd = dev(x)
+    out = dev_empty(2 * len(x))
+    gpu_ctx.log_probe_device(xd, out)
+    o = host(out).reshape(-1, 2)
+    mine, lib = o[:, 0], o[:, 1]
+    ulp = np.spacing(np.abs(lib))
+    err = np.abs(mine - lib)
+    assert np.all(err <= 4 * ulp), (err / ulp).max()
