@@ -5,10 +5,12 @@
 // gets its own context (stream + grow-only device buffers), so the functions are reentrant,
 // unlike the reference whose Tree:: globals are shared (drivers/upward.cpp:51-59).
 #include <algorithm>
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "treecodes_b200.h"
 #include <initializer_list>
@@ -48,6 +50,7 @@ void phase_mark(Context &c, int idx) {
 long long scratch_layout(const Context &c, int nkinds, int nwarps, int nitems,
                          long long max_entries, ScratchLayout &s) {
     const long long per_warp = nwarps > 0 ? ((long long)nitems + nwarps - 1) / nwarps : 0;
+    max_entries = std::min<long long>(max_entries, INT_MAX / 2);   // offsets stay ints
     long long total = 0;
     for (int k = 0; k < 3; ++k) {
         long long cap = k < nkinds ? c.list_per_item[k] * per_warp + 16 : 0;
@@ -57,6 +60,35 @@ long long scratch_layout(const Context &c, int nkinds, int nwarps, int nitems,
         total += cap * nwarps;
     }
     return total;
+}
+
+ListScratch::~ListScratch() {
+    if (owned && p) cudaFreeAsync(p, stream);
+}
+
+int list_scratch(Context &c, int nkinds, int nwarps, int nitems, size_t entry_bytes,
+                 ScratchLayout &sl, ListScratch &out) {
+    const long long per_warp = nwarps > 0 ? ((long long)nitems + nwarps - 1) / nwarps : 0;
+    long long need = 0;
+    for (int k = 0; k < nkinds; ++k) need += (c.list_per_item[k] * per_warp + 16) * nwarps;
+    const long long have = (long long)(c.buf[S_REC].bytes / entry_bytes);
+    if (need <= std::min<long long>(have, INT_MAX / 2)) {
+        scratch_layout(c, nkinds, nwarps, nitems, have, sl);
+        out.p = c.buf[S_REC].p;
+        return TC_OK;
+    }
+    const long long n = scratch_layout(c, nkinds, nwarps, nitems,
+                                       (512ll << 20) / (long long)entry_bytes, sl);
+    const cudaError_t e = cudaMallocAsync(&out.p, (size_t)n * entry_bytes + 16, c.stream);
+    if (e != cudaSuccess) {
+        out.p = nullptr;
+        set_error(TC_ERR_ALLOC, "cudaMallocAsync(%lld bytes) for the list scratch failed: %s",
+                  n * (long long)entry_bytes, cudaGetErrorString(e));
+        return TC_ERR_ALLOC;
+    }
+    out.owned = true;
+    out.stream = c.stream;
+    return TC_OK;
 }
 
 void scratch_learn(Context &c, int nkinds, int nwarps, int nitems, const unsigned *longest) {
@@ -109,6 +141,32 @@ int device_sm_count() {
     return sms;
 }
 
+// The contexts' small page-locked read-back areas (4 KB each) come from slabs allocated once
+// per process and recycled: cudaMallocHost per context cost a synchronising call on every
+// context creation, which stalled the other contexts' work whenever a serving client arrived.
+constexpr size_t PINNED_AREA = 4096, PINNED_SLAB = 64 * PINNED_AREA;
+static std::mutex g_pinned_mu;
+static std::vector<unsigned *> g_pinned_free;
+
+static unsigned *pinned_area() {
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    if (g_pinned_free.empty()) {
+        void *slab = nullptr;
+        if (cudaMallocHost(&slab, PINNED_SLAB) != cudaSuccess) return nullptr;
+        for (size_t o = 0; o < PINNED_SLAB; o += PINNED_AREA)
+            g_pinned_free.push_back(reinterpret_cast<unsigned *>(static_cast<char *>(slab) + o));
+    }
+    unsigned *a = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    return a;
+}
+
+static void pinned_release(unsigned *a) {
+    if (!a) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(a);
+}
+
 static int context_init(Context &c, int device, cudaStream_t stream) {
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -142,7 +200,11 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_totals, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_inputs, cudaEventDisableTiming));
-    TC_CUDA_TRY(cudaMallocHost(&c.h_pinned, 4096));
+    c.h_pinned = pinned_area();
+    if (!c.h_pinned) {
+        set_error(TC_ERR_ALLOC, "page-locked host allocation failed");
+        return TC_ERR_ALLOC;
+    }
     for (auto &ev : c.ev) TC_CUDA_TRY(cudaEventCreate(&ev));
     unsigned *err;
     unsigned long long *stats;
@@ -164,15 +226,20 @@ static void context_free(Context &c) {
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     if (c.aux) cudaStreamSynchronize(c.aux);
+    // stream-ordered frees (cudaFree would synchronise the whole device), then the pool's
+    // unused blocks back to the driver
+    cudaStream_t fs = c.stream ? c.stream : c.aux;
     for (auto &b : c.buf)
-        if (b.p) cudaFree(b.p);
+        if (b.p) cudaFreeAsync(b.p, fs);
+    if (fs) cudaStreamSynchronize(fs);
     release_pool_cache(c.device);
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs})
         if (ev) cudaEventDestroy(ev);
     if (c.aux) cudaStreamDestroy(c.aux);
-    if (c.h_pinned) cudaFreeHost(c.h_pinned);
+    pinned_release(c.h_pinned);
+    c.h_pinned = nullptr;
     if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
 }
 
@@ -545,10 +612,11 @@ TC_API int tc_context_trim(tc_context *ctx) {
     for (int s = 0; s < S_NUM_SLOTS; ++s) {
         if (s == S_ERR || s == S_STATS) continue;   // created with the context, tiny
         DevBuf &b = c.buf[s];
-        if (b.p) cudaFree(b.p);
+        if (b.p) cudaFreeAsync(b.p, c.stream);   // no device-wide synchronisation
         b.p = nullptr;
         b.bytes = 0;
     }
+    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
     release_pool_cache(c.device);
     c.nnodes = c.nsrc = 0;
     return TC_OK;

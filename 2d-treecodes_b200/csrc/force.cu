@@ -721,14 +721,15 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                                 (long long)sm_count() * 16);
     // One walk counts the lists and writes them into per-warp scratch runs; after the scan a
     // copy puts them in CSR order.  If a run outgrew its region the second walk (MODE 1) writes
-    // them instead, and the regions are sized up for the next solve.
+    // them instead, and the regions are sized up for the next solve.  The runs live in the
+    // sort's record buffer when they fit in it, else in a block held only for the build.
     const int nwarps = trgrid * TR_WARPS;
-    ScratchLayout sl;   // at most 512 MB in all (a longer run takes the second walk)
-    const long long nscratch = scratch_layout(c, 3, nwarps, nbricks, (512ll << 20) / 4, sl);
-    int *scratch, *sstart, *meta;
+    ScratchLayout sl;
+    ListScratch ls;   // released (when transient) after the copy, in stream order
+    int *sstart, *meta;
     {
         AuxScope on_aux(c);
-        if ((rc = ensure(c, S_LSCRATCH, (size_t)nscratch + 1, &scratch)) ||
+        if ((rc = list_scratch(c, 3, nwarps, nbricks, sizeof(int), sl, ls)) ||
             (rc = ensure(c, S_LSTART, (size_t)3 * nbricks, &sstart)) ||
             (rc = ensure(c, S_LMETA, 4, &meta)))
             return rc;
@@ -740,8 +741,8 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_fork, 0));
         TC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(int) * 4, c.stream));
         k_force_lists<2><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
-            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr, scratch,
-            sl, sstart, meta, err, stats);
+            nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr,
+            static_cast<int *>(ls.p), sl, sstart, meta, err, stats);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
         for (int k = 0; k < 4; ++k)
@@ -775,8 +776,8 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         if (!overflow) {
             k_force_lists_copy<<<(int)std::min<long long>((nbricks + 7) / 8,
                                                           (long long)sm_count() * 16),
-                                 256, 0, c.stream>>>(nbricks, counts, offs, sstart, scratch,
-                                                     lists);
+                                 256, 0, c.stream>>>(nbricks, counts, offs, sstart,
+                                                     static_cast<const int *>(ls.p), lists);
         } else {
             k_force_lists<1><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
                 nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, nullptr,

@@ -636,11 +636,12 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
     int *ko, *vo;
     // One walk counts the lists and writes them into per-warp scratch runs; after the scan a
     // copy puts them in CSR order.  If a run outgrew its region a second walk writes them
-    // instead, and the regions are sized up for the next solve (at most 512 MB in all).
+    // instead, and the regions are sized up for the next solve.  The runs live in the sort's
+    // record buffer when they fit in it, else in a block held only for the build.
     const int nwarps = grid * PT_WARPS;
-    ScratchLayout sl;   // at most 512 MB in all (a longer run takes the second walk)
-    const long long nscratch = scratch_layout(c, 2, nwarps, ngroups, (512ll << 20) / 8, sl);
-    int *scratch, *sstart, *meta;
+    ScratchLayout sl;
+    ListScratch ls;   // released (when transient) after the copy, in stream order
+    int *sstart, *meta;
     unsigned long long *stats = slot_ptr<unsigned long long>(c, S_STATS);
     TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
     {
@@ -650,14 +651,14 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
         if ((rc = radix_sort_pairs(c, tkeys, nullptr, m, 2 * LMAX, tkeys2, tperm2, tkeys, tperm,
                                    &ko, &vo)))
             return rc;
-        if ((rc = ensure(c, S_LSCRATCH, (size_t)2 * nscratch + 2, &scratch)) ||
+        if ((rc = list_scratch(c, 2, nwarps, ngroups, sizeof(int2), sl, ls)) ||
             (rc = ensure(c, S_LSTART, (size_t)2 * ngroups, &sstart)) ||
             (rc = ensure(c, S_LMETA, 4, &meta)))
             return rc;
         TC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(int) * 4, c.stream));
         k_potential_lists<2><<<grid, PT_WARPS * 32, 0, c.stream>>>(
             ngroups, m, xt, yt, vo, theta, tnode, c.nnodes, counts, nullptr, nullptr,
-            reinterpret_cast<int2 *>(scratch), sl, sstart, meta, err, stats);
+            static_cast<int2 *>(ls.p), sl, sstart, meta, err, stats);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 3 * ngroups))) return rc;
         for (int k = 0; k < 3; ++k)
@@ -690,7 +691,7 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
             k_potential_lists_copy<<<(int)std::min<long long>((ngroups + 7) / 8,
                                                               (long long)sm_count_p() * 16),
                                      256, 0, c.stream>>>(ngroups, counts, offs, sstart,
-                                                         reinterpret_cast<int2 *>(scratch), lists);
+                                                         static_cast<const int2 *>(ls.p), lists);
         } else {
             // the second walk adds the work counters again: clear the first walk's
             TC_CUDA_TRY(cudaMemsetAsync(stats + STAT_E2P_PAIRS, 0, 2 * sizeof(unsigned long long),

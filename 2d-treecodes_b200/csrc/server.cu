@@ -112,7 +112,8 @@ size_t footprint_estimate(int kind, long long n, long long ntargets, long long n
         b += (size_t)m * 16 + (size_t)m * 64;   // outputs + per-brick lists and partial sums
     } else {
         // staged targets, output, target sort, partials and the per-group lists, whose far
-        // part grows as 1/theta^2 (about 14 entries per target at theta = 0.3)
+        // part grows as 1/theta^2 (about 14 entries per target at theta = 0.3); the list
+        // build's scratch, held only while the lists are built, is not charged
         b += (size_t)ntargets * 210;
     }
     return b + (4u << 20);

@@ -35,7 +35,7 @@ enum Slot {
     S_TNODE, S_RANGE, S_CELL, S_MASS, S_W, S_WX, S_WY, S_EXPS, S_UPCNT,
     // force traversal / lists
     S_FCOUNT, S_FOFF, S_E2L, S_E2P, S_P2P, S_BRICK_CTR, S_FPART, S_SEXP, S_SSCALE, S_TASKMAP,
-    S_LSCRATCH, S_LSTART, S_LMETA,
+    S_LSTART, S_LMETA,
     // potential targets / lists
     S_TKEYS, S_TPERM, S_TKEYS2, S_TPERM2, S_PCOUNT, S_POFF, S_PE2P, S_PP2P,
     // misc
@@ -96,9 +96,22 @@ struct ScratchLayout {
 
 struct Context;
 // Regions for `nkinds` kinds, `nwarps` warps and `nitems` bricks / groups, from the context's
-// learned sizes, at most `max_entries` entries in all; returns the entries needed.
+// learned sizes, at most `max_entries` entries in all (smaller regions when they do not fit);
+// returns the entries used.
 long long scratch_layout(const Context &c, int nkinds, int nwarps, int nitems,
                          long long max_entries, ScratchLayout &s);
+// Scratch of a one-walk list build: the sort's record buffer (32 B per source, dead once the
+// sources are gathered) when the regions fit in it, else a transient block from the device's
+// pool (at most 512 MB), allocated on the context's current stream and released on it, in
+// stream order, when the guard goes out of scope after the last use has been enqueued.
+struct ListScratch {
+    void *p = nullptr;
+    bool owned = false;
+    cudaStream_t stream = nullptr;
+    ~ListScratch();
+};
+int list_scratch(Context &c, int nkinds, int nwarps, int nitems, size_t entry_bytes,
+                 ScratchLayout &sl, ListScratch &out);
 // Raises the learned sizes from a build's per-kind longest runs (meta[1..nkinds]).
 void scratch_learn(Context &c, int nkinds, int nwarps, int nitems, const unsigned *longest);
 
