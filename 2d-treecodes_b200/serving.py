@@ -113,12 +113,14 @@ class Materialiser:
         if spec["followup"] and spec["client"] in self.state:
             xs, ys, vs = self.state[spec["client"]]
             o = spec["noise_off"] % (len(self.noise) - 2 * n)
-            xs = xs + 1e-3 * self.noise[o:o + n]
-            ys = ys + 1e-3 * self.noise[o + n:o + 2 * n]
+            # advected sources in page-locked memory (torch's caching host allocator recycles
+            # the blocks), so that the server's copies of them are direct DMA
+            xs = np.add(xs, 1e-3 * self.noise[o:o + n], out=pinned_empty(n))
+            ys = np.add(ys, 1e-3 * self.noise[o + n:o + 2 * n], out=pinned_empty(n))
         else:
             sl = slice(spec["off"], spec["off"] + n)
             xs, ys = xm[sl], ym[sl]            # read-only views of the master set
-            vs = vm[sl] / n if scaled else vm[sl]
+            vs = np.divide(vm[sl], n, out=pinned_empty(n)) if scaled else vm[sl]
         if spec["resident"]:
             if spec["step"] >= spec["last_step"]:
                 self.state.pop(spec["client"], None)
