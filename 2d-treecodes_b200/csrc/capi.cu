@@ -200,6 +200,7 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_totals, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_inputs, cudaEventDisableTiming));
+    for (auto &ev : c.ev_chunk) TC_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     c.h_pinned = pinned_area();
     if (!c.h_pinned) {
         set_error(TC_ERR_ALLOC, "page-locked host allocation failed");
@@ -236,6 +237,8 @@ static void context_free(Context &c) {
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs})
+        if (ev) cudaEventDestroy(ev);
+    for (auto &ev : c.ev_chunk)
         if (ev) cudaEventDestroy(ev);
     if (c.aux) cudaStreamDestroy(c.aux);
     pinned_release(c.h_pinned);
@@ -327,7 +330,9 @@ static int potential_device(Context &c, double theta, const double *xs, const do
 static int force_device(Context &c, double theta, const double *xs, const double *ys,
                         const double *vs, int n, const double *x0s, const double *y0s,
                         const double *hs, int nb, double *xo, double *yo,
-                        cudaEvent_t values_ready = nullptr) {
+                        cudaEvent_t values_ready = nullptr, double *host_x = nullptr,
+                        double *host_y = nullptr) {
+    c.host_copied = false;
     if (n < 0 || nb < 0) {
         set_error(TC_ERR_INVALID, "negative size (nsources %d, nblocks %d)", n, nb);
         return TC_ERR_INVALID;
@@ -347,7 +352,9 @@ static int force_device(Context &c, double theta, const double *xs, const double
     int rc;
     phase_mark(c, 0);
     if ((rc = build_tree_moments(c, 1, xs, ys, vs, n, values_ready))) return rc;
-    if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo, expansions_then_mark))) return rc;
+    if ((rc = force_mrag(c, theta, x0s, y0s, hs, nb, xo, yo, expansions_then_mark, host_x,
+                         host_y)))
+        return rc;
     phase_mark(c, 5);
     if ((rc = check_device_errors(c, "treecode_force_mrag"))) return rc;
     c.counts.p2p_pairs = (long long)stat_counter(c, STAT_P2P_SOURCES) * TILE * TILE;
@@ -439,12 +446,15 @@ static int force_host(Context &c, double theta, const double *xs, const double *
                           {{S_VIN, vs, (size_t)n, &dv}})) ||
         (rc = ensure(c, S_OUTX, nt, &dox)) || (rc = ensure(c, S_OUTY, nt, &doy)))
         return rc;
-    rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy, c.ev_inputs);
+    // the outputs come back run by run while later runs are evaluated (force_mrag)
+    rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy, c.ev_inputs, xo, yo);
     const cudaError_t e = cudaStreamSynchronize(c.aux);
     if (rc) return rc;
     TC_CUDA_TRY(e);
-    TC_CUDA_TRY(cudaMemcpyAsync(xo, dox, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaMemcpyAsync(yo, doy, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
+    if (!c.host_copied) {
+        TC_CUDA_TRY(cudaMemcpyAsync(xo, dox, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
+        TC_CUDA_TRY(cudaMemcpyAsync(yo, doy, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
+    }
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
     return TC_OK;
 }

@@ -96,6 +96,8 @@ constexpr int TR_STACK = 2048;
 // A brick's evaluation is split into tasks of at most P2P_SEG near-field sources (task 0 also
 // does the far field), so that the few bricks on a dense region do not serialise the kernel.
 constexpr int P2P_SEG = 2048;
+// Runs of blocks whose outputs are copied to the host while the next run is evaluated.
+constexpr int FORCE_CHUNKS = 4;
 
 // MODE 1: write the lists at the scanned offsets (CSR); MODE 2: count them and write each
 // warp's entries into its own scratch region (ScratchLayout), recording where each brick's run
@@ -286,7 +288,8 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     const int2 *__restrict__ range, const double *__restrict__ xs,
     const double *__restrict__ ys, const double *__restrict__ vs,
     const int *__restrict__ offs, const int *__restrict__ lists, double *__restrict__ xout,
-    double *__restrict__ yout, double *__restrict__ partial, int *task_ctr,
+    double *__restrict__ yout, double *__restrict__ partial, int brick_lo, int brick_hi,
+    int *task_ctr,
     const float2 *__restrict__ sexp, const float *__restrict__ sscale,
     const int *__restrict__ task_brick) {
     const BlockLayout L = LBS ? BlockLayout{LBS, LBS - 3} : L_arg;
@@ -309,14 +312,15 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
     // evaluates its far field and the first P2P_SEG near-field sources, task p > 0 the p-th
     // segment.  Costs vary by orders of magnitude between bricks, so warps take tasks one at a
     // time from a global counter.
+    // This launch evaluates the tasks of bricks [brick_lo, brick_hi).
     const int *toff = offs + 3 * nbricks;
     const int tbase = toff[0];
-    const int ntasks = toff[nbricks] - tbase;
+    const int task_lo = toff[brick_lo] - tbase, task_hi = toff[brick_hi] - tbase;
     for (;;) {
         int task = 0;
-        if (lane == 0) task = atomicAdd(task_ctr, 1);
+        if (lane == 0) task = task_lo + atomicAdd(task_ctr, 1);
         task = __shfl_sync(FULL_MASK, task, 0);
-        if (task >= ntasks) break;
+        if (task >= task_hi) break;
         const int brick = task_brick[task];
         const int part = task - (toff[brick] - tbase);
         const int nparts = toff[brick + 1] - toff[brick];
@@ -667,13 +671,14 @@ __global__ void k_scale_coeffs(int nnodes, const TNode *__restrict__ tnode,
 }
 
 // Sum of the parts of every multi-task brick, in task order (deterministic).
-__global__ void k_force_gather_parts(int nbricks, BlockLayout L, const int *__restrict__ offs,
+__global__ void k_force_gather_parts(int nbricks, int brick_lo, int brick_hi, BlockLayout L,
+                                     const int *__restrict__ offs,
                                      const double *__restrict__ partial, double *__restrict__ xout,
                                      double *__restrict__ yout) {
     const int lane = lane_id();
     const int *toff = offs + 3 * nbricks;
     const int tbase = toff[0];
-    for (int brick = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; brick < nbricks;
+    for (int brick = brick_lo + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); brick < brick_hi;
          brick += (gridDim.x * blockDim.x) >> 5) {
         const int t0 = toff[brick] - tbase, np = toff[brick + 1] - toff[brick];
         if (np <= 1) continue;
@@ -703,7 +708,8 @@ static int sm_count() { return device_sm_count(); }
 // work, which the traversal does not read) runs on the main stream meanwhile, and the
 // evaluation waits for both.
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
-               int nblocks, double *xout, double *yout, OverlapFn between) {
+               int nblocks, double *xout, double *yout, OverlapFn between, double *host_x,
+               double *host_y) {
     BlockLayout L = {0, 0};
     while ((1 << L.lbs) < c.blocksize) ++L.lbs;   // 8, 16, 32 or 64 (tc_set_blocksize)
     L.lbps = L.lbs - 3;
@@ -794,7 +800,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)) ||
         (rc = ensure(c, S_TASKMAP, (size_t)ntasks, &task_brick)))
         return rc;
-    TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, sizeof(int), c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, 4 * sizeof(int), c.stream));
     k_task_map<<<(int)std::min<long long>((nbricks + 255) / 256, (long long)sm_count() * 8), 256, 0,
                  c.stream>>>(nbricks, offs, task_brick);
     TC_KERNEL_CHECK();
@@ -823,22 +829,49 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                               : blocks_per_sm<k_force_eval<P, false, LBS32>>(EV_WARPS * 32, 0);
         const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
                                                     (long long)sm_count() * occ);
+        // With host outputs of 2^21 targets or more (a copy of >= 32 MB, ~0.6 ms over PCIe) the
+        // blocks are evaluated in FORCE_CHUNKS runs, each copied to the host on the auxiliary
+        // stream while the next one is evaluated; below that the runs' tails cost more than
+        // the overlap gains (measured: 16M sheet e2e 11.07 -> 10.67 ms, 1M vortex 2.01 ->
+        // 2.27 ms if split).
+        const size_t per_block = (size_t)1 << (2 * L.lbs);
+        const int nchunks =
+            host_x && (size_t)nblocks * per_block >= ((size_t)1 << 21) && nblocks >= FORCE_CHUNKS
+                ? FORCE_CHUNKS
+                : 1;
         phase_mark(c, 6);
-        eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
-            nbricks, L, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS), slot_ptr<double>(c, S_EXPS),
-            slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
-            slot_ptr<double>(c, S_VS), offs, lists, xout, yout, partial, brick_ctr, sexp, sscale,
-            task_brick);
-        TC_KERNEL_CHECK();
+        for (int k = 0; k < nchunks; ++k) {
+            const int blk0 = (int)((long long)nblocks * k / nchunks);
+            const int blk1 = (int)((long long)nblocks * (k + 1) / nchunks);
+            const int b0 = blk0 << (2 * L.lbps), b1 = blk1 << (2 * L.lbps);
+            eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
+                nbricks, L, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS),
+                slot_ptr<double>(c, S_EXPS), slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS),
+                slot_ptr<double>(c, S_YS), slot_ptr<double>(c, S_VS), offs, lists, xout, yout,
+                partial, b0, b1, brick_ctr + k, sexp, sscale, task_brick);
+            TC_KERNEL_CHECK();
+            if (k == nchunks - 1) phase_mark(c, 7);
+            if (ntasks > nbricks) {
+                k_force_gather_parts<<<(int)std::min<long long>((b1 - b0 + 7) / 8,
+                                                                (long long)sm_count() * 16),
+                                       256, 0, c.stream>>>(nbricks, b0, b1, L, offs, partial,
+                                                           xout, yout);
+                TC_KERNEL_CHECK();
+            }
+            if (nchunks > 1) {
+                const size_t o = blk0 * per_block, cnt = (size_t)(blk1 - blk0) * per_block;
+                TC_CUDA_TRY(cudaEventRecord(c.ev_chunk[k], c.stream));
+                TC_CUDA_TRY(cudaStreamWaitEvent(c.aux, c.ev_chunk[k], 0));
+                TC_CUDA_TRY(cudaMemcpyAsync(host_x + o, xout + o, sizeof(double) * cnt,
+                                            cudaMemcpyDeviceToHost, c.aux));
+                TC_CUDA_TRY(cudaMemcpyAsync(host_y + o, yout + o, sizeof(double) * cnt,
+                                            cudaMemcpyDeviceToHost, c.aux));
+            }
+        }
+        c.host_copied = nchunks > 1;
         return TC_OK;
     });
     if (rc) return rc;
-    phase_mark(c, 7);
-    if (ntasks > nbricks) {
-        k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8, (long long)sm_count() * 16),
-                               256, 0, c.stream>>>(nbricks, L, offs, partial, xout, yout);
-        TC_KERNEL_CHECK();
-    }
     return TC_OK;
 }
 

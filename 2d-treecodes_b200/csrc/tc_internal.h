@@ -126,6 +126,8 @@ struct Context {
     // host entry points: x/y are copied on `stream`, v (and targets) on `aux` after them;
     // ev_inputs marks v's arrival
     cudaEvent_t ev_inputs = nullptr;
+    cudaEvent_t ev_chunk[4] = {};        // force output runs ready for their host copy
+    bool host_copied = false;
     // a source sort whose values arrive late (sort_sources / finish_sources)
     const double *late_x = nullptr, *late_y = nullptr, *late_v = nullptr;
     cudaEvent_t late_ready = nullptr;
@@ -234,8 +236,12 @@ struct AuxScope {
 typedef int (*OverlapFn)(Context &c);
 
 // ---- force.cu
+// With host_x / host_y, the outputs are also copied there, run by run while later runs are
+// evaluated (c.host_copied tells whether that happened; the copies are on the auxiliary
+// stream).
 int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, const double *hs,
-               int nblocks, double *xout, double *yout, OverlapFn between);
+               int nblocks, double *xout, double *yout, OverlapFn between,
+               double *host_x = nullptr, double *host_y = nullptr);
 
 // ---- potential.cu
 int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out,
