@@ -249,3 +249,18 @@ def test_potential_log_within_a_few_ulp_of_the_library(gpu_ctx):
     ulp = np.spacing(np.abs(lib))
     err = np.abs(mine - lib)
     assert np.all(err <= 4 * ulp), (err / ulp).max()
+
+
+def test_force_host_outputs_copied_in_runs(gpu_ctx):
+    """Host outputs of 2^21 targets or more come back in runs of blocks copied while later runs
+    are evaluated: the same values as the device entry point, bit for bit, both precisions."""
+    w = W.lamb_oseen_force(n=100000, blocks_per_side=48, h=1.0 / (32 * 48))   # 2304 blocks
+    for precision in (0, 1):
+        gpu_ctx.set_precision(precision)
+        try:
+            hx, hy = gpu_ctx.force_mrag_host(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"],
+                                             w["y0s"], w["hs"])
+            dx, dy = gpu_force(gpu_ctx, w)
+        finally:
+            gpu_ctx.set_precision(0)
+        assert np.array_equal(hx, dx) and np.array_equal(hy, dy)
