@@ -25,11 +25,13 @@ constexpr BinomTable make_binom_table() {
 // Natural logarithm of a positive normal double, for the potential kernels' log r^2 terms
 // (arguments r^2 + 10 eps or |z|^2 of a far cell, never zero, subnormal or infinite).  From the
 // mathematics: x = 2^e m with m in [sqrt(1/2), sqrt(2)), s = (m - 1) / (m + 1), and
-// log m = 2 atanh s = 2 s (1 + s^2/3 + s^4/5 + ... + s^20/21), the atanh series cut where
-// |s| <= 0.1716 leaves a remainder below 2^-55 of it; log x = e ln 2 + log m, with ln 2 split
-// into a head of 21 bits (e * head exact) and a tail.  The division is a refined reciprocal
-// (rcp_nr).  About 30 instructions against the library log's ~100; within a few ulp of it
-// (tests/test_gpu_parity.py checks the bound on 2^20 arguments).
+// log m = 2 atanh s = 2 s (1 + s^2 q(s^2)), q(z) = (atanh(sqrt z) / sqrt z - 1) / z; log x =
+// e ln 2 + log m, with ln 2 split into a head of 21 bits (e * head exact) and a tail.  q is a
+// degree-6 polynomial fitted here to it on Chebyshev nodes over z in [0, ((sqrt 2 - 1) /
+// (sqrt 2 + 1))^2] (error below 2e-16, which the factor z <= 0.0295 scales to under 2^-57 of
+// log m).  The division is a refined reciprocal (rcp_nr).  About 25 instructions against the
+// library log's ~100; within a few ulp of it (tests/test_gpu_parity.py checks the bound on
+// 2^20 arguments).
 __device__ __forceinline__ double log_pos(double x) {
     const int lo = __double2loint(x);
     int hi = __double2hiint(x);
@@ -43,16 +45,13 @@ __device__ __forceinline__ double log_pos(double x) {
     const double f = m - 1.0;
     const double s = f * rcp_nr(2.0 + f);
     const double z = s * s;
-    double q = 1.0 / 21.0;
-    q = fma(q, z, 1.0 / 19.0);
-    q = fma(q, z, 1.0 / 17.0);
-    q = fma(q, z, 1.0 / 15.0);
-    q = fma(q, z, 1.0 / 13.0);
-    q = fma(q, z, 1.0 / 11.0);
-    q = fma(q, z, 1.0 / 9.0);
-    q = fma(q, z, 1.0 / 7.0);
-    q = fma(q, z, 1.0 / 5.0);
-    q = fma(q, z, 1.0 / 3.0);
+    double q = 0x1.2b584aae78a57p-4;
+    q = fma(q, z, 0x1.39fe606542ddep-4);
+    q = fma(q, z, 0x1.7462b4ab2ef6bp-4);
+    q = fma(q, z, 0x1.c71c62e5800a1p-4);
+    q = fma(q, z, 0x1.2492492df148dp-3);
+    q = fma(q, z, 0x1.99999999952e2p-3);
+    q = fma(q, z, 0x1.5555555555558p-2);
     const double two_s = 2.0 * s;
     const double logm = fma(two_s * z, q, two_s);
     constexpr double LN2_HEAD = 0x1.62e42p-1, LN2_TAIL = 0x1.fdf473de6af28p-22;
