@@ -78,7 +78,7 @@ int list_scratch(Context &c, int nkinds, int nwarps, int nitems, size_t entry_by
         return TC_OK;
     }
     const long long n = scratch_layout(c, nkinds, nwarps, nitems,
-                                       (512ll << 20) / (long long)entry_bytes, sl);
+                                       (2048ll << 20) / (long long)entry_bytes, sl);
     const cudaError_t e = cudaMallocAsync(&out.p, (size_t)n * entry_bytes + 16, c.stream);
     if (e != cudaSuccess) {
         out.p = nullptr;

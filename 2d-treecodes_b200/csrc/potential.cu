@@ -287,7 +287,9 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
     double *__restrict__ partial, int *task_ctr, const int *__restrict__ task_group,
     const float2 *__restrict__ sexp, const float *__restrict__ sscale) {
     __shared__ cplx s_coef[PE_WARPS][P];
-    __shared__ float2 s_coef32[PE_WARPS][P];
+    // mixed E2P coefficients in pairs (D_2j.re, D_2j+1.re, D_2j.im, D_2j+1.im): the even and
+    // the odd series run side by side in f32x2 lanes
+    __shared__ float4 s_coef32[PE_WARPS][P / 2];
     __shared__ double2 s_xy[PE_WARPS][PE_CHUNK];
     __shared__ double s_v[PE_WARPS][PE_CHUNK];
     // mixed form: the tile as negated float offsets (hi + lo) from the group's reference point,
@@ -355,7 +357,11 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                 const float R = R_n;
                 __syncwarp();
                 if (lane < P) {
-                    if (MIXED) s_coef32[warp][lane] = c32_n;
+                    if (MIXED) {
+                        float *cp = reinterpret_cast<float *>(s_coef32[warp]);
+                        cp[4 * (lane >> 1) + (lane & 1)] = c32_n.x;
+                        cp[4 * (lane >> 1) + 2 + (lane & 1)] = c32_n.y;
+                    }
                     else s_coef[warp][lane] = {cr_n, ci_n};
                 }
                 __syncwarp();
@@ -368,13 +374,25 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                         const float zr = (float)rz, zi = (float)iz;
                         const float inv = rcp_approx(zr * zr + zi * zi);
                         const float ur = R * zr * inv, ui = -R * zi * inv;
-                        float2 q = s_coef32[warp][P - 1];
+                        // Q(u') = E(w) + u' O(w), w = u'^2, E and O the even and odd parts
+                        // of the series, evaluated together by Horner in f32x2 lanes
+                        const float wr = fmaf(ur, ur, -ui * ui), wi = 2.f * ur * ui;
+                        const float2 wr2 = make_float2(wr, wr), wi2 = make_float2(wi, wi);
+                        const float2 nwi2 = make_float2(-wi, -wi);
+                        const float4 cl = s_coef32[warp][P / 2 - 1];
+                        float2 qr2 = make_float2(cl.x, cl.y), qi2 = make_float2(cl.z, cl.w);
 #pragma unroll
-                        for (int k = P - 2; k >= 0; --k) {
-                            const float2 d = s_coef32[warp][k];
-                            q = make_float2(fmaf(q.x, ur, fmaf(-q.y, ui, d.x)),
-                                            fmaf(q.x, ui, fmaf(q.y, ur, d.y)));
+                        for (int j = P / 2 - 2; j >= 0; --j) {
+                            const float4 d = s_coef32[warp][j];
+                            const float2 tr = __ffma2_rn(qi2, nwi2, make_float2(d.x, d.y));
+                            const float2 ti = __ffma2_rn(qi2, wr2, make_float2(d.z, d.w));
+                            const float2 nqr = __ffma2_rn(qr2, wr2, tr);
+                            qi2 = __ffma2_rn(qr2, wi2, ti);
+                            qr2 = nqr;
                         }
+                        const float2 q = make_float2(
+                            qr2.x + fmaf(ur, qr2.y, -ui * qi2.y),
+                            qi2.x + fmaf(ur, qi2.y, ui * qr2.y));
                         two_sum_add(sh, sl, ur * q.x - ui * q.y);
                         far += mm * log_pos(r2) * 0.5;
                     } else {

@@ -102,7 +102,7 @@ long long scratch_layout(const Context &c, int nkinds, int nwarps, int nitems,
                          long long max_entries, ScratchLayout &s);
 // Scratch of a one-walk list build: the sort's record buffer (32 B per source, dead once the
 // sources are gathered) when the regions fit in it, else a transient block from the device's
-// pool (at most 512 MB), allocated on the context's current stream and released on it, in
+// pool (at most 2 GB), allocated on the context's current stream and released on it, in
 // stream order, when the guard goes out of scope after the last use has been enqueued.
 struct ListScratch {
     void *p = nullptr;
