@@ -201,6 +201,8 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_inputs, cudaEventDisableTiming));
     for (auto &ev : c.ev_chunk) TC_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_leafset, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_moments, cudaEventDisableTiming));
     c.h_pinned = pinned_area();
     if (!c.h_pinned) {
         set_error(TC_ERR_ALLOC, "page-locked host allocation failed");
@@ -236,7 +238,7 @@ static void context_free(Context &c) {
     release_pool_cache(c.device);
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
-    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs})
+    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs, c.ev_leafset, c.ev_moments})
         if (ev) cudaEventDestroy(ev);
     for (auto &ev : c.ev_chunk)
         if (ev) cudaEventDestroy(ev);

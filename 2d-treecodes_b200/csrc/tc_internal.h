@@ -127,6 +127,8 @@ struct Context {
     // ev_inputs marks v's arrival
     cudaEvent_t ev_inputs = nullptr;
     cudaEvent_t ev_chunk[4] = {};        // force output runs ready for their host copy
+    cudaEvent_t ev_leafset = nullptr;     // leaf moments written (main stream)
+    cudaEvent_t ev_moments = nullptr;     // parent moments written (auxiliary stream)
     bool host_copied = false;
     // a source sort whose values arrive late (sort_sources / finish_sources)
     const double *late_x = nullptr, *late_y = nullptr, *late_v = nullptr;

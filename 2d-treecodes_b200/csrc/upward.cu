@@ -161,11 +161,14 @@ __global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 4 : 3) void k_leaf_p2e(
     int2 nrg = {0, 0};
     int4 ncl = {0, 0, 0, 0};
     double ncx = 0, ncy = 0;
+    // (the com only for leaves: the parents' moments may be written meanwhile)
     if (next < nnodes) {
         nrg = range[next];
         ncl = cell[next];
-        ncx = tnode[next].xcom;
-        ncy = tnode[next].ycom;
+        if (is_leaf(nrg, ncl, leafcap)) {
+            ncx = tnode[next].xcom;
+            ncy = tnode[next].ycom;
+        }
     }
     while (next < nnodes) {
         const int node = next;
@@ -176,8 +179,10 @@ __global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 4 : 3) void k_leaf_p2e(
         if (next < nnodes) {
             nrg = range[next];
             ncl = cell[next];
-            ncx = tnode[next].xcom;
-            ncy = tnode[next].ycom;
+            if (is_leaf(nrg, ncl, leafcap)) {
+                ncx = tnode[next].xcom;
+                ncy = tnode[next].ycom;
+            }
         }
         if (!is_leaf(rg, cl, leafcap) || rg.x < 0 || rg.y < rg.x || rg.y > nsrc) continue;
         int e = 0;   // R = 2^e (mixed form)
@@ -712,6 +717,12 @@ int upward_moments(Context &c) {
         nn, c.nsrc, c.leafcap, slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS),
         slot_ptr<double>(c, S_VS), range, cell, tnode, mass, w, wx, wy, frame, err);
     TC_KERNEL_CHECK();
+    // The parent moments run on the auxiliary stream, beside the leaves' P2E on the main one
+    // (P2E reads only the leaves' own moments; the E2E waits for ev_moments, and anything
+    // queued later on the auxiliary stream, such as the interaction lists, follows them).
+    TC_CUDA_TRY(cudaEventRecord(c.ev_leafset, c.stream));
+    AuxScope on_aux(c);
+    TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_leafset, 0));
     // inner nodes exist on levels 0 .. LMAX-1, deepest first
     const LevelOffsets offs = level_offsets(c);
     const int ltop = small_top(c, MOM_TOP_MAX);
@@ -727,6 +738,7 @@ int upward_moments(Context &c) {
                                                        frame, err);
         TC_KERNEL_CHECK();
     }
+    TC_CUDA_TRY(cudaEventRecord(c.ev_moments, c.stream));
     return TC_OK;
 }
 
@@ -760,6 +772,8 @@ static int run_expansions(Context &c) {
     p2e<<<grid, UP_WARPS * 32, smem, c.stream>>>(nn, c.nsrc, c.leafcap, xs, ys, vs, range, cell,
                                                  tnode, exps, frame);
     TC_KERNEL_CHECK();
+    // the parents' moments (expansion centres) come from the auxiliary stream
+    TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_moments, 0));
     // E2E deepest level first: wide levels thread per node, narrow ones warp per node, the
     // small top levels in one single-block launch
     const LevelOffsets offs = level_offsets(c);
