@@ -9,7 +9,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "treecodes_b200.h"
@@ -99,6 +101,29 @@ void scratch_learn(Context &c, int nkinds, int nwarps, int nitems, const unsigne
     }
 }
 
+// Host waits of a solve.  By default the thread spins in the CUDA call, the lowest latency.  A
+// context with sleeping_waits polls every 20 us and sleeps in between: the request server's
+// slot threads wait that way, so that four waiting slots do not take four host cores from the
+// threads that stage inputs and submit requests.
+template <class Query>
+static cudaError_t poll_and_sleep(Query query) {
+    for (;;) {
+        const cudaError_t e = query();
+        if (e != cudaErrorNotReady) return e;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+cudaError_t wait_stream(Context &c, cudaStream_t s) {
+    if (!c.sleeping_waits) return cudaStreamSynchronize(s);
+    return poll_and_sleep([s] { return cudaStreamQuery(s); });
+}
+
+cudaError_t wait_event(Context &c, cudaEvent_t e) {
+    if (!c.sleeping_waits) return cudaEventSynchronize(e);
+    return poll_and_sleep([e] { return cudaEventQuery(e); });
+}
+
 // Reads back the device error word and the work counters (one sync).  The counters land in
 // h_pinned[16 ...] as unsigned long long.
 int check_device_errors(Context &c, const char *where) {
@@ -108,7 +133,7 @@ int check_device_errors(Context &c, const char *where) {
     TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned + 16, c.buf[S_STATS].p,
                                 sizeof(unsigned long long) * STAT_SLOTS, cudaMemcpyDeviceToHost,
                                 c.stream));
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    TC_CUDA_TRY(wait_stream(c, c.stream));
     c.counts.launches = g_launches;
     const unsigned e = c.h_pinned[8];
     if (e & DEVERR_SPIN_LIMIT) {
@@ -167,6 +192,31 @@ static void pinned_release(unsigned *a) {
     g_pinned_free.push_back(a);
 }
 
+// Loads every kernel of the library on `device`, once per process.  Under lazy module loading
+// (the CUDA default) a kernel is loaded at its first launch, and loading may synchronise the
+// whole device: in the request server, the first solve of a form, order or list-walk mode not
+// seen before stalled every concurrent solve.  Querying each kernel's attributes loads it, so
+// the first context pays that cost at start-up instead.
+static int preload_kernels(int device) {
+    static std::mutex mu;
+    static std::vector<int> loaded;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(loaded.begin(), loaded.end(), device) != loaded.end()) return TC_OK;
+    KernelList v;
+    kernels_sort(v);
+    kernels_tree(v);
+    kernels_upward(v);
+    kernels_force(v);
+    kernels_potential(v);
+    kernels_direct(v);
+    for (const void *k : v) {
+        cudaFuncAttributes a;
+        TC_CUDA_TRY(cudaFuncGetAttributes(&a, k));
+    }
+    loaded.push_back(device);
+    return TC_OK;
+}
+
 static int context_init(Context &c, int device, cudaStream_t stream) {
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -178,6 +228,7 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     if (device < 0) TC_CUDA_TRY(cudaGetDevice(&device));
     TC_CUDA_TRY(cudaSetDevice(device));
     c.device = device;
+    if (int rc = preload_kernels(device)) return rc;
     if (stream) {
         c.stream = stream;
         c.own_stream = false;
@@ -250,7 +301,7 @@ static void context_free(Context &c) {
 
 static void finish_timing(Context &c) {
     if (!c.timing) return;
-    cudaEventSynchronize(c.ev[5]);
+    wait_event(c, c.ev[5]);
     float t[6] = {};
     for (int i = 1; i <= 5; ++i) cudaEventElapsedTime(&t[i], c.ev[i - 1], c.ev[i]);
     c.times.sort_ms = t[1];
@@ -422,11 +473,11 @@ static int potential_host(Context &c, double theta, const double *xs, const doub
         return rc;
     rc = potential_device(c, theta, dx, dy, dv, n, dxt, dyt, m, dout, c.ev_inputs);
     // the copies on the auxiliary stream read the caller's memory: done before returning
-    const cudaError_t e = cudaStreamSynchronize(c.aux);
+    const cudaError_t e = wait_stream(c, c.aux);
     if (rc) return rc;
     TC_CUDA_TRY(e);
     TC_CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    TC_CUDA_TRY(wait_stream(c, c.stream));
     return TC_OK;
 }
 
@@ -450,14 +501,14 @@ static int force_host(Context &c, double theta, const double *xs, const double *
         return rc;
     // the outputs come back run by run while later runs are evaluated (force_mrag)
     rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy, c.ev_inputs, xo, yo);
-    const cudaError_t e = cudaStreamSynchronize(c.aux);
+    const cudaError_t e = wait_stream(c, c.aux);
     if (rc) return rc;
     TC_CUDA_TRY(e);
     if (!c.host_copied) {
         TC_CUDA_TRY(cudaMemcpyAsync(xo, dox, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
         TC_CUDA_TRY(cudaMemcpyAsync(yo, doy, sizeof(double) * nt, cudaMemcpyDeviceToHost, c.stream));
     }
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    TC_CUDA_TRY(wait_stream(c, c.stream));
     return TC_OK;
 }
 
@@ -560,6 +611,16 @@ TC_API int tc_set_precision(tc_context *ctx, int precision) {
         return TC_ERR_INVALID;
     }
     ctx->c.precision = precision;
+    return TC_OK;
+}
+
+TC_API int tc_set_host_waits(tc_context *ctx, int sleeping) {
+    clear_error();
+    if (!ctx || sleeping < 0 || sleeping > 1) {
+        set_error(TC_ERR_INVALID, "invalid host wait mode %d", sleeping);
+        return TC_ERR_INVALID;
+    }
+    ctx->c.sleeping_waits = sleeping != 0;
     return TC_OK;
 }
 

@@ -157,4 +157,10 @@ int measure_fma_peak(int fp64, double *tflops) {
     return TC_OK;
 }
 
+void kernels_direct(KernelList &v) {
+    v.insert(v.end(), {(const void *)k_direct_potential, (const void *)k_direct_force,
+                       (const void *)k_log_probe, (const void *)k_fma_peak<float>,
+                       (const void *)k_fma_peak<double>});
+}
+
 }  // namespace tc

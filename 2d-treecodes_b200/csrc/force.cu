@@ -762,7 +762,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         cudaStreamSynchronize(c.aux);   // leave nothing of this solve in flight
         return rc;
     }
-    TC_CUDA_TRY(cudaEventSynchronize(c.ev_totals));
+    TC_CUDA_TRY(wait_event(c, c.ev_totals));
     int tot[4];
     for (int k = 0; k < 4; ++k) tot[k] = (int)c.h_pinned[32 + k];
     const bool overflow = c.h_pinned[36] != 0;
@@ -873,6 +873,18 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     });
     if (rc) return rc;
     return TC_OK;
+}
+
+void kernels_force(KernelList &v) {
+    v.insert(v.end(), {(const void *)k_force_lists<1>, (const void *)k_force_lists<2>,
+                       (const void *)k_force_lists_copy, (const void *)k_task_map,
+                       (const void *)k_force_gather_parts});
+#define TC_FORCE_KERNELS(P)                                                                      \
+    v.insert(v.end(), {(const void *)k_force_eval<P, true, 5>, (const void *)k_force_eval<P, true, 0>, \
+                       (const void *)k_force_eval<P, false, 5>,                                  \
+                       (const void *)k_force_eval<P, false, 0>, (const void *)k_scale_coeffs<P, true>});
+    TC_FOR_EACH_ORDER(TC_FORCE_KERNELS)
+#undef TC_FORCE_KERNELS
 }
 
 }  // namespace tc

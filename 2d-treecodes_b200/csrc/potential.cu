@@ -690,7 +690,7 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
         cudaStreamSynchronize(c.aux);   // leave nothing of this solve in flight
         return rc;
     }
-    TC_CUDA_TRY(cudaEventSynchronize(c.ev_totals));
+    TC_CUDA_TRY(wait_event(c, c.ev_totals));
     const int n_e2p = (int)c.h_pinned[32], total = (int)c.h_pinned[33];
     const int ntasks = (int)c.h_pinned[34] - total;
     const bool overflow = c.h_pinned[36] != 0;
@@ -771,6 +771,17 @@ int potential(Context &c, double theta, const double *xt, const double *yt, int 
         TC_KERNEL_CHECK();
     }
     return TC_OK;
+}
+
+void kernels_potential(KernelList &v) {
+    v.insert(v.end(), {(const void *)k_potential_lists<1>, (const void *)k_potential_lists<2>,
+                       (const void *)k_potential_lists_copy, (const void *)k_task_map_groups,
+                       (const void *)k_potential_gather_parts});
+#define TC_POTENTIAL_KERNELS(P)                                                                  \
+    v.insert(v.end(), {(const void *)k_potential_eval<P, true>,                                 \
+                       (const void *)k_potential_eval<P, false>, (const void *)k_scale_coeffs_pot<P>});
+    TC_FOR_EACH_ORDER(TC_POTENTIAL_KERNELS)
+#undef TC_POTENTIAL_KERNELS
 }
 
 }  // namespace tc

@@ -135,7 +135,10 @@ int validate(const tc_request &r) {
 }
 
 int run_request(tc_context *ctx, const tc_request &r) {
-    int rc = tc_set_precision(ctx, r.precision);
+    // slot threads sleep while their solve runs instead of spinning on a host core
+    int rc = tc_set_host_waits(ctx, 1);
+    if (rc) return rc;
+    rc = tc_set_precision(ctx, r.precision);
     if (rc) return rc;
     if (r.kind == TC_REQUEST_POTENTIAL)
         return tc_potential_host(ctx, r.theta, r.xsources, r.ysources, r.sourcevalues, r.nsources,

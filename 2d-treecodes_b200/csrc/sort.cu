@@ -901,6 +901,17 @@ static unsigned char *noalloc_scratch_base(int device) {
     return static_cast<unsigned char *>(addr[device]);
 }
 
+void kernels_sort(KernelList &v) {
+    v.insert(v.end(), {(const void *)k_bbox, (const void *)k_keys, (const void *)k_target_keys,
+                       (const void *)k_gather3, (const void *)k_hist, (const void *)k_hist_scan,
+                       (const void *)k_onesweep, (const void *)k_keys_pack<true>,
+                       (const void *)k_keys_pack<false>, (const void *)k_onesweep_items,
+                       (const void *)k_gather_sources<true>, (const void *)k_gather_sources<false>,
+                       (const void *)k_pack_rec, (const void *)k_items_split,
+                       (const void *)k_scan_reduce, (const void *)k_scan_blocks,
+                       (const void *)k_scan_apply});
+}
+
 }  // namespace tc
 
 extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const double *ysources,

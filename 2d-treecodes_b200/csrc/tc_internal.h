@@ -8,6 +8,7 @@
 #include <string>
 #include <type_traits>
 #include <utility>
+#include <vector>
 
 #include "tc_common.cuh"
 
@@ -143,6 +144,8 @@ struct Context {
     // scratch region is sized for, raised after every solve to what it needed
     int list_per_item[3] = {32, 32, 32};
     int list_walks = 0;                   // walks the last list build took (1 or 2)
+    // host waits of a solve: spin in the CUDA call (false) or poll and sleep (wait_stream)
+    bool sleeping_waits = false;
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};
@@ -249,8 +252,21 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
 int potential(Context &c, double theta, const double *xt, const double *yt, int m, double *out,
               OverlapFn between);
 
+// ---- kernel lists: each source file's kernels, every instance the library launches (for
+// preload_kernels in capi.cu)
+using KernelList = std::vector<const void *>;
+void kernels_sort(KernelList &v);
+void kernels_tree(KernelList &v);
+void kernels_upward(KernelList &v);
+void kernels_force(KernelList &v);
+void kernels_potential(KernelList &v);
+void kernels_direct(KernelList &v);
+
 // ---- capi.cu
 int check_device_errors(Context &c, const char *where);
+// A solve's host waits for a stream / an event (see Context::sleeping_waits).
+cudaError_t wait_stream(Context &c, cudaStream_t s);
+cudaError_t wait_event(Context &c, cudaEvent_t e);
 void phase_mark(Context &c, int idx);
 
 }  // namespace tc

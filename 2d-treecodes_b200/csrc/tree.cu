@@ -381,7 +381,7 @@ int build_topology(Context &c, int leafcap) {
     // the level totals and the list length, in one read-back
     TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, totals, sizeof(int) * (LMAX + 1),
                                 cudaMemcpyDeviceToHost, c.stream));
-    TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    TC_CUDA_TRY(wait_stream(c, c.stream));
     const int nlist = (int)c.h_pinned[LMAX];
     if (nlist > cap) {
         set_error(TC_ERR_INVALID, "tree list length %d exceeds its bound %d", nlist, cap);
@@ -427,6 +427,12 @@ int build_topology(Context &c, int leafcap) {
         TC_KERNEL_CHECK();
     }
     return TC_OK;
+}
+
+void kernels_tree(KernelList &v) {
+    v.insert(v.end(), {(const void *)k_tree_list, (const void *)k_rank_count,
+                       (const void *)k_rank_scan, (const void *)k_rank_apply,
+                       (const void *)k_tree_root, (const void *)k_tree_children});
 }
 
 }  // namespace tc

@@ -827,4 +827,15 @@ int upward_pass(Context &c, int order) {
     return TC_OK;
 }
 
+void kernels_upward(KernelList &v) {
+    v.insert(v.end(), {(const void *)k_leaf_setup, (const void *)k_moments_level,
+                       (const void *)k_moments_top});
+#define TC_UPWARD_KERNELS(P)                                                                     \
+    v.insert(v.end(), {(const void *)k_leaf_p2e<P, true>, (const void *)k_leaf_p2e<P, false>,    \
+                       (const void *)k_upward_level<P>, (const void *)k_upward_wide<P>,           \
+                       (const void *)k_upward_top<P>});
+    TC_FOR_EACH_ORDER(TC_UPWARD_KERNELS)
+#undef TC_UPWARD_KERNELS
+}
+
 }  // namespace tc

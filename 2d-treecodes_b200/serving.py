@@ -41,6 +41,25 @@ def pinned_empty(n):
         return np.empty(int(n))
 
 
+def warm_pinned_cache(max_bytes=1 << 25, per_class=12):
+    """Fills torch's page-locked block cache: `per_class` blocks of every power-of-two size
+    class from 4 KB to `max_bytes`, allocated and released at once.  The cache keeps freed blocks
+    by class, so later `pinned_empty` calls reuse them; an empty class instead calls the driver's
+    page-locked allocation, which may synchronise the device and stall every solve in flight."""
+    held, total, b = [], 0, 4096
+    try:
+        import torch
+        while b <= max_bytes:
+            for _ in range(per_class):
+                held.append(torch.empty(b, dtype=torch.uint8, pin_memory=True))
+                total += b
+            b *= 2
+    except Exception:   # no CUDA driver: pinned_empty hands out pageable memory then
+        return 0
+    del held
+    return total
+
+
 def pinned_copy(a):
     out = pinned_empty(len(a))
     out[:] = a
@@ -104,8 +123,10 @@ class Materialiser:
 
     def __init__(self, log2_max=22, seed=1456):
         self.log2_max = log2_max
-        self.masters, self.noise = _masters(log2_max, seed)
+        self.masters, noise = _masters(log2_max, seed)
+        self.noise = 1e-3 * noise       # the advection step, scaled once
         self.state = {}
+        warm_pinned_cache(8 << log2_max)
 
     def __call__(self, spec):
         n = spec["n"]
@@ -115,8 +136,8 @@ class Materialiser:
             o = spec["noise_off"] % (len(self.noise) - 2 * n)
             # advected sources in page-locked memory (torch's caching host allocator recycles
             # the blocks), so that the server's copies of them are direct DMA
-            xs = np.add(xs, 1e-3 * self.noise[o:o + n], out=pinned_empty(n))
-            ys = np.add(ys, 1e-3 * self.noise[o + n:o + 2 * n], out=pinned_empty(n))
+            xs = np.add(xs, self.noise[o:o + n], out=pinned_empty(n))
+            ys = np.add(ys, self.noise[o + n:o + 2 * n], out=pinned_empty(n))
         else:
             sl = slice(spec["off"], spec["off"] + n)
             xs, ys = xm[sl], ym[sl]            # read-only views of the master set

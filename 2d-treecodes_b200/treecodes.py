@@ -40,6 +40,7 @@ SIGNATURES = {
     "tc_context_create": (_i, [ctypes.POINTER(_vp), _i, _vp]),
     "tc_context_destroy": (None, [_vp]),
     "tc_set_precision": (_i, [_vp, _i]),
+    "tc_set_host_waits": (_i, [_vp, _i]),
     "tc_set_orders": (_i, [_vp, _i, _i]),
     "tc_supported_orders": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
     "tc_set_blocksize": (_i, [_vp, _i]),
@@ -237,6 +238,11 @@ class Context:
 
     def set_precision(self, mode):
         _check(self.lib.tc_set_precision(self.h, int(mode)))
+
+    def set_host_waits(self, sleeping):
+        """0: the solving thread spins while the device works (lowest latency); 1: it polls
+        and sleeps, leaving the host core to other threads."""
+        _check(self.lib.tc_set_host_waits(self.h, int(sleeping)))
 
     def set_orders(self, potential_order=ORDER_POTENTIAL, force_order=ORDER_FORCE):
         """Expansion orders of the next solves (the reference's build-time potential-order and

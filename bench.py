@@ -568,14 +568,17 @@ def run_serving(args, T):
                       "sources": "log-uniform [2^12, 2^22]", "force_share": 0.7,
                       "followup_share": 0.2, "theta": list(S.THETAS),
                       "distributions": list(S.DISTRIBUTIONS), "host_memory": "page-locked",
-                      "warm_up": "60 requests of another seed, not counted",
+                      "warm_up": "60 requests of another seed in each form, not counted",
                       "latency": "scheduled arrival to completion (host clock)"}}
     m = S.Materialiser()
     srv = T.Server(slots=args.serving_slots,
                    hbm_budget_bytes=int(args.serving_budget_gb * (1 << 30)),
                    host_alloc=S.pinned_empty)
     try:
-        S.run_stream(srv, S.make_stream(nreq=60, rate_hz=args.serving_rate, seed=99), 1, m)
+        warm = S.make_stream(nreq=60, rate_hz=args.serving_rate, seed=99)
+        for precision in (1, 0):
+            m.state.clear()
+            S.run_stream(srv, warm, precision, m)
         for precision, name in ((1, "mixed"), (0, "fp64")):
             m.state.clear()
             summary, _ = S.run_stream(srv, specs, precision, m)

@@ -98,6 +98,10 @@ typedef struct {
 TC_API int tc_context_create(tc_context **ctx, int device, void *cuda_stream);
 TC_API void tc_context_destroy(tc_context *ctx);
 TC_API int tc_set_precision(tc_context *ctx, int precision);
+/* How the calling thread waits for the device inside a solve: 0 (the default) spins in the CUDA
+ * call, the lowest latency; 1 polls every 20 us and sleeps in between, which leaves the host core
+ * to other threads (the request server's slots wait this way). */
+TC_API int tc_set_host_waits(tc_context *ctx, int sleeping);
 /* Expansion orders of the context's next solves: the reference fixes them when it is built
  * (Makefile:13-14 of the reference, potential-order = 12 and force-order = 24, which stay the
  * defaults here).  Any order that tc_supported_orders lists may be chosen, independently for

@@ -121,3 +121,27 @@ def test_resident_client_steps_in_order_and_release(materialiser):
     assert_same(outs, [solo(s, d, 1) for s, d in zip(steps, datas)])
     # the steps differ (each advects the previous one), so order mattered
     assert not np.array_equal(outs[0][0], outs[1][0])
+
+
+def test_sleeping_host_waits_give_the_same_results():
+    """tc_set_host_waits(1), the way the server's slots wait, changes only how the host thread
+    waits: both solves equal the spinning default bit for bit; other modes are refused."""
+    import workloads as W
+    w = W.lamb_oseen_force(n=40000, blocks_per_side=2, h=1.0 / 64)
+    p = W.uniform_potential(n=30000)
+    out = {}
+    for mode in (0, 1):
+        ctx = T.Context(device=0)
+        try:
+            ctx.set_host_waits(mode)
+            f = ctx.force_mrag_host(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"],
+                                    w["hs"])
+            q = ctx.potential_host(p["theta"], p["xs"], p["ys"], p["vs"], p["xt"], p["yt"])
+            out[mode] = (f[0], f[1], q)
+            for bad in (-1, 2):
+                with pytest.raises(T.TreecodeError, match="wait mode"):
+                    ctx.set_host_waits(bad)
+        finally:
+            ctx.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
