@@ -169,7 +169,8 @@ int device_sm_count() {
 // The contexts' small page-locked read-back areas (4 KB each) come from slabs allocated once
 // per process and recycled: cudaMallocHost per context cost a synchronising call on every
 // context creation, which stalled the other contexts' work whenever a serving client arrived.
-constexpr size_t PINNED_AREA = 4096, PINNED_SLAB = 64 * PINNED_AREA;
+// A slab serves 256 contexts (a request server keeps hundreds of resident clients).
+constexpr size_t PINNED_AREA = 4096, PINNED_SLAB = 256 * PINNED_AREA;
 static std::mutex g_pinned_mu;
 static std::vector<unsigned *> g_pinned_free;
 
@@ -190,6 +191,27 @@ static void pinned_release(unsigned *a) {
     if (!a) return;
     std::lock_guard<std::mutex> lock(g_pinned_mu);
     g_pinned_free.push_back(a);
+}
+
+// Hands the pool blocks that no context holds back to the driver.
+static cudaError_t release_pool_cache(int device) {
+    cudaMemPool_t pool;
+    cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, device);
+    return e == cudaSuccess ? cudaMemPoolTrimTo(pool, 0) : e;
+}
+
+// Live contexts per device.  Freed buffers stay cached in the device's pool while any context
+// lives, for the next allocation of any of them: a trim at every context's end (a request
+// server evicting idle clients) handed the memory back only for the next solve to map it anew.
+// The last context of a device hands the cache back (tc_release_cached_memory does it at once).
+static std::mutex g_live_mu;
+static std::vector<int> g_live;
+
+static void context_counted(int device, int delta) {
+    std::lock_guard<std::mutex> lock(g_live_mu);
+    if ((int)g_live.size() <= device) g_live.resize(device + 1, 0);
+    g_live[device] += delta;
+    if (g_live[device] == 0) release_pool_cache(device);
 }
 
 // Loads every kernel of the library on `device`, once per process.  Under lazy module loading
@@ -267,26 +289,22 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     if ((rc = ensure(c, S_STATS, STAT_SLOTS, &stats))) return rc;
     TC_CUDA_TRY(cudaMemsetAsync(err, 0, 64 * sizeof(unsigned), c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(stats, 0, STAT_SLOTS * sizeof(unsigned long long), c.stream));
+    context_counted(device, +1);
+    c.live = true;
     return TC_OK;
-}
-
-// Hands the pool blocks that no context holds back to the driver.
-static void release_pool_cache(int device) {
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
 }
 
 static void context_free(Context &c) {
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     if (c.aux) cudaStreamSynchronize(c.aux);
-    // stream-ordered frees (cudaFree would synchronise the whole device), then the pool's
-    // unused blocks back to the driver
+    // stream-ordered frees (cudaFree would synchronise the whole device)
     cudaStream_t fs = c.stream ? c.stream : c.aux;
     for (auto &b : c.buf)
         if (b.p) cudaFreeAsync(b.p, fs);
     if (fs) cudaStreamSynchronize(fs);
-    release_pool_cache(c.device);
+    if (c.live) context_counted(c.device, -1);
+    c.live = false;
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs, c.ev_leafset, c.ev_moments})
@@ -690,8 +708,15 @@ TC_API int tc_context_trim(tc_context *ctx) {
         b.bytes = 0;
     }
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    release_pool_cache(c.device);
     c.nnodes = c.nsrc = 0;
+    return TC_OK;
+}
+
+TC_API int tc_release_cached_memory(int device) {
+    clear_error();
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return TC_ERR_NO_DEVICE;
+    TC_CUDA_TRY(cudaSetDevice(device));
+    TC_CUDA_TRY(release_pool_cache(device));
     return TC_OK;
 }
 

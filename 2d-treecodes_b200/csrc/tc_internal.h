@@ -146,6 +146,7 @@ struct Context {
     int list_walks = 0;                   // walks the last list build took (1 or 2)
     // host waits of a solve: spin in the CUDA call (false) or poll and sleep (wait_stream)
     bool sleeping_waits = false;
+    bool live = false;                    // counted among the device's live contexts
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};

@@ -5,7 +5,8 @@ force_mrag solve (70% force) with a source count drawn log-uniformly in [2^12, 2
 drawn from one of the four benchmark distributions (uniform, Gaussian mixture, Lamb-Oseen
 vortex, vortex sheet) and theta from {0.3, 0.5, 0.7}.  A fifth of the requests are follow-up
 steps of an earlier client: that client's previous sources advected by 1e-3 N(0,1), solved on
-the client's resident context.  Potential targets are a copy of the source coordinates; force
+the client's resident context, which the driver releases once the client's last step is done.
+Potential targets are a copy of the source coordinates; force
 targets are a g x g grid of 32 x 32-point blocks tiling [0,1)^2 with g = round(sqrt(N / 2048))
 (about N/2 targets).
 
@@ -192,6 +193,9 @@ def run_stream(server, specs, precision, materialise, keep_outputs=False):
                 continue
             t_done = time.perf_counter()
             records[i] = dict(res, t_done=t_done, t_sub=t_sub)
+            spec = specs[i]
+            if spec["resident"] and spec["step"] == spec["last_step"]:
+                server.release_client(spec["client"])   # the client's session is over
             if keep_outputs:
                 outputs[i] = outs
 

@@ -41,6 +41,7 @@ SIGNATURES = {
     "tc_context_destroy": (None, [_vp]),
     "tc_set_precision": (_i, [_vp, _i]),
     "tc_set_host_waits": (_i, [_vp, _i]),
+    "tc_release_cached_memory": (_i, [_i]),
     "tc_set_orders": (_i, [_vp, _i, _i]),
     "tc_supported_orders": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
     "tc_set_blocksize": (_i, [_vp, _i]),
@@ -190,6 +191,12 @@ def supported_orders():
     buf = (ctypes.c_int * n)()
     load().tc_supported_orders(buf, n)
     return list(buf)
+
+
+def release_cached_memory(device=-1):
+    """Hands the device's cached, unused pool memory back to the driver (destroyed and trimmed
+    contexts leave their memory cached while another context of the device lives)."""
+    _check(load().tc_release_cached_memory(int(device)))
 
 
 def measure_fma_peak(fp64=True):

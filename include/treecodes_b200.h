@@ -201,8 +201,13 @@ TC_API int tc_sort_sources_noalloc(const double *xsources, const double *ysource
 
 /* Device memory held by a context's grow-only buffers, in bytes. */
 TC_API size_t tc_context_device_bytes(tc_context *ctx);
-/* Frees a context's device buffers; the next solve on it allocates them again. */
+/* Frees a context's device buffers; the next solve on it allocates them again.  Freed memory
+ * (here and in tc_context_destroy) stays cached in the device's stream-ordered pool for the
+ * process's next allocations while any context of the device lives; the last context's
+ * destruction, or tc_release_cached_memory, hands it back to the driver. */
 TC_API int tc_context_trim(tc_context *ctx);
+/* Hands the device's cached, unused pool memory back to the driver (device < 0: current). */
+TC_API int tc_release_cached_memory(int device);
 
 /* ---- serving loop ---------------------------------------------------------------------
  * A request server on one GPU: solves submitted from any thread are queued, admitted in

@@ -145,3 +145,32 @@ def test_sleeping_host_waits_give_the_same_results():
             ctx.close()
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+def test_trimmed_memory_stays_cached_until_released():
+    """tc_context_trim frees a context's buffers into the device's pool, which keeps them for
+    the next allocations while contexts live; tc_release_cached_memory hands them back."""
+    import torch
+    import workloads as W
+    w = W.lamb_oseen_force(n=1 << 20, blocks_per_side=4, h=1.0 / 128)
+    keep = T.Context(device=0)   # another live context: trims and destroys keep the cache
+    ctx = T.Context(device=0)
+    try:
+        ctx.force_mrag_host(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"], w["hs"])
+        held = ctx.device_bytes()
+        assert held > 64 << 20
+        ctx.trim()
+        assert ctx.device_bytes() < 1 << 20
+        free0 = torch.cuda.mem_get_info(0)[0]
+        T.release_cached_memory(0)
+        free1 = torch.cuda.mem_get_info(0)[0]
+        assert free1 - free0 > held // 2, (free0, free1, held)
+        # the context solves again after the trim, with the same result
+        a = ctx.force_mrag_host(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"],
+                                w["hs"])
+        b = keep.force_mrag_host(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"],
+                                 w["hs"])
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    finally:
+        ctx.close()
+        keep.close()
