@@ -5,11 +5,11 @@
 // gets its own context (stream + grow-only device buffers), so the functions are reentrant,
 // unlike the reference whose Tree:: globals are shared (drivers/upward.cpp:51-59).
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <chrono>
 #include <mutex>
 #include <thread>
 #include <vector>
