@@ -474,6 +474,14 @@ static int stage_split(Context &c, std::initializer_list<StagedArray> first,
     return TC_OK;
 }
 
+// Error return of a host entry point after staging began: copies already queued on either
+// stream may still read the caller's memory, so both streams are waited for before returning.
+static int drain_and_fail(Context &c, int rc) {
+    wait_stream(c, c.aux);
+    wait_stream(c, c.stream);
+    return rc;
+}
+
 static int potential_host(Context &c, double theta, const double *xs, const double *ys,
                           const double *vs, int n, const double *xt, const double *yt, int m,
                           double *out) {
@@ -489,7 +497,7 @@ static int potential_host(Context &c, double theta, const double *xs, const doub
                           {{S_VIN, vs, (size_t)n, &dv}, {S_XT, xt, (size_t)m, &dxt},
                            {S_YT, yt, (size_t)m, &dyt}})) ||
         (rc = ensure(c, S_OUTX, m, &dout)))
-        return rc;
+        return drain_and_fail(c, rc);
     rc = potential_device(c, theta, dx, dy, dv, n, dxt, dyt, m, dout, c.ev_inputs);
     // the copies on the auxiliary stream read the caller's memory: done before returning
     const cudaError_t e = wait_stream(c, c.aux);
@@ -517,7 +525,7 @@ static int force_host(Context &c, double theta, const double *xs, const double *
                               {S_H, hs, (size_t)nb, &dh}},
                           {{S_VIN, vs, (size_t)n, &dv}})) ||
         (rc = ensure(c, S_OUTX, nt, &dox)) || (rc = ensure(c, S_OUTY, nt, &doy)))
-        return rc;
+        return drain_and_fail(c, rc);
     // the outputs come back run by run while later runs are evaluated (force_mrag)
     rc = force_device(c, theta, dx, dy, dv, n, d0x, d0y, dh, nb, dox, doy, c.ev_inputs, xo, yo);
     const cudaError_t e = wait_stream(c, c.aux);
@@ -640,6 +648,18 @@ TC_API int tc_set_host_waits(tc_context *ctx, int sleeping) {
         return TC_ERR_INVALID;
     }
     ctx->c.sleeping_waits = sleeping != 0;
+    return TC_OK;
+}
+
+TC_API int tc_set_wait_test(tc_context *ctx, int stall, int spin_limit, int stack_limit) {
+    clear_error();
+    if (!ctx || stall < TC_STALL_NONE || stall > TC_STALL_TREE) {
+        set_error(TC_ERR_INVALID, "invalid wait test setting (stall %d)", stall);
+        return TC_ERR_INVALID;
+    }
+    ctx->c.test_stall = stall;
+    ctx->c.spin_limit = spin_limit > 0 ? spin_limit : DEFAULT_SPIN_LIMIT;
+    ctx->c.stack_limit = stack_limit > 0 ? stack_limit : 0;
     return TC_OK;
 }
 

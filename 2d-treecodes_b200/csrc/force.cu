@@ -110,7 +110,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
     const double *__restrict__ hs, double theta, const TNode *__restrict__ tnode, int nnodes,
     int *__restrict__ counts, const int *__restrict__ offs, int *__restrict__ lists,
     int *__restrict__ scratch, ScratchLayout sl, int *__restrict__ sstart, int *meta,
-    unsigned *err, unsigned long long *stats) {
+    unsigned *err, unsigned long long *stats, int stack_cap) {
     constexpr bool FILL = MODE == 1;
     __shared__ int stack_all[TR_WARPS][TR_STACK];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
@@ -178,7 +178,7 @@ __global__ __launch_bounds__(TR_WARPS * 32) void k_force_lists(
             }
             const unsigned bd = __ballot_sync(FULL_MASK, kind == K_DESCEND);
             const int nd4 = 4 * __popc(bd);
-            if (top + nd4 > TR_STACK) {
+            if (top + nd4 > stack_cap) {
                 if (lane == 0) atomicOr(err, DEVERR_STACK);
                 break;
             }
@@ -741,6 +741,8 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
             return rc;
     }
     unsigned long long *stats = slot_ptr<unsigned long long>(c, S_STATS);
+    // traversal stack entries per warp: all of them, or fewer as a context's test setting
+    const int stack_cap = c.stack_limit > 0 ? std::min(c.stack_limit, TR_STACK) : TR_STACK;
     TC_CUDA_TRY(cudaEventRecord(c.ev_fork, c.stream));
     {
         AuxScope on_aux(c);
@@ -748,7 +750,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         TC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(int) * 4, c.stream));
         k_force_lists<2><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
             nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, counts, nullptr, nullptr,
-            static_cast<int *>(ls.p), sl, sstart, meta, err, stats);
+            static_cast<int *>(ls.p), sl, sstart, meta, err, stats, stack_cap);
         TC_KERNEL_CHECK();
         if ((rc = exclusive_scan(c, counts, offs, 4 * nbricks))) return rc;
         for (int k = 0; k < 4; ++k)
@@ -787,7 +789,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         } else {
             k_force_lists<1><<<trgrid, TR_WARPS * 32, 0, c.stream>>>(
                 nbricks, L, x0s, y0s, hs, theta, tnode, c.nnodes, nullptr, offs, lists, nullptr,
-                sl, nullptr, nullptr, err, nullptr);
+                sl, nullptr, nullptr, err, nullptr, stack_cap);
         }
         TC_KERNEL_CHECK();
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));

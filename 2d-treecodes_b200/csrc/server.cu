@@ -204,7 +204,10 @@ Job *tc_server::pick(int slot, size_t *reserve, tc_context **ctx) {
             if (ci != clients.end() && ci->second.busy) continue;
         }
         const size_t held = k > 0 ? (clients.count(k) ? clients[k].bytes : 0) : pool_bytes[slot];
-        const size_t est = (size_t)((double)j->estimate * ratio[j->req.kind]);
+        // the charge: the estimate scaled by the learned actual/estimate ratio, at most the
+        // whole budget, so that admitting it never charges more than the budget
+        const size_t est =
+            std::min(budget, (size_t)((double)j->estimate * ratio[j->req.kind]));
         const size_t need = est > held ? est - held : 0;
         if (j->estimate > budget) {
             // can never fit: fail it without running

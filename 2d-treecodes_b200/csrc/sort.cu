@@ -183,7 +183,7 @@ constexpr int RS_RADIX = 256;
 constexpr unsigned RS_FLAG_AGG = 1u << 30;
 constexpr unsigned RS_FLAG_INC = 2u << 30;
 constexpr unsigned RS_VALMASK = (1u << 30) - 1;
-constexpr int RS_SPIN_LIMIT = 1 << 22;
+constexpr int RS_SPIN_LIMIT = DEFAULT_SPIN_LIMIT;
 constexpr int RS_MAX_PASSES = 4;
 
 // Histograms of every 8-bit digit of the keys, in one read.
@@ -232,10 +232,11 @@ __device__ __forceinline__ unsigned digit_peers(unsigned vmask, int d) {
 // statuses of LB_WINDOW predecessors are read at once (independent loads, each coalesced over
 // the CTA's digit threads), which cuts the walk of ~17 dependent L2 round trips measured on
 // 16M keys to ~6.  A predecessor that has published nothing yet is read again from there; the
-// number of reads without progress is bounded (DEVERR_SPIN_LIMIT).
+// number of reads without progress is bounded by `spin_limit` (DEVERR_SPIN_LIMIT).
 constexpr int LB_WINDOW = 4;
 
-__device__ __forceinline__ int lookback(const unsigned *status, int tile, int d, unsigned *err) {
+__device__ __forceinline__ int lookback(const unsigned *status, int tile, int d, unsigned *err,
+                                        int spin_limit = RS_SPIN_LIMIT) {
     int excl = 0;
     int spins = 0;
     int j = tile - 1;
@@ -259,7 +260,7 @@ __device__ __forceinline__ int lookback(const unsigned *status, int tile, int d,
             if (flag == RS_FLAG_INC) return excl;
         }
         j -= used;
-        if (used == 0 && ++spins > RS_SPIN_LIMIT) {
+        if (used == 0 && ++spins > spin_limit) {
             atomicOr(err, DEVERR_SPIN_LIMIT);
             break;
         }
@@ -444,6 +445,8 @@ __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
 // (256 threads x 12, four CTAs per SM); the tile's digit counts, then the global digit offsets
 // by decoupled look-back, then the stable rank within each warp from digit ballots; items are
 // placed in sorted order in shared memory and written out in runs of equal digits.
+// `stall_tile` (a test setting, -1 otherwise) names a tile that publishes nothing, so that the
+// tiles after it wait until `spin_limit` and report DEVERR_SPIN_LIMIT.
 constexpr int PS_THREADS = 256;
 constexpr int PS_WARPS = PS_THREADS / 32;
 constexpr int PS_ITEMS = 12;
@@ -452,7 +455,7 @@ constexpr int PS_TILE = PS_THREADS * PS_ITEMS;
 __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
     const unsigned long long *__restrict__ in, unsigned long long *__restrict__ out, int n,
     int shift, const int *__restrict__ digit_offsets, unsigned *status, int *tile_counter,
-    unsigned *err) {
+    unsigned *err, int spin_limit, int stall_tile) {
     __shared__ unsigned long long s_items[PS_TILE];
     __shared__ int s_whist[PS_WARPS][RS_RADIX];
     __shared__ int s_count[RS_RADIX];
@@ -486,13 +489,14 @@ __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
     __syncthreads();
     const int total = s_count[d];
     unsigned *mine = status + (size_t)tile * RS_RADIX + d;
+    const bool publish = tile != stall_tile;
     int excl = 0;
     if (tile == 0) {
-        atomicExch(mine, RS_FLAG_INC | (unsigned)total);
+        if (publish) atomicExch(mine, RS_FLAG_INC | (unsigned)total);
     } else {
-        atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
-        excl = lookback(status, tile, d, err);
-        atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
+        if (publish) atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
+        excl = lookback(status, tile, d, err, spin_limit);
+        if (publish) atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
     }
 
     const unsigned lt = lanemask_lt();
@@ -811,10 +815,13 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
         const bool odd = p & 1;
         k_onesweep_items<<<ntiles, PS_THREADS, 0, c.stream>>>(
             odd ? items_b : items_a, odd ? items_a : items_b, n, 32 + 8 * p,
-            offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err);
+            offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err,
+            c.spin_limit, p == 0 && c.test_stall == TC_STALL_SORT ? 0 : -1);
         TC_KERNEL_CHECK();
     }
     c.nsrc = n;
+    // a test stall leaves the passes' output unordered: report it before anything reads it
+    if (c.test_stall == TC_STALL_SORT && (rc = check_device_errors(c, "source sort"))) return rc;
     if (values_ready) {
         // the keys now (the tree needs nothing else); x/y/v in finish_sources
         k_items_split<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(items_a, n, keys, perm);

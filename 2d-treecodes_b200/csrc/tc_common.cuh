@@ -41,6 +41,10 @@ struct Frame {
 
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
+// Reads without progress after which a device wait on another CTA's published state gives up
+// and raises DEVERR_SPIN_LIMIT (a context's test setting can lower it, tc_set_wait_test).
+constexpr int DEFAULT_SPIN_LIMIT = 1 << 22;
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

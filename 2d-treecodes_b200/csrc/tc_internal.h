@@ -147,6 +147,11 @@ struct Context {
     // host waits of a solve: spin in the CUDA call (false) or poll and sleep (wait_stream)
     bool sleeping_waits = false;
     bool live = false;                    // counted among the device's live contexts
+    // test settings (tc_set_wait_test): a look-back tile that never publishes (TC_STALL_*),
+    // the bound of the device waits, and the force traversal's stack capacity (0: full)
+    int test_stall = TC_STALL_NONE;
+    int spin_limit = DEFAULT_SPIN_LIMIT;
+    int stack_limit = 0;
     bool timing = false;
     cudaEvent_t ev[8] = {};
     PhaseTimes times = {};

@@ -26,10 +26,10 @@ constexpr BinomTable make_binom_table() {
 // (arguments r^2 + 10 eps or |z|^2 of a far cell, never zero, subnormal or infinite).  From the
 // mathematics: x = 2^e m with m in [sqrt(1/2), sqrt(2)), s = (m - 1) / (m + 1), and
 // log m = 2 atanh s = 2 s (1 + s^2 q(s^2)), q(z) = (atanh(sqrt z) / sqrt z - 1) / z; log x =
-// e ln 2 + log m, with ln 2 split into a head of 21 bits (e * head exact) and a tail.  q is a
-// degree-6 polynomial fitted here to it on Chebyshev nodes over z in [0, ((sqrt 2 - 1) /
+// e ln 2 + log m, with ln 2 split into a head of 21 bits (e * head exact) and a tail.  q is the
+// degree-6 interpolant of it at the 7 first-kind Chebyshev nodes of z in [0, ((sqrt 2 - 1) /
 // (sqrt 2 + 1))^2] (error below 2e-16, which the factor z <= 0.0295 scales to under 2^-57 of
-// log m).  The division is a refined reciprocal (rcp_nr).  About 25 instructions against the
+// log m); fit_log_poly.py beside this file regenerates the coefficients.  The division is a refined reciprocal (rcp_nr).  About 25 instructions against the
 // library log's ~100; within a few ulp of it (tests/test_gpu_parity.py checks the bound on
 // 2^20 arguments).
 __device__ __forceinline__ double log_pos(double x) {

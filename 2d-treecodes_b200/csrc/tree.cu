@@ -64,13 +64,15 @@ constexpr int TL_TILE = TL_THREADS * TL_ITEMS;
 constexpr int TL_HALO = LEAF_POTENTIAL;           // the largest leaf capacity
 constexpr int TL_STAGE = TL_TILE + 1 + TL_HALO;   // staged keys per tile
 constexpr unsigned TL_AGG = 1u << 30, TL_INC = 2u << 30, TL_VAL = (1u << 30) - 1;
-constexpr int TL_SPIN_LIMIT = 1 << 22;
+// `stall_tile` (a test setting, -1 otherwise) names a tile that publishes nothing, so that the
+// tile after it waits until `spin_limit` and reports DEVERR_SPIN_LIMIT.
 
 __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict__ keys, int n,
                                                           int leafcap, int cap, unsigned *status,
                                                           int *tile_counter, int *__restrict__ lpos,
                                                           unsigned short *__restrict__ lmask,
-                                                          int *nlist_out, unsigned *err) {
+                                                          int *nlist_out, unsigned *err,
+                                                          int spin_limit, int stall_tile) {
     __shared__ int s_tile, s_excl;
     // the tile's keys with one before and leafcap after, staged by coalesced loads; word q is
     // kept at q + q / 32 so that the 16-source runs of a warp's threads hit distinct banks
@@ -118,11 +120,12 @@ __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict_
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         unsigned *mine = status + tile;
+        const bool publish = tile != stall_tile;
         int excl = 0;
         if (tile == 0) {
-            if (lane == 0) atomicExch(mine, TL_INC | (unsigned)total);
+            if (lane == 0 && publish) atomicExch(mine, TL_INC | (unsigned)total);
         } else {
-            if (lane == 0) atomicExch(mine, TL_AGG | (unsigned)total);
+            if (lane == 0 && publish) atomicExch(mine, TL_AGG | (unsigned)total);
             int j = tile - 1, spins = 0;
             for (;;) {
                 const int jj = j - lane;
@@ -139,7 +142,7 @@ __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict_
                     const int first_none = __ffs(none & upto) - 1;
                     excl += __reduce_add_sync(FULL_MASK, lane < first_none ? st & TL_VAL : 0u);
                     j -= first_none;
-                    if (first_none == 0 && ++spins > TL_SPIN_LIMIT) {
+                    if (first_none == 0 && ++spins > spin_limit) {
                         if (lane == 0) atomicOr(err, DEVERR_SPIN_LIMIT);
                         break;
                     }
@@ -149,7 +152,7 @@ __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict_
                 if (inc) break;
                 j -= 32;
             }
-            if (lane == 0) atomicExch(mine, TL_INC | (unsigned)(excl + total));
+            if (lane == 0 && publish) atomicExch(mine, TL_INC | (unsigned)(excl + total));
         }
         if (lane == 0) {
             s_excl = excl;
@@ -370,8 +373,11 @@ int build_topology(Context &c, int leafcap) {
     TC_CUDA_TRY(cudaMemsetAsync(tl_status, 0, sizeof(unsigned) * ntl, c.stream));
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     k_tree_list<<<ntl, TL_THREADS, 0, c.stream>>>(keys, n, leafcap, cap, tl_status, tl_counter,
-                                                   lpos, lmask, d_nlist, err);
+                                                   lpos, lmask, d_nlist, err, c.spin_limit,
+                                                   c.test_stall == TC_STALL_TREE ? 0 : -1);
     TC_KERNEL_CHECK();
+    // a test stall leaves the list offsets wrong: report it before anything reads them
+    if (c.test_stall == TC_STALL_TREE && (rc = check_device_errors(c, "tree build"))) return rc;
     k_rank_count<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk);
     TC_KERNEL_CHECK();
     k_rank_scan<<<LMAX, 1024, 0, c.stream>>>(blkc, nblk, totals);

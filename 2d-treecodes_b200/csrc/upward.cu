@@ -18,12 +18,18 @@
 //    (l0 + l1) + (l2 + l3); a lane whose own weight sum is zero measures the radius about the
 //    origin (upward-common.ispc:44-45 tests the varying wsum);
 //  * leaf com = wx/w, or the cell centre fma(0.5, h, fma(cx, h, xmin)) when w == 0;
-//  * parent sums over children as (c0 + c3) + (c1 + c2), the order the compiled driver uses;
+//  * parent sums over children as (c0 + c3) + (c1 + c2): the reference's source adds c0..c3 in
+//    sequence (upward.cpp:105-115), and this is the reassociation g++ -O3 --fast-math (the
+//    reference's release flags) makes of that loop in the compiled driver the parity tests
+//    run against; a build of the reference without fast-math would sum in sequence;
 //  * parent radius min(max_c (sqrt(fma(rx, rx, ry*ry)) + r_c), (double)1.4143f * ext / 2^l)
 //    over children with nonzero weight;
 //  * when all four children are negligible (|w| < 1.1e-16) the parent's expansion is zeroed and
-//    child 3 -- the last child to arrive in the reference's sequential subtree order -- becomes
-//    an empty leaf (upward.cpp:173-180); with exactly three negligible children the remaining
+//    the child that arrives last becomes an empty leaf (upward.cpp:173-180).  Which child that
+//    is depends on the reference's OpenMP task timing; below the task threshold (5000 sources
+//    per cell, upward.cpp:271) its subtrees complete in child order, so it is child 3, which is
+//    what this code always picks (the oracle fixtures take that serial path); with exactly
+//    three negligible children the remaining
 //    child's coefficients are copied unshifted (upward.cpp:182-188).
 // The expansion coefficients themselves are sums whose order is free (the parity gate on them
 // is a relative tolerance), so P2E and E2E use whatever order suits the GPU.

@@ -41,6 +41,7 @@ SIGNATURES = {
     "tc_context_destroy": (None, [_vp]),
     "tc_set_precision": (_i, [_vp, _i]),
     "tc_set_host_waits": (_i, [_vp, _i]),
+    "tc_set_wait_test": (_i, [_vp, _i, _i, _i]),
     "tc_release_cached_memory": (_i, [_i]),
     "tc_set_orders": (_i, [_vp, _i, _i]),
     "tc_supported_orders": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
@@ -250,6 +251,14 @@ class Context:
         """0: the solving thread spins while the device works (lowest latency); 1: it polls
         and sleeps, leaving the host core to other threads."""
         _check(self.lib.tc_set_host_waits(self.h, int(sleeping)))
+
+    def set_wait_test(self, stall=0, spin_limit=0, stack_limit=0):
+        """Test settings: `stall` 1 (source sort) or 2 (tree build) makes one look-back tile
+        publish nothing, so the next one's bounded wait runs out (TC_ERR_TIMEOUT); `spin_limit`
+        bounds the device waits (0: the default); `stack_limit` caps the force traversal stack
+        per warp (0: all of it; exceeding it gives TC_ERR_CAPACITY).  No argument restores the
+        defaults."""
+        _check(self.lib.tc_set_wait_test(self.h, int(stall), int(spin_limit), int(stack_limit)))
 
     def set_orders(self, potential_order=ORDER_POTENTIAL, force_order=ORDER_FORCE):
         """Expansion orders of the next solves (the reference's build-time potential-order and

@@ -16,9 +16,12 @@ form measured on the same inputs (`plain_fp64`), so the mixed-vs-FP64 ratio is i
   roofline  the evaluation kernel (k_force_eval): algorithmic flops per launch / its event time,
             against the measured FMA throughput of this GPU (FP64, or FP32 for the mixed form);
             DRAM traffic per launch from the committed ncu capture
-  cpu_baseline  the reference's drivers (oracle/_ref) on the host cores, bounded sample
+  e2e_fp64  the plain FP64 form through the reference-compatible treecode_force_mrag, host
+            buffers: the matched-precision figure against the reference arm
+  cpu_baseline  the reference's drivers (oracle/_ref) on the host cores: whole calls, measured
 
---impl reference times the reference's own CPU implementation instead (rank 0 only).
+--impl reference times the reference's own CPU implementation instead (rank 0 only): one
+whole treecode_force_mrag call per step on every host core.
 Multi-GPU (torchrun): every rank solves its own independent copy of the workload (weak
 scaling, seeds differ by rank); only the timing barrier/max-reduction is collective.
 """
@@ -48,6 +51,7 @@ ORDER_FORCE = 24
 PHASES = ("sort_ms", "tree_ms", "upward_ms", "lists_ms", "eval_ms", "total_ms", "eval_kernel_ms")
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_force_eval.vortex_sheet_force.txt")
 PROFILE_TRAFFIC_MIXED = os.path.join(ROOT, "profiles", "k_force_eval.mixed.vortex_sheet_force.txt")
+L2_BYTES = 126 << 20
 
 
 def parse_args():
@@ -64,8 +68,8 @@ def parse_args():
                    help="only `warmup` + `steps` device solves and a timing line (for profilers)")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     p.add_argument("--theta", type=float, default=None, help="override the workload's theta")
-    p.add_argument("--serving-requests", type=int, default=400,
-                   help="requests of the serving stream (the full stream has 2000)")
+    p.add_argument("--serving-requests", type=int, default=2000,
+                   help="requests of the serving stream")
     p.add_argument("--serving-rate", type=float, default=200.0, help="Poisson arrival rate, 1/s")
     p.add_argument("--serving-slots", type=int, default=4)
     p.add_argument("--serving-budget-gb", type=float, default=40.0)
@@ -224,14 +228,14 @@ def _capture_stdout(fn):
     return out, text
 
 
-def cpu_reference_step(w, sample_blocks=512, sample_targets=1 << 19):
-    """One bounded step of the reference's CPU implementation (oracle/_ref: the reference's
-    drivers compiled verbatim + the restated ISPC kernels, node capacity raised for large
-    inputs, OpenMP on every host core).  force_mrag: the full tree build plus the evaluation of
-    `sample_blocks` evenly strided blocks, the evaluation (the driver's own DW timer) scaled to
-    all blocks.  potential: the tree build alone (no targets) and the build plus an evenly
-    strided sample of `sample_targets` targets; the difference is scaled to all targets.
-    Returns (seconds for the full workload, description)."""
+def cpu_reference_step(w, sample_targets=1 << 19):
+    """One step of the reference's CPU implementation (oracle/_ref: the reference's drivers
+    compiled verbatim + the restated ISPC kernels, node capacity raised for large inputs,
+    OpenMP on every host core).  force_mrag: one whole call over all sources and all blocks,
+    timed by the wall clock (measured, nothing scaled).  potential (a sample, since a 4M-target
+    call takes seconds to tens of seconds): the tree build alone (no targets) and the build
+    plus an evenly strided sample of `sample_targets` targets; the difference is scaled to all
+    targets.  Returns (seconds for the full workload, description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O  # the checker / CPU baseline only
     if w["kind"] == "potential":
@@ -254,29 +258,38 @@ def cpu_reference_step(w, sample_blocks=512, sample_targets=1 << 19):
                 f"scaled by {m}/{len(idx)}")
         return full, desc
     nb = len(w["x0s"])
-    stride = max(1, nb // sample_blocks)
-    idx = np.arange(0, nb, stride)[:sample_blocks]
 
     def run():
         t0 = time.perf_counter()
-        O.force_mrag(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"][idx], w["y0s"][idx],
-                     w["hs"][idx], mode="big")
+        O.force_mrag(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"], w["hs"],
+                     mode="big")
         return time.perf_counter() - t0
 
     wall, text = _capture_stdout(run)
     # drivers/treecode-force.cpp:234 prints "UP: <s>s DW: <s>s" (tree build + upward pass,
-    # then the evaluation of the requested blocks)
+    # then the evaluation of the blocks); reported beside the measured wall time
     mt = re.findall(r"UP:\s*([0-9.eE+-]+)s\s+DW:\s*([0-9.eE+-]+)s", text)
-    if not mt:
-        raise RuntimeError("the reference driver printed no UP/DW timers")
-    evals = float(mt[-1][1])
-    build = wall - evals
-    full = build + evals * nb / len(idx)
-    desc = (f"tree build + upward pass of all {len(w['xs'])} sources, evaluation of {len(idx)} "
-            f"of {nb} blocks (every {stride}th) scaled by {nb}/{len(idx)}; the evaluation time "
-            f"is the reference driver's own DW timer ({evals:.3f} s), the rest is wall time "
-            f"({build:.2f} s)")
-    return full, desc
+    split = (f"; the driver's own timers: UP {float(mt[-1][0]):.3f} s, DW {float(mt[-1][1]):.3f} s"
+             if mt else "")
+    desc = (f"one whole treecode_force_mrag call: tree build + upward pass of all "
+            f"{len(w['xs'])} sources and the evaluation of all {nb} blocks, wall time "
+            f"{wall:.3f} s (measured, not scaled){split}")
+    return wall, desc
+
+
+def bench_config(w, precision, flush_desc):
+    """The `config` object of both arms: the same keys, only `precision` differs."""
+    return {"workload": w["name"], "theta": w["theta"],
+            "order": ORDER_FORCE if w["kind"] == "force" else 12,
+            "sources": len(w["xs"]), "targets": n_targets(w), "precision": precision,
+            "l2": flush_desc}
+
+
+def l2_desc(w):
+    in_bytes = sum(int(a.nbytes) for a in w.values() if isinstance(a, np.ndarray))
+    if in_bytes >= 2 * L2_BYTES:
+        return f"inputs larger than L2 ({in_bytes / 1e6:.0f} MB per step)"
+    return f"L2 flushed before every timed step (inputs {in_bytes / 1e6:.1f} MB)"
 
 
 def run_reference(args, ws, rank):
@@ -297,10 +310,8 @@ def run_reference(args, ws, rank):
         "impl": "reference", "metric": METRIC, "value": val, "unit": "Mtargets/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded PCG64)",
-        "config": {"workload": w["name"], "theta": w["theta"],
-                   "order": ORDER_FORCE if w["kind"] == "force" else 12,
-                   "sources": len(w["xs"]), "targets": n_targets(w), "precision": "fp64"},
+        "data": "synthetic (seeded PCG64; the reference's datasets are not available)",
+        "config": bench_config(w, "fp64", l2_desc(w)),
         "cpu_baseline": {"value": val, "unit": "Mtargets/s", "cores": cores, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": val, "unit": "Mtargets/s", "h2d_bytes_per_step": 0,
@@ -351,9 +362,8 @@ def run_b200(args, ws, rank, local):
         return 0
 
     in_bytes = sum(int(a.nbytes) for a in w.values() if isinstance(a, np.ndarray))
-    l2_bytes = 126 << 20
-    flush = (torch.zeros((2 * l2_bytes) // 8, dtype=torch.float64, device=dev)
-             if in_bytes < 2 * l2_bytes else None)
+    flush = (torch.zeros((2 * L2_BYTES) // 8, dtype=torch.float64, device=dev)
+             if in_bytes < 2 * L2_BYTES else None)
 
     def timed(precision, steps, sample_clocks=False):
         """Device time per step of `steps` solves (CUDA events on the library's stream, max over
@@ -513,13 +523,22 @@ def run_b200(args, ws, rank, local):
                + " (C ABI, host pointers, FP64)",
                "value": ws * m / (e2e_ref_ms * 1e-3) / 1e6, "ms_per_step": e2e_ref_ms}}
 
-    # ---- CPU baseline (rank 0, N = 1)
+    e2e_fp64 = {"value": ws * m / (e2e_ref_ms * 1e-3) / 1e6, "unit": "Mtargets/s",
+                "ms_per_step": e2e_ref_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": e2e["reference_entry_point"]["api"],
+                "note": "plain FP64 through the reference-compatible entry point: the "
+                        "matched-precision figure against the reference arm"}
+
+    # ---- CPU baseline (rank 0, N = 1): one untimed call, then the mean of two measured calls
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            t_full, desc = cpu_reference_step(w)
+            cpu_reference_step(w)
+            runs = [cpu_reference_step(w) for _ in range(2)]
+            t_full = sum(t for t, _ in runs) / len(runs)
             cpu = {"value": m / t_full / 1e6, "unit": "Mtargets/s", "cores": os.cpu_count(),
-                   "kind": "reference", "sample": desc}
+                   "kind": "reference",
+                   "sample": f"mean of 2 calls after 1 untimed; last: {runs[-1][1]}"}
         except Exception as exc:  # the oracle libraries are built in the source container
             cpu = {"value": None, "unit": "Mtargets/s", "cores": os.cpu_count(),
                    "kind": "reference", "sample": f"unavailable: {exc}"}
@@ -536,16 +555,12 @@ def run_b200(args, ws, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if mixed else "f64",
             "data": "synthetic (seeded PCG64; the reference's datasets are not available)",
-            "config": {"workload": w["name"], "theta": w["theta"],
-                       "order": ORDER_FORCE if kind == "force" else 12,
-                       "sources": len(w["xs"]), "targets": m, "precision": args.precision,
-                       "parallelism": f"{ws} independent solves (one per GPU)",
-                       "l2": (f"inputs larger than L2 ({in_bytes / 1e6:.0f} MB per step)"
-                              if flush is None else
-                              f"L2 flushed before every timed step (inputs {in_bytes / 1e6:.1f} MB)")},
+            "config": bench_config(w, args.precision, l2_desc(w)),
+            "parallelism": f"{ws} independent solves (one per GPU)",
             "accuracy": acc,
             "plain_fp64": other,
             "e2e": e2e,
+            "e2e_fp64": e2e_fp64,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -78,6 +78,9 @@ typedef struct tc_context tc_context;
 
 typedef enum { TC_PRECISION_FP64 = 0, TC_PRECISION_MIXED = 1 } tc_precision;
 
+/* Stages whose first look-back tile can be told never to publish (tc_set_wait_test). */
+typedef enum { TC_STALL_NONE = 0, TC_STALL_SORT = 1, TC_STALL_TREE = 2 } tc_stall;
+
 typedef struct {
     /* phase times in ms (filled when timing is enabled) */
     float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms;
@@ -102,6 +105,22 @@ TC_API int tc_set_precision(tc_context *ctx, int precision);
  * call, the lowest latency; 1 polls every 20 us and sleeps in between, which leaves the host core
  * to other threads (the request server's slots wait this way). */
 TC_API int tc_set_host_waits(tc_context *ctx, int sleeping);
+/* Test settings that make the library's bounded device waits and capacities run out on
+ * purpose, so that their error paths can be exercised without faulting or hanging a GPU (no
+ * counterpart in the reference, whose overflows are silent, drivers/upward.cpp:253).
+ *   stall:       TC_STALL_SORT / TC_STALL_TREE: in the source sort's first radix pass, or in
+ *                the tree build's list pass, tile 0 publishes nothing, so the tile after it
+ *                waits on it until the spin limit, raises the device error flag and moves on;
+ *                the solve then stops after that stage with TC_ERR_TIMEOUT.  Needs more
+ *                sources than one tile (3072 for the sort, 4096 for the tree).
+ *   spin_limit:  reads without progress after which a device wait gives up (<= 0: the default,
+ *                4,194,304).
+ *   stack_limit: traversal stack entries per warp of the force lists (<= 0: all 2048); a walk
+ *                that would exceed it stops with the lists so far and the solve returns
+ *                TC_ERR_CAPACITY.
+ * tc_set_wait_test(ctx, TC_STALL_NONE, 0, 0) restores the defaults; the context stays usable
+ * after every such failure. */
+TC_API int tc_set_wait_test(tc_context *ctx, int stall, int spin_limit, int stack_limit);
 /* Expansion orders of the context's next solves: the reference fixes them when it is built
  * (Makefile:13-14 of the reference, potential-order = 12 and force-order = 24, which stay the
  * defaults here).  Any order that tc_supported_orders lists may be chosen, independently for

@@ -4,7 +4,7 @@ Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`
 module, and only as the checker / the timed CPU reference.  It loads the shared objects
 that ``oracle/Makefile`` builds into ``oracle/_ref/``:
 
-* ``libref_{potential,force}_{exact64,faithful,big}.so`` -- the reference's own drivers
+* ``libref_{potential,force}_{exact64,faithful,big,exact64_big}.so`` -- the reference's own drivers
   (drivers/treecode-potential.cpp, drivers/treecode-force.cpp, drivers/upward.cpp,
   drivers/sort-sources.cpp) compiled verbatim, linked against the restated ISPC kernels
   of ``ispc_kernels.cpp`` and the dump hooks of ``hooks.cpp``;
@@ -44,7 +44,8 @@ def available() -> bool:
 
 
 def lib(kind: str, mode: str = "exact64"):
-    """kind: 'potential' | 'force' | 'direct'; mode: 'exact64' | 'faithful' | 'big', or
+    """kind: 'potential' | 'force' | 'direct'; mode: 'exact64' | 'faithful' | 'big' (faithful
+    kernels, node capacity raised) | 'exact64_big' (EXACT64 kernels, node capacity raised), or
     'exact64_o8' / 'exact64_o16' / 'exact64_o28' (the EXACT64 build at that expansion order),
     'exact64_b16' / 'exact64_b64' (force, the EXACT64 build with that MRAG block side)."""
     key = (kind, mode)
@@ -121,7 +122,8 @@ def tree(xs, ys, vs, kind="potential", mode="exact64", leafcap=None):
     n = len(xs)
     p = ORDER[kind]
     leafcap = LEAF[kind] if leafcap is None else leafcap
-    cap = 1024
+    # the node bound of the raised-capacity builds (oracle/Makefile), so one build suffices
+    cap = max(1024, int(60 * (n / (leafcap + 1.0) + 1) + 1))
     L = lib(kind, mode)
     while True:
         s = np.zeros(cap, np.int32); e = np.zeros(cap, np.int32)

@@ -92,6 +92,8 @@ def test_lamb_oseen_force_full_size(gpu_ctx):
 
 @pytest.mark.parametrize("theta", [0.3, 0.5, 0.7])
 def test_gaussian_mixture_potential_theta_sweep(gpu_ctx, theta):
+    """A quarter-million-source mixture, every target compared (the full-size 4M mixture is
+    compared on a target sample in test_gpu_fullsize.py)."""
     w = W.gaussian_mixture_potential(n=1 << 18)
     if theta == 0.5:
         live_tree_check(gpu_ctx, "potential", w)
