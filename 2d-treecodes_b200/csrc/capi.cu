@@ -277,6 +277,7 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     for (auto &ev : c.ev_chunk) TC_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_leafset, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_moments, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_near, cudaEventDisableTiming));
     c.h_pinned = pinned_area();
     if (!c.h_pinned) {
         set_error(TC_ERR_ALLOC, "page-locked host allocation failed");
@@ -308,7 +309,8 @@ static void context_free(Context &c) {
     c.live = false;
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
-    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs, c.ev_leafset, c.ev_moments})
+    for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs, c.ev_leafset, c.ev_moments,
+                           c.ev_near})
         if (ev) cudaEventDestroy(ev);
     for (auto &ev : c.ev_chunk)
         if (ev) cudaEventDestroy(ev);
@@ -331,9 +333,13 @@ static void finish_timing(Context &c) {
     float tot = 0;
     cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
     c.times.total_ms = tot;
-    float k = 0;
+    // the evaluation kernel (potential), or the far-field kernel plus the near-field one
+    // (force; the near field runs on the auxiliary stream, beside the upward pass)
+    float k = 0, nk = 0;
     cudaEventElapsedTime(&k, c.ev[6], c.ev[7]);
-    c.times.eval_kernel_ms = k;
+    if (c.near_marked) cudaEventElapsedTime(&nk, c.ev[9], c.ev[10]);
+    c.times.far_kernel_ms = c.near_marked ? k : 0.f;
+    c.times.eval_kernel_ms = k + nk;
 }
 
 // Sort, topology and upward pass for `kind` (0 potential, 1 force).
@@ -344,6 +350,7 @@ static int build_tree_moments(Context &c, int kind, const double *x, const doubl
                               const double *v, int n, cudaEvent_t values_ready = nullptr) {
     int rc;
     g_launches = 0;
+    c.near_marked = false;
     TC_CUDA_TRY(cudaMemsetAsync(slot_ptr<unsigned>(c, S_ERR), 0, sizeof(unsigned), c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(c.buf[S_STATS].p, 0, STAT_SLOTS * sizeof(unsigned long long),
                                 c.stream));
@@ -764,6 +771,7 @@ TC_API int tc_get_stats(tc_context *ctx, tc_stats *out) {
     out->launches = c.counts.launches;
     out->eval_kernel_ms = c.times.eval_kernel_ms;
     out->list_walks = c.list_walks;
+    out->far_kernel_ms = c.times.far_kernel_ms;
     return TC_OK;
 }
 

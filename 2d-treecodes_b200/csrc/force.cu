@@ -1,5 +1,5 @@
-// force.cu -- treecode_force_mrag on the GPU: per-brick interaction lists, then one fused
-// far-field + near-field evaluation per 8 x 8 brick.
+// force.cu -- treecode_force_mrag on the GPU: per-brick interaction lists, then the far field
+// and the near field of every 8 x 8 brick.
 //
 // Restates drivers/treecode-force.cpp:94-199 (traversal) and kernels/force-kernels.m4
 // (P2P, E2P, E2L, L2P).  An MRAG block of 32 x 32 targets is 16 bricks of 8 x 8
@@ -15,13 +15,13 @@
 //    r_brick = 4.949747468305833 h), so every decision is the reference's.
 // 2. exclusive scan of the 3 x nbricks counts -> list offsets (E2L | E2P | P2P lists).
 // 3. k_force_lists<true>: same walk, writes node ids into the lists.
-// 4. k_force_eval: persistent warps take evaluation tasks from an atomic counter; a task is a
-//    brick's far field plus its first P2P_SEG near-field sources, or a further P2P_SEG-source
-//    segment of its near field.  2 targets per lane; local expansion from the E2L list (lane l
-//    owns coefficient l), L2P, E2P from the E2P list, P2P over the leaves of the P2P list with
-//    source tiles staged in shared memory.  Single-task bricks write straight into the
-//    ix + 32*(iy + 32*ib) layout (treecode-force.cpp:191-197); the parts of multi-task bricks
-//    are added in task order by k_force_gather_parts, so results are deterministic.
+// 4. k_force_far: persistent warps over bricks, 2 targets per lane; local expansion from the
+//    E2L list (lane l owns coefficient l), L2P, E2P from the E2P list, written into the
+//    ix + 32*(iy + 32*ib) layout (treecode-force.cpp:191-197).
+// 5. k_force_near: persistent warps over tasks, a task being a segment of at most P2P_SEG
+//    sources of a brick's P2P list; P2P over the listed leaves with source tiles staged in
+//    shared memory.  Single-task bricks add their sums to the outputs; the parts of multi-task
+//    bricks are added in task order by k_force_gather_parts, so results are deterministic.
 #include <cfloat>
 
 #include "tc_internal.h"
@@ -237,20 +237,63 @@ __global__ __launch_bounds__(256) void k_force_lists_copy(int nbricks,
 }
 
 // ------------------------------------------------------------------------------ evaluation
+// The far field and the near field are two kernels, each with its own register budget: the
+// far field keeps the FP64 E2L binomials in registers, the near field runs at a higher
+// occupancy.
+//  * k_force_far: persistent warps take bricks from an atomic counter; per brick the local
+//    expansion from the E2L list (lane l owns coefficient l), L2P, and E2P over the E2P list,
+//    2 targets per lane, written to the outputs at ix + 32*(iy + 32*ib)
+//    (treecode-force.cpp:191-197).
+//  * k_force_near: persistent warps take tasks from an atomic counter; a task is a segment of
+//    at most P2P_SEG sources of a brick's P2P list, so that the few bricks on a dense region do
+//    not serialise the kernel.  Source tiles are staged in shared memory, the next tile loaded
+//    into registers meanwhile.  A brick with one task adds its near field to the output; the
+//    tasks of a multi-task brick write partial sums that k_force_gather_parts adds to the
+//    output in task order, so results are deterministic.
 constexpr int EV_WARPS = 4;
 constexpr int EV_CHUNK = 32;
+constexpr int NEAR_MIN_BLOCKS = 8;   // near field: at most 64 registers per thread
 
 template <int P>
-struct EvalShared {
+struct FarShared {
     cplx coef[P];                 // E2L: a_k z^-(k+1); E2P: (k+1) a_k
     cplx local[P + 1];            // local expansion L_1..L_P
-    double2 sxy[EV_CHUNK];        // P2P source tile
+    float4 coef32[P];             // mixed E2P: scaled coefficient j as (re, re, im, im)
+    float2 cf[P];                 // mixed E2L: D_k u^(k+1)
+    float4 lf[P + 1];             // mixed L2P: l M_l as (re, re, im, im)
+};
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// z^e for 0 <= e < 32 by square-and-multiply, FP32
+__device__ __forceinline__ float2 cpowf_int(float2 z, int e) {
+    float2 r = make_float2(1.f, 0.f), b = z;
+#pragma unroll
+    for (int bit = 0; bit < 5; ++bit) {
+        if (e & (1 << bit)) r = cmulf(r, b);
+        b = cmulf(b, b);
+    }
+    return r;
+}
+
+// Near-field source tile.  Plain form: the sources' x, y, v.  Mixed form: for each source k of
+// the tile its offsets from the brick's 8 target columns (dx[c][k]) and 8 target rows
+// (dy[r][k]) as floats, and its value; rows padded to 34 words so that the 8 columns (4 rows) a
+// warp reads at once fall in distinct banks.
+constexpr int NEAR_ROW = EV_CHUNK + 2;
+template <bool MIXED>
+struct NearShared {
+    double2 sxy[EV_CHUNK];
     double sv[EV_CHUNK];
-    // mixed form: scaled E2P coefficients and the P2P tile as float offsets (hi + lo) from the
-    // brick corner
-    float2 coef32[P];
-    float4 sxy32[EV_CHUNK];       // (x hi, x lo, y hi, y lo)
-    float sv32[EV_CHUNK];
+};
+template <>
+struct NearShared<true> {
+    float dx[TILE][NEAR_ROW];
+    float dy[TILE][NEAR_ROW];
+    float v[EV_CHUNK];
+    float ch[TILE], cl[TILE];     // c h as float hi + lo, c = 0..7 (the task's brick)
 };
 
 __device__ __forceinline__ float rcp_approx_f32(float x) {
@@ -274,56 +317,45 @@ __device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
     lo = (float)(v - (double)hi);
 }
 
-// MIXED = false: plain FP64.  MIXED = true: P2P and E2P in FP32 (float offsets from the brick
-// corner split into hi + lo parts, scaled multipole coefficients, compensated per-target
-// sums); the local expansion (E2L, L2P) stays FP64.
+// MIXED = false: plain FP64.  MIXED = true: E2P in FP32 on scaled multipole coefficients with
+// compensated per-target sums, the two targets of a lane side by side in paired-FP32 (f32x2)
+// registers; the local expansion (E2L, L2P) stays FP64.
 // LBS > 0: the block layout of side 2^LBS fixed at compile time (the default side 32 has its
 // own instances: the layout arithmetic on kernel arguments measured 3% slower); LBS = 0: the
 // layout L given at run time.
 template <int P, bool MIXED, int LBS>
-__global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
+__global__ __launch_bounds__(EV_WARPS * 32, MIXED ? 5 : 4) void k_force_far(
     int nbricks, BlockLayout L_arg, const double *__restrict__ x0s, const double *__restrict__ y0s,
     const double *__restrict__ hs, const TNode *__restrict__ tnode,
     const double *__restrict__ mass, const double *__restrict__ exps,
-    const int2 *__restrict__ range, const double *__restrict__ xs,
-    const double *__restrict__ ys, const double *__restrict__ vs,
     const int *__restrict__ offs, const int *__restrict__ lists, double *__restrict__ xout,
-    double *__restrict__ yout, double *__restrict__ partial, int brick_lo, int brick_hi,
-    int *task_ctr,
-    const float2 *__restrict__ sexp, const float *__restrict__ sscale,
-    const int *__restrict__ task_brick) {
+    double *__restrict__ yout, int brick_lo, int brick_hi, int *brick_ctr,
+    const float2 *__restrict__ sexp, const float *__restrict__ sscale) {
     const BlockLayout L = LBS ? BlockLayout{LBS, LBS - 3} : L_arg;
-    __shared__ EvalShared<P> shared[EV_WARPS];
+    __shared__ FarShared<P> shared[EV_WARPS];
     const int lane = lane_id(), warp = threadIdx.x >> 5;
-    EvalShared<P> &sh = shared[warp];
+    FarShared<P> &sh = shared[warp];
     const int tx = lane & 7, ty = lane >> 3;   // targets (tx, ty) and (tx, ty + 4)
-    const double eps = 10 * DBL_EPSILON;
 
-    // signed binomials of lane l = lane + 1: (-1)^k C(l+k-1, k-1), k = 1..P
-    double bsg[P];
+    // signed binomials of lane l = lane + 1: (-1)^k C(l+k-1, k-1), k = 1..P, in registers
+    // (in shared memory, for a higher occupancy, the kernel measured 18% slower); the mixed
+    // form's FP32 E2L uses them divided by k (its coefficients carry a factor k, see E2L)
+    using bsg_t = typename std::conditional<MIXED, float, double>::type;
+    bsg_t bsg[P];
     {
         const int l = lane < P ? lane + 1 : 1;
 #pragma unroll
-        for (int k = 1; k <= P; ++k)
-            bsg[k - 1] = (k & 1 ? -1.0 : 1.0) * c_binom_f.c[l + k - 1][k - 1];
+        for (int k = 1; k <= P; ++k) {
+            const double b = (k & 1 ? -1.0 : 1.0) * c_binom_f.c[l + k - 1][k - 1];
+            bsg[k - 1] = (bsg_t)(MIXED ? b / k : b);
+        }
     }
 
-    // Tasks: brick b owns tasks [toff[b], toff[b+1]) (relative to toff[0]); task 0 of a brick
-    // evaluates its far field and the first P2P_SEG near-field sources, task p > 0 the p-th
-    // segment.  Costs vary by orders of magnitude between bricks, so warps take tasks one at a
-    // time from a global counter.
-    // This launch evaluates the tasks of bricks [brick_lo, brick_hi).
-    const int *toff = offs + 3 * nbricks;
-    const int tbase = toff[0];
-    const int task_lo = toff[brick_lo] - tbase, task_hi = toff[brick_hi] - tbase;
     for (;;) {
-        int task = 0;
-        if (lane == 0) task = task_lo + atomicAdd(task_ctr, 1);
-        task = __shfl_sync(FULL_MASK, task, 0);
-        if (task >= task_hi) break;
-        const int brick = task_brick[task];
-        const int part = task - (toff[brick] - tbase);
-        const int nparts = toff[brick + 1] - toff[brick];
+        int brick = 0;
+        if (lane == 0) brick = brick_lo + atomicAdd(brick_ctr, 1);
+        brick = __shfl_sync(FULL_MASK, brick, 0);
+        if (brick >= brick_hi) break;
         int blk, bx, by;
         brick_of(L, brick, blk, bx, by);
         const double h = hs[blk];
@@ -331,9 +363,87 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
 
         // ---------------- E2L: local expansion about the brick centre (force-kernels.m4:102-155)
-        if (part == 0) {
+        if constexpr (MIXED) {
+            // FP32 on power-of-two scaled quantities: R the cell's scale, rho >= r_brick the
+            // brick's, u = R / z0, w = rho / z0, D_k = (k+1) a_k / R^(k+1) (sexp).  Scaled local
+            // coefficients M_l = L_l rho^(l-1) = (w^l / rho) [-m/l + sum_k (-1)^k C(l+k-1, k-1)
+            // (D_{k-1} / k) u^k]: an E2L cell has d > 3 r and r >= r_brick, so every term is
+            // bounded by the cell's mass times ((r + rho) / d)^(l+k) < (2/3)^(l+k) (up to the
+            // roundings of R and rho), nothing over- or underflows FP32, and the rounding errors
+            // stay relative to the terms.  Lane l - 1 forms M_l; L2P uses l M_l.
             const int beg = offs[brick], end = offs[brick + 1];
-            cplx L = {0.0, 0.0};
+            float2 Ml = make_float2(0.f, 0.f);
+            const int l = lane + 1;
+            const float minv = -1.f / (float)l;
+            int erho = 0;
+            frexp(b.rbrick, &erho);
+            const double rho = ldexp(1.0, erho);   // 2^e > r_brick
+            TNode nd_n = {};
+            double m_n = 0;
+            float sc_n = 1.f;
+            float2 c_n = make_float2(0.f, 0.f);
+            auto fetch = [&](int at) {
+                const int node = lists[at];
+                nd_n = tnode[node];
+                m_n = mass[node];
+                sc_n = sscale[node];
+                if (lane < P) c_n = sexp[(size_t)node * P + lane];
+            };
+            if (beg < end) fetch(beg);
+            for (int it = beg; it < end; ++it) {
+                const TNode nd = nd_n;
+                const float m = (float)m_n;
+                const double R = sc_n;
+                const float2 dk = c_n;
+                if (it + 1 < end) fetch(it + 1);
+                const double zx = nd.xcom - b.x0b, zy = nd.ycom - b.y0b;
+                const double iz = rcp_nr(zx * zx + zy * zy);
+                const float2 u = make_float2((float)(R * zx * iz), (float)(-R * zy * iz));
+                const float2 w = make_float2((float)(rho * zx * iz), (float)(-rho * zy * iz));
+                __syncwarp();
+                if (lane < P) sh.cf[lane] = cmulf(dk, cpowf_int(u, l));   // D_{l-1} u^l
+                __syncwarp();
+                if (lane < P) {
+                    float tr = l == 1 ? -m : m * minv, ti = 0.f;
+#pragma unroll
+                    for (int k = 0; k < P; ++k) {
+                        const float2 ck = sh.cf[k];
+                        tr = fmaf(bsg[k], ck.x, tr);
+                        ti = fmaf(bsg[k], ck.y, ti);
+                    }
+                    const float2 t = cmulf(make_float2(tr, ti), cpowf_int(w, l));
+                    Ml.x += t.x;
+                    Ml.y += t.y;
+                }
+            }
+            __syncwarp();
+            if (lane < P)
+                sh.lf[lane + 1] = make_float4(l * Ml.x, l * Ml.x, l * Ml.y, l * Ml.y);
+            __syncwarp();
+            // L2P (force-kernels.m4:157-191): sum_l l M_l (z / rho)^(l-1) / rho, the lane's two
+            // targets side by side in f32x2 registers
+            const float inv_rho = (float)(1.0 / rho);
+            const float zxr = (float)((-3.5 * h + tx * h) / rho);
+            const float2 zre = make_float2(zxr, zxr);
+            const float2 zim = make_float2((float)((-3.5 * h + ty * h) / rho),
+                                           (float)((-3.5 * h + (ty + 4) * h) / rho));
+            const float2 nzim = make_float2(-zim.x, -zim.y);
+            const float4 top = sh.lf[P];
+            float2 are = make_float2(top.x, top.y), aim = make_float2(top.z, top.w);
+#pragma unroll
+            for (int q = P - 1; q >= 1; --q) {
+                const float4 c = sh.lf[q];
+                const float2 nre = __ffma2_rn(are, zre, __ffma2_rn(aim, nzim, make_float2(c.x, c.y)));
+                aim = __ffma2_rn(are, zim, __ffma2_rn(aim, zre, make_float2(c.z, c.w)));
+                are = nre;
+            }
+            ax0 += (double)(are.x * inv_rho);
+            ay0 -= (double)(aim.x * inv_rho);
+            ax1 += (double)(are.y * inv_rho);
+            ay1 -= (double)(aim.y * inv_rho);
+        } else {
+            const int beg = offs[brick], end = offs[brick + 1];
+            cplx Lc = {0.0, 0.0};
             const int l = lane + 1;
             const double minv = -1.0 / l;
             // the next cell is loaded while the current one is used
@@ -372,16 +482,14 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
                         tr = fma(bsg[k], ck.re, tr);
                         ti = fma(bsg[k], ck.im, ti);
                     }
-                    L = cfma({tr, ti}, zl, L);
+                    Lc = cfma({tr, ti}, zl, Lc);
                 }
                 __syncwarp();
             }
-            if (lane < P) sh.local[lane + 1] = L;
+            if (lane < P) sh.local[lane + 1] = Lc;
             __syncwarp();
-        }
 
-        // ---------------- L2P (force-kernels.m4:157-191): sum_l l L_l z^(l-1), z about the centre
-        if (part == 0) {
+            // L2P (force-kernels.m4:157-191): sum_l l L_l z^(l-1), z about the centre
             const double xr = -3.5 * h + tx * h;
             const double yr0 = -3.5 * h + ty * h, yr1 = -3.5 * h + (ty + 4) * h;
             cplx acc0 = {P * sh.local[P].re, P * sh.local[P].im}, acc1 = acc0;
@@ -399,9 +507,10 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
         }
 
         // ---------------- E2P (force-kernels.m4:57-98): w = m/z - sum (j+1) a_j z^-(j+2)
-        if (MIXED && part == 0) {
+        if (MIXED) {
             // FP32: u = 1/z, u' = R u with R the cell's power-of-two radius, scaled coefficients
-            // D_j = (j+1) a_j / R^(j+1), w = u (m - u' Q(u')), Q(u') = sum_j D_j u'^j
+            // D_j = (j+1) a_j / R^(j+1), w = u (m - u' Q(u')), Q(u') = sum_j D_j u'^j; the
+            // Horner steps of the lane's two targets run side by side in f32x2 registers
             const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
             float hx0 = 0, lx0 = 0, hy0 = 0, ly0 = 0, hx1 = 0, lx1 = 0, hy1 = 0, ly1 = 0;
             TNode nd_n = {};
@@ -420,7 +529,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
                 const TNode nd = nd_n;
                 const float m = (float)m_n, R = sc_n;
                 __syncwarp();
-                if (lane < P) sh.coef32[lane] = c_n;
+                if (lane < P) sh.coef32[lane] = make_float4(c_n.x, c_n.x, c_n.y, c_n.y);
                 __syncwarp();
                 if (it + 1 < end) fetch(it + 1);
                 const float rx = (float)((b.xlo - nd.xcom) + tx * h);
@@ -430,15 +539,18 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
                 const float i1 = rcp_approx_f32(rx * rx + ry1 * ry1);
                 const float2 u0 = make_float2(rx * i0, -ry0 * i0), u1 = make_float2(rx * i1, -ry1 * i1);
                 const float2 v0 = make_float2(R * u0.x, R * u0.y), v1 = make_float2(R * u1.x, R * u1.y);
-                float2 q0 = sh.coef32[P - 1], q1 = q0;
+                const float2 vre = make_float2(v0.x, v1.x), vim = make_float2(v0.y, v1.y);
+                const float2 nvim = make_float2(-v0.y, -v1.y);
+                const float4 top = sh.coef32[P - 1];
+                float2 qre = make_float2(top.x, top.y), qim = make_float2(top.z, top.w);
 #pragma unroll
                 for (int j = P - 2; j >= 0; --j) {
-                    const float2 dj = sh.coef32[j];
-                    q0 = make_float2(fmaf(q0.x, v0.x, fmaf(-q0.y, v0.y, dj.x)),
-                                     fmaf(q0.x, v0.y, fmaf(q0.y, v0.x, dj.y)));
-                    q1 = make_float2(fmaf(q1.x, v1.x, fmaf(-q1.y, v1.y, dj.x)),
-                                     fmaf(q1.x, v1.y, fmaf(q1.y, v1.x, dj.y)));
+                    const float4 d = sh.coef32[j];
+                    const float2 nre = __ffma2_rn(qre, vre, __ffma2_rn(qim, nvim, make_float2(d.x, d.y)));
+                    qim = __ffma2_rn(qre, vim, __ffma2_rn(qim, vre, make_float2(d.z, d.w)));
+                    qre = nre;
                 }
+                const float2 q0 = make_float2(qre.x, qim.x), q1 = make_float2(qre.y, qim.y);
                 const float t0x = m - (v0.x * q0.x - v0.y * q0.y), t0y = -(v0.x * q0.y + v0.y * q0.x);
                 const float t1x = m - (v1.x * q1.x - v1.y * q1.y), t1y = -(v1.x * q1.y + v1.y * q1.x);
                 two_sum_acc(hx0, lx0, u0.x * t0x - u0.y * t0y);
@@ -450,8 +562,7 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             ay0 += (double)hy0 + (double)ly0;
             ax1 += (double)hx1 + (double)lx1;
             ay1 += (double)hy1 + (double)ly1;
-        }
-        if (!MIXED && part == 0) {
+        } else {
             const int beg = offs[nbricks + brick], end = offs[nbricks + brick + 1];
             // the next cell's record and coefficients are loaded while the current one is used
             TNode nd_n = {};
@@ -498,101 +609,158 @@ __global__ __launch_bounds__(EV_WARPS * 32) void k_force_eval(
             }
         }
 
-        // ---------------- P2P (force-kernels.m4:15-55): sum v (xr, yr) / (xr^2 + yr^2 + eps)
-        {
-            const int beg = offs[2 * nbricks + brick], end = offs[2 * nbricks + brick + 1];
+        // added to the near field that k_force_near (and k_force_gather_parts) wrote
+        const size_t o0 = target_index(L, blk, bx, by, tx, ty);
+        const size_t o1 = o0 + ((size_t)4 << L.lbs);
+        xout[o0] += ax0;
+        yout[o0] += ay0;
+        xout[o1] += ax1;
+        yout[o1] += ay1;
+        __syncwarp();
+    }
+}
+
+// P2P (force-kernels.m4:15-55): sum v (xr, yr) / (xr^2 + yr^2 + eps) over the sources of a
+// task's segment.  MIXED = true: FP32 pairs on offsets from the brick corner (each source's
+// offset to every target column and row formed once per tile from float hi + lo parts, so the
+// separation keeps a few float ulps of itself), two sources per step in f32x2 registers, one
+// reciprocal per source for both of the lane's targets (1/d0 = d1 / (d0 d1)), FP32 sums per
+// tile added into compensated per-target sums.
+template <bool MIXED, int LBS>
+__global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
+    int nbricks, BlockLayout L_arg, const double *__restrict__ x0s, const double *__restrict__ y0s,
+    const double *__restrict__ hs, const int2 *__restrict__ range, const double *__restrict__ xs,
+    const double *__restrict__ ys, const double *__restrict__ vs, const int *__restrict__ offs,
+    const int *__restrict__ lists, double *__restrict__ xout, double *__restrict__ yout,
+    double *__restrict__ partial, int brick_lo, int brick_hi, int *task_ctr,
+    const int *__restrict__ task_brick) {
+    const BlockLayout L = LBS ? BlockLayout{LBS, LBS - 3} : L_arg;
+    __shared__ NearShared<MIXED> shared[EV_WARPS];
+    const int lane = lane_id(), warp = threadIdx.x >> 5;
+    NearShared<MIXED> &sh = shared[warp];
+    const int tx = lane & 7, ty = lane >> 3;   // targets (tx, ty) and (tx, ty + 4)
+    const double eps = 10 * DBL_EPSILON;
+
+    // Tasks: brick b owns tasks [toff[b], toff[b+1]) (relative to toff[0]); task p covers
+    // sources [p * P2P_SEG, (p + 1) * P2P_SEG) of the brick's P2P sequence.  This launch
+    // evaluates the tasks of bricks [brick_lo, brick_hi).
+    const int *toff = offs + 3 * nbricks;
+    const int tbase = toff[0];
+    const int task_lo = toff[brick_lo] - tbase, task_hi = toff[brick_hi] - tbase;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = task_lo + atomicAdd(task_ctr, 1);
+        task = __shfl_sync(FULL_MASK, task, 0);
+        if (task >= task_hi) break;
+        const int brick = task_brick[task];
+        const int part = task - (toff[brick] - tbase);
+        const int nparts = toff[brick + 1] - toff[brick];
+        const int beg = offs[2 * nbricks + brick], end = offs[2 * nbricks + brick + 1];
+        int blk, bx, by;
+        brick_of(L, brick, blk, bx, by);
+        const double h = hs[blk];
+        const Brick b = brick_geometry(x0s[blk], y0s[blk], h, bx, by);
+        double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
+
+        // Tiles of up to EV_CHUNK consecutive sources walk the listed leaves in order.
+        int it = beg, s_next = 0, e_next = 0;
+        auto take = [&]() { return range[lists[it++]]; };
+        int skip = part * P2P_SEG, budget = P2P_SEG;
+        while (it < end) {
+            const int2 rg = take();
+            const int cnt = rg.y - rg.x;
+            if (skip < cnt) {
+                s_next = rg.x + skip;
+                e_next = rg.y;
+                break;
+            }
+            skip -= cnt;
+        }
+        auto next_tile = [&](int &t0, int &tn) {
+            while (s_next >= e_next && it < end) {
+                const int2 rg = take();
+                s_next = rg.x;
+                e_next = rg.y;
+            }
+            t0 = s_next;
+            tn = min(min(EV_CHUNK, e_next - s_next), budget);
+            if (tn < 0) tn = 0;
+            s_next += tn;
+            budget -= tn;
+        };
+        int t0, tn;
+        next_tile(t0, tn);
+        double px = 0, py = 0, pv = 0;
+        if (lane < tn) {
+            px = xs[t0 + lane];
+            py = ys[t0 + lane];
+            pv = vs[t0 + lane];
+        }
+        if constexpr (MIXED) {
+            const float epsf = (float)eps;
+            const float2 eps2 = make_float2(epsf, epsf);
+            float hx0 = 0, lx0 = 0, hy0 = 0, ly0 = 0, hx1 = 0, lx1 = 0, hy1 = 0, ly1 = 0;
+            if (lane < TILE) split_f32(lane * h, sh.ch[lane], sh.cl[lane]);
+            while (tn > 0) {
+                const int cnt = tn;
+                __syncwarp();
+                {
+                    // offsets of source `lane` from every target column / row: (c h - q) with
+                    // q = source - corner, both as float hi + lo; slots past the tile get a
+                    // zero value (and unit offsets), so steps may take two sources at a time
+                    float qxh, qxl, qyh, qyl;
+                    split_f32(px - b.xlo, qxh, qxl);
+                    split_f32(py - b.ylo, qyh, qyl);
+                    const bool live = lane < cnt;
+#pragma unroll
+                    for (int c = 0; c < TILE; ++c) {
+                        const float ch = sh.ch[c], cl = sh.cl[c];
+                        sh.dx[c][lane] = live ? (ch - qxh) + (cl - qxl) : 1.f;
+                        sh.dy[c][lane] = live ? (ch - qyh) + (cl - qyl) : 1.f;
+                    }
+                    sh.v[lane] = live ? (float)pv : 0.f;
+                }
+                __syncwarp();
+                next_tile(t0, tn);
+                if (lane < tn) {
+                    px = xs[t0 + lane];
+                    py = ys[t0 + lane];
+                    pv = vs[t0 + lane];
+                }
+                const float2 *dxr = reinterpret_cast<const float2 *>(sh.dx[tx]);
+                const float2 *dyr0 = reinterpret_cast<const float2 *>(sh.dy[ty]);
+                const float2 *dyr1 = reinterpret_cast<const float2 *>(sh.dy[ty + 4]);
+                const float2 *vr2 = reinterpret_cast<const float2 *>(sh.v);
+                float2 fx0 = make_float2(0.f, 0.f), fy0 = fx0, fx1 = fx0, fy1 = fx0;
+                const int npair = (cnt + 1) >> 1;
+#pragma unroll 4
+                for (int k = 0; k < npair; ++k) {
+                    const float2 dx = dxr[k], dy0 = dyr0[k], dy1 = dyr1[k], v = vr2[k];
+                    const float2 dx2e = __ffma2_rn(dx, dx, eps2);
+                    const float2 d0 = __ffma2_rn(dy0, dy0, dx2e);
+                    const float2 d1 = __ffma2_rn(dy1, dy1, dx2e);
+                    const float2 p = __fmul2_rn(d0, d1);
+                    const float2 r = make_float2(rcp_approx_f32(p.x), rcp_approx_f32(p.y));
+                    const float2 vr = __fmul2_rn(v, r);
+                    const float2 f0 = __fmul2_rn(vr, d1), f1 = __fmul2_rn(vr, d0);
+                    fx0 = __ffma2_rn(dx, f0, fx0);
+                    fy0 = __ffma2_rn(dy0, f0, fy0);
+                    fx1 = __ffma2_rn(dx, f1, fx1);
+                    fy1 = __ffma2_rn(dy1, f1, fy1);
+                }
+                two_sum_acc(hx0, lx0, fx0.x + fx0.y);
+                two_sum_acc(hy0, ly0, fy0.x + fy0.y);
+                two_sum_acc(hx1, lx1, fx1.x + fx1.y);
+                two_sum_acc(hy1, ly1, fy1.x + fy1.y);
+            }
+            ax0 = (double)hx0 + (double)lx0;
+            ay0 = (double)hy0 + (double)ly0;
+            ax1 = (double)hx1 + (double)lx1;
+            ay1 = (double)hy1 + (double)ly1;
+        } else {
             const double xt = b.xlo + tx * h;
             const double yt0 = b.ylo + ty * h, yt1 = b.ylo + (ty + 4) * h;
-            // Tiles of up to EV_CHUNK consecutive sources walk the listed leaves in order; the
-            // next tile is loaded into registers while the current one is evaluated.  This task
-            // covers sources [part * P2P_SEG, (part + 1) * P2P_SEG) of the brick's sequence.
-            int it = beg, s_next = 0, e_next = 0;
-            int skip = part * P2P_SEG, budget = P2P_SEG;
-            while (it < end) {
-                const int2 rg = range[lists[it++]];
-                const int cnt = rg.y - rg.x;
-                if (skip < cnt) {
-                    s_next = rg.x + skip;
-                    e_next = rg.y;
-                    break;
-                }
-                skip -= cnt;
-            }
-            auto next_tile = [&](int &t0, int &tn) {
-                while (s_next >= e_next && it < end) {
-                    const int2 rg = range[lists[it++]];
-                    s_next = rg.x;
-                    e_next = rg.y;
-                }
-                t0 = s_next;
-                tn = min(min(EV_CHUNK, e_next - s_next), budget);
-                if (tn < 0) tn = 0;
-                s_next += tn;
-                budget -= tn;
-            };
-            int t0, tn;
-            next_tile(t0, tn);
-            double px = 0, py = 0, pv = 0;
-            if (lane < tn) {
-                px = xs[t0 + lane];
-                py = ys[t0 + lane];
-                pv = vs[t0 + lane];
-            }
-            if (MIXED) {
-                // FP32 pairs on offsets from the brick corner; differences of (hi, lo) splits
-                // keep the separation accurate to a few float ulps of itself
-                // the second target's y offset is the first one's plus 4h, added in float: one
-                // rounding of a quantity of the size of the offset itself
-                float txh, txl, ty0h, ty0l;
-                split_f32(tx * h, txh, txl);
-                split_f32(ty * h, ty0h, ty0l);
-                const float four_h = (float)(4.0 * h);
-                const float epsf = (float)eps;
-                float hx0 = 0, lx0 = 0, hy0 = 0, ly0 = 0, hx1 = 0, lx1 = 0, hy1 = 0, ly1 = 0;
-                while (tn > 0) {
-                    const int cnt = tn;
-                    __syncwarp();
-                    {
-                        float4 q;
-                        split_f32(px - b.xlo, q.x, q.y);
-                        split_f32(py - b.ylo, q.z, q.w);
-                        sh.sxy32[lane] = q;
-                        sh.sv32[lane] = (float)pv;
-                    }
-                    __syncwarp();
-                    next_tile(t0, tn);
-                    if (lane < tn) {
-                        px = xs[t0 + lane];
-                        py = ys[t0 + lane];
-                        pv = vs[t0 + lane];
-                    }
-                    float fx0 = 0, fy0 = 0, fx1 = 0, fy1 = 0;
-#pragma unroll 4
-                    for (int k = 0; k < cnt; ++k) {
-                        const float v = sh.sv32[k];
-                        const float4 q = sh.sxy32[k];
-                        const float dx = (txh - q.x) + (txl - q.y);
-                        const float dy0 = (ty0h - q.z) + (ty0l - q.w);
-                        const float dy1 = dy0 + four_h;
-                        const float dx2e = fmaf(dx, dx, epsf);
-                        const float f0 = v * rcp_approx_f32(fmaf(dy0, dy0, dx2e));
-                        const float f1 = v * rcp_approx_f32(fmaf(dy1, dy1, dx2e));
-                        fx0 = fmaf(dx, f0, fx0);
-                        fy0 = fmaf(dy0, f0, fy0);
-                        fx1 = fmaf(dx, f1, fx1);
-                        fy1 = fmaf(dy1, f1, fy1);
-                    }
-                    two_sum_acc(hx0, lx0, fx0);
-                    two_sum_acc(hy0, ly0, fy0);
-                    two_sum_acc(hx1, lx1, fx1);
-                    two_sum_acc(hy1, ly1, fy1);
-                }
-                ax0 += (double)hx0 + (double)lx0;
-                ay0 += (double)hy0 + (double)ly0;
-                ax1 += (double)hx1 + (double)lx1;
-                ay1 += (double)hy1 + (double)ly1;
-            }
-            while (!MIXED && tn > 0) {
+            while (tn > 0) {
                 const int cnt = tn;
                 __syncwarp();
                 sh.sxy[lane] = make_double2(px, py);
@@ -670,7 +838,7 @@ __global__ void k_scale_coeffs(int nnodes, const TNode *__restrict__ tnode,
     }
 }
 
-// Sum of the parts of every multi-task brick, in task order (deterministic).
+// The near field of every multi-task brick: its parts added in task order (deterministic).
 __global__ void k_force_gather_parts(int nbricks, int brick_lo, int brick_hi, BlockLayout L,
                                      const int *__restrict__ offs,
                                      const double *__restrict__ partial, double *__restrict__ xout,
@@ -682,6 +850,12 @@ __global__ void k_force_gather_parts(int nbricks, int brick_lo, int brick_hi, Bl
          brick += (gridDim.x * blockDim.x) >> 5) {
         const int t0 = toff[brick] - tbase, np = toff[brick + 1] - toff[brick];
         if (np <= 1) continue;
+        const int tx = lane & 7, ty = lane >> 3;
+        int blk, bx, by;
+        brick_of(L, brick, blk, bx, by);
+        const size_t o0 = target_index(L, blk, bx, by, tx, ty);
+        const size_t o1 = o0 + ((size_t)4 << L.lbs);
+        // the parts in task order
         double ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
         for (int p = 0; p < np; ++p) {
             const double *pp = partial + (size_t)(t0 + p) * 4 * 32;
@@ -690,11 +864,6 @@ __global__ void k_force_gather_parts(int nbricks, int brick_lo, int brick_hi, Bl
             ax1 += pp[64 + lane];
             ay1 += pp[96 + lane];
         }
-        const int tx = lane & 7, ty = lane >> 3;
-        int blk, bx, by;
-        brick_of(L, brick, blk, bx, by);
-        const size_t o0 = target_index(L, blk, bx, by, tx, ty);
-        const size_t o1 = o0 + ((size_t)4 << L.lbs);
         xout[o0] = ax0;
         yout[o0] = ay0;
         xout[o1] = ax1;
@@ -794,18 +963,51 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         TC_KERNEL_CHECK();
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
     }
+    // The near field reads the sources and the P2P lists only, not the expansions: it runs on
+    // the auxiliary stream as soon as the lists are in place, while the upward pass may still be
+    // forming expansions on the main stream.  It writes the outputs (near field only); the far
+    // field, on the main stream, waits for it and adds its part.
+    int *brick_ctr, *task_brick;
+    {
+        AuxScope on_aux(c);
+        double *partial;
+        if ((rc = ensure(c, S_BRICK_CTR, FORCE_CHUNKS + 1, &brick_ctr)) ||
+            (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)) ||
+            (rc = ensure(c, S_TASKMAP, (size_t)ntasks, &task_brick)))
+            return rc;
+        // work counters: far-field runs [0, FORCE_CHUNKS), the near field FORCE_CHUNKS
+        TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, (FORCE_CHUNKS + 1) * sizeof(int), c.stream));
+        k_task_map<<<(int)std::min<long long>((nbricks + 255) / 256, (long long)sm_count() * 8),
+                     256, 0, c.stream>>>(nbricks, offs, task_brick);
+        TC_KERNEL_CHECK();
+        const bool mixed = c.precision == 1;
+        constexpr int LBS32 = 5;   // the default block side, 32
+        const bool fixed = L.lbs == LBS32;
+        auto near = mixed ? (fixed ? k_force_near<true, LBS32> : k_force_near<true, 0>)
+                          : (fixed ? k_force_near<false, LBS32> : k_force_near<false, 0>);
+        const int occ_near = mixed ? blocks_per_sm<k_force_near<true, LBS32>>(EV_WARPS * 32, 0)
+                                   : blocks_per_sm<k_force_near<false, LBS32>>(EV_WARPS * 32, 0);
+        const int neargrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
+                                                      (long long)sm_count() * occ_near);
+        phase_mark(c, 9);
+        near<<<neargrid, EV_WARPS * 32, 0, c.stream>>>(
+            nbricks, L, x0s, y0s, hs, slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS),
+            slot_ptr<double>(c, S_YS), slot_ptr<double>(c, S_VS), offs, lists, xout, yout,
+            partial, 0, nbricks, brick_ctr + FORCE_CHUNKS, task_brick);
+        TC_KERNEL_CHECK();
+        if (ntasks > nbricks) {
+            k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8,
+                                                            (long long)sm_count() * 16),
+                                   256, 0, c.stream>>>(nbricks, 0, nbricks, L, offs, partial, xout,
+                                                       yout);
+            TC_KERNEL_CHECK();
+        }
+        phase_mark(c, 10);
+        c.near_marked = c.timing;
+        TC_CUDA_TRY(cudaEventRecord(c.ev_near, c.stream));
+    }
     TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
     phase_mark(c, 4);
-    int *brick_ctr, *task_brick;
-    double *partial;
-    if ((rc = ensure(c, S_BRICK_CTR, 4, &brick_ctr)) ||
-        (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)) ||
-        (rc = ensure(c, S_TASKMAP, (size_t)ntasks, &task_brick)))
-        return rc;
-    TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, 4 * sizeof(int), c.stream));
-    k_task_map<<<(int)std::min<long long>((nbricks + 255) / 256, (long long)sm_count() * 8), 256, 0,
-                 c.stream>>>(nbricks, offs, task_brick);
-    TC_KERNEL_CHECK();
     // the evaluation for the tree's expansion order
     rc = dispatch_order(c.order, [&](auto order) -> int {
         constexpr int P = decltype(order)::value;
@@ -825,12 +1027,14 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         }
         constexpr int LBS32 = 5;   // the default block side, 32
         const bool fixed = L.lbs == LBS32;
-        auto eval = mixed ? (fixed ? k_force_eval<P, true, LBS32> : k_force_eval<P, true, 0>)
-                          : (fixed ? k_force_eval<P, false, LBS32> : k_force_eval<P, false, 0>);
-        const int occ = mixed ? blocks_per_sm<k_force_eval<P, true, LBS32>>(EV_WARPS * 32, 0)
-                              : blocks_per_sm<k_force_eval<P, false, LBS32>>(EV_WARPS * 32, 0);
-        const int evgrid = (int)std::min<long long>((ntasks + EV_WARPS - 1) / EV_WARPS,
-                                                    (long long)sm_count() * occ);
+        auto far = mixed ? (fixed ? k_force_far<P, true, LBS32> : k_force_far<P, true, 0>)
+                         : (fixed ? k_force_far<P, false, LBS32> : k_force_far<P, false, 0>);
+        const int occ_far = mixed ? blocks_per_sm<k_force_far<P, true, LBS32>>(EV_WARPS * 32, 0)
+                                  : blocks_per_sm<k_force_far<P, false, LBS32>>(EV_WARPS * 32, 0);
+        const int fargrid = (int)std::min<long long>((nbricks + EV_WARPS - 1) / EV_WARPS,
+                                                     (long long)sm_count() * occ_far);
+        // the far field adds to the near field's outputs
+        TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_near, 0));
         // With host outputs of 2^21 targets or more (a copy of >= 32 MB, ~0.6 ms over PCIe) the
         // blocks are evaluated in FORCE_CHUNKS runs, each copied to the host on the auxiliary
         // stream while the next one is evaluated; below that the runs' tails cost more than
@@ -846,20 +1050,12 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
             const int blk0 = (int)((long long)nblocks * k / nchunks);
             const int blk1 = (int)((long long)nblocks * (k + 1) / nchunks);
             const int b0 = blk0 << (2 * L.lbps), b1 = blk1 << (2 * L.lbps);
-            eval<<<evgrid, EV_WARPS * 32, 0, c.stream>>>(
+            far<<<fargrid, EV_WARPS * 32, 0, c.stream>>>(
                 nbricks, L, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS),
-                slot_ptr<double>(c, S_EXPS), slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS),
-                slot_ptr<double>(c, S_YS), slot_ptr<double>(c, S_VS), offs, lists, xout, yout,
-                partial, b0, b1, brick_ctr + k, sexp, sscale, task_brick);
+                slot_ptr<double>(c, S_EXPS), offs, lists, xout, yout, b0, b1, brick_ctr + k, sexp,
+                sscale);
             TC_KERNEL_CHECK();
             if (k == nchunks - 1) phase_mark(c, 7);
-            if (ntasks > nbricks) {
-                k_force_gather_parts<<<(int)std::min<long long>((b1 - b0 + 7) / 8,
-                                                                (long long)sm_count() * 16),
-                                       256, 0, c.stream>>>(nbricks, b0, b1, L, offs, partial,
-                                                           xout, yout);
-                TC_KERNEL_CHECK();
-            }
             if (nchunks > 1) {
                 const size_t o = blk0 * per_block, cnt = (size_t)(blk1 - blk0) * per_block;
                 TC_CUDA_TRY(cudaEventRecord(c.ev_chunk[k], c.stream));
@@ -880,11 +1076,13 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
 void kernels_force(KernelList &v) {
     v.insert(v.end(), {(const void *)k_force_lists<1>, (const void *)k_force_lists<2>,
                        (const void *)k_force_lists_copy, (const void *)k_task_map,
-                       (const void *)k_force_gather_parts});
+                       (const void *)k_force_gather_parts, (const void *)k_force_near<true, 5>,
+                       (const void *)k_force_near<true, 0>, (const void *)k_force_near<false, 5>,
+                       (const void *)k_force_near<false, 0>});
 #define TC_FORCE_KERNELS(P)                                                                      \
-    v.insert(v.end(), {(const void *)k_force_eval<P, true, 5>, (const void *)k_force_eval<P, true, 0>, \
-                       (const void *)k_force_eval<P, false, 5>,                                  \
-                       (const void *)k_force_eval<P, false, 0>, (const void *)k_scale_coeffs<P, true>});
+    v.insert(v.end(), {(const void *)k_force_far<P, true, 5>, (const void *)k_force_far<P, true, 0>, \
+                       (const void *)k_force_far<P, false, 5>,                                   \
+                       (const void *)k_force_far<P, false, 0>, (const void *)k_scale_coeffs<P, true>});
     TC_FOR_EACH_ORDER(TC_FORCE_KERNELS)
 #undef TC_FORCE_KERNELS
 }

@@ -131,16 +131,6 @@ __device__ __forceinline__ int quantize(double v, double vmin, double scale) {
     return (int)floor(__dmul_rn(__dsub_rn(v, vmin), scale));
 }
 
-__global__ void k_keys(const double *__restrict__ x, const double *__restrict__ y, int n,
-                       const Frame *__restrict__ frame, int *__restrict__ keys) {
-    const Frame f = *frame;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int kx = quantize(x[i], f.xmin, f.scale);
-        const int ky = quantize(y[i], f.ymin, f.scale);
-        keys[i] = spread_bits(kx) | (spread_bits(ky) << 1);
-    }
-}
-
 // Target keys in the source frame, clamped to the quantisation range (targets may lie outside
 // the sources' square).  Used only to group nearby targets; it does not affect results.
 __global__ void k_target_keys(const double *__restrict__ x, const double *__restrict__ y, int n,
@@ -155,22 +145,6 @@ __global__ void k_target_keys(const double *__restrict__ x, const double *__rest
         if (qx != qx) qx = 0;
         if (qy != qy) qy = 0;
         keys[i] = spread_bits((int)qx) | (spread_bits((int)qy) << 1);
-    }
-}
-
-__global__ void k_gather3(const double *__restrict__ x, const double *__restrict__ y,
-                          const double *__restrict__ v, const int *__restrict__ perm, int n,
-                          double *__restrict__ xs, double *__restrict__ ys,
-                          double *__restrict__ vs, unsigned *err) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int j = perm[i];
-        if ((unsigned)j >= (unsigned)n) {
-            atomicOr(err, DEVERR_BOUNDS);
-            continue;
-        }
-        xs[i] = x[j];
-        ys[i] = y[j];
-        vs[i] = v[j];
     }
 }
 
@@ -400,7 +374,8 @@ __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
     };
     const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) |
-          (PACK ? reinterpret_cast<uintptr_t>(v) : 0)) & 15) == 0) {
+          reinterpret_cast<uintptr_t>(items) | (PACK ? reinterpret_cast<uintptr_t>(v) : 0)) &
+         15) == 0) {
         // 16-byte loads and stores: two sources per thread and step
         const double2 *x2 = reinterpret_cast<const double2 *>(x);
         const double2 *y2 = reinterpret_cast<const double2 *>(y);
@@ -441,21 +416,98 @@ __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
     }
 }
 
+// Resident values (the device entry points): the records are written by the first radix pass
+// itself, grouped by the top 8 bits of the key (256 buckets, each a square of 1/16 of the
+// frame's side), so that the final gather reads a window of the sorted order from a compact
+// range of records, L2-resident, instead of from anywhere in HBM:
+//   * k_key_hist reads x and y once and writes the histograms of the four radix digits and of
+//     the top 8 key bits (the buckets);
+//   * k_onesweep_items<true> (the first pass) reads x, y, v, forms the keys, claims each
+//     source a record slot in its bucket (tile counts in shared memory, one global atomic per
+//     tile and bucket) and writes the record (x, y, v, index); its items carry the record's
+//     position, key << 32 | slot;
+//   * three more passes over the items; the gather reads each record from its bucket.
+// Slots within a bucket depend on tile timing, but they are only payload: the passes order by
+// the key half alone and keep input order for equal keys, so the sorted keys, permutation and
+// sources do not depend on them.
+constexpr int NB_BUCKETS = 256;
+constexpr int BUCKET_SHIFT = 2 * LMAX - 8;   // the top 8 of the 30 key bits
+
+__device__ __forceinline__ int morton_key(double xv, double yv, const Frame &f) {
+    return spread_bits(quantize(xv, f.xmin, f.scale)) |
+           (spread_bits(quantize(yv, f.ymin, f.scale)) << 1);
+}
+
+__global__ __launch_bounds__(256) void k_key_hist(const double *__restrict__ x,
+                                                  const double *__restrict__ y, int n,
+                                                  const Frame *__restrict__ frame, int npasses,
+                                                  int *__restrict__ hist) {
+    __shared__ int s[RS_MAX_PASSES + 1][RS_RADIX];
+    for (int i = threadIdx.x; i < (RS_MAX_PASSES + 1) * RS_RADIX; i += blockDim.x)
+        (&s[0][0])[i] = 0;
+    __syncthreads();
+    const Frame f = *frame;
+    auto count = [&](double xv, double yv) {
+        const unsigned k = (unsigned)morton_key(xv, yv, f);
+        for (int p = 0; p < npasses; ++p) atomicAdd(&s[p][(k >> (8 * p)) & 0xFF], 1);
+        atomicAdd(&s[RS_MAX_PASSES][k >> BUCKET_SHIFT], 1);
+    };
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0) {
+        const double2 *x2 = reinterpret_cast<const double2 *>(x);
+        const double2 *y2 = reinterpret_cast<const double2 *>(y);
+        for (int i = gid; i < n / 2; i += stride) {
+            const double2 a = x2[i], b = y2[i];
+            count(a.x, b.x);
+            count(a.y, b.y);
+        }
+        if ((n & 1) && gid == 0) count(x[n - 1], y[n - 1]);
+    } else {
+        for (int i = gid; i < n; i += stride) count(x[i], y[i]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < (RS_MAX_PASSES + 1) * RS_RADIX; i += blockDim.x) {
+        const int c = (&s[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// One 32-byte store of four doubles (st.global.v4.f64; `p` 32-byte aligned).
+__device__ __forceinline__ void st_global_v4(double2 *p, double a, double b, double c, double d) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c),
+                 "d"(d)
+                 : "memory");
+}
+
+// The first pass's inputs: the resident sources, the frame, and where records go.
+struct FirstPass {
+    const double *x, *y, *v;
+    const Frame *frame;
+    double2 *rec;               // 2 per source: (x, y), (v, index as bits)
+    const int *bucket_off;      // exclusive scan of the bucket histogram
+    int *bucket_fill;           // slots claimed per bucket so far (zeroed per sort)
+};
+
 // One onesweep pass over 8-byte items, digit (item >> shift) & 0xFF: tiles of 3072 items
 // (256 threads x 12, four CTAs per SM); the tile's digit counts, then the global digit offsets
 // by decoupled look-back, then the stable rank within each warp from digit ballots; items are
 // placed in sorted order in shared memory and written out in runs of equal digits.
-// `stall_tile` (a test setting, -1 otherwise) names a tile that publishes nothing, so that the
-// tiles after it wait until `spin_limit` and report DEVERR_SPIN_LIMIT.
+// `stall_tile` (a test setting, -1 otherwise) names a tile that publishes into `sink` instead
+// of its status words, so that the tiles after it wait until `spin_limit` and report
+// DEVERR_SPIN_LIMIT.
 constexpr int PS_THREADS = 256;
 constexpr int PS_WARPS = PS_THREADS / 32;
 constexpr int PS_ITEMS = 12;
 constexpr int PS_TILE = PS_THREADS * PS_ITEMS;
 
-__global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
+// FIRST: the first pass of resident values (the tile's items formed from x, y, v, records
+// written to their buckets, see FirstPass); otherwise the items are read from `in`.  STALL:
+// the instance that honours stall_tile (the test setting; the others ignore it).
+template <bool FIRST, bool STALL = false>
+__global__ __launch_bounds__(PS_THREADS, FIRST ? 3 : 4) void k_onesweep_items(
     const unsigned long long *__restrict__ in, unsigned long long *__restrict__ out, int n,
     int shift, const int *__restrict__ digit_offsets, unsigned *status, int *tile_counter,
-    unsigned *err, int spin_limit, int stall_tile) {
+    unsigned *err, int spin_limit, int stall_tile, unsigned *sink, FirstPass fp) {
     __shared__ unsigned long long s_items[PS_TILE];
     __shared__ int s_whist[PS_WARPS][RS_RADIX];
     __shared__ int s_count[RS_RADIX];
@@ -467,6 +519,7 @@ __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1);
     for (int i = tid; i < PS_WARPS * RS_RADIX; i += PS_THREADS) (&s_whist[0][0])[i] = 0;
     s_count[tid] = 0;
+    if (FIRST) s_global[tid] = 0;   // the tile's count per bucket, first
     __syncthreads();
     const int tile = s_tile;
     const int tile_base = tile * PS_TILE;
@@ -475,10 +528,72 @@ __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
 
     unsigned long long item[PS_ITEMS];
     int rank[PS_ITEMS];
+    if constexpr (FIRST) {
+        // keys and each source's slot among the tile's sources of its bucket; the loads are
+        // issued in batches of FB before the shared atomics that consume them
+        const Frame f = *fp.frame;
+        constexpr int FB = 4;
+        static_assert(PS_ITEMS % FB == 0, "whole batches");
 #pragma unroll
-    for (int k = 0; k < PS_ITEMS; ++k) {
-        const int idx = warp_base + k * 32 + lane;
-        item[k] = idx < n ? in[idx] : 0ull;
+        for (int k0 = 0; k0 < PS_ITEMS; k0 += FB) {
+            double xv[FB], yv[FB];
+#pragma unroll
+            for (int k = 0; k < FB; ++k) {
+                const int idx = warp_base + (k0 + k) * 32 + lane;
+                xv[k] = idx < n ? __ldg(fp.x + idx) : 0.0;
+                yv[k] = idx < n ? __ldg(fp.y + idx) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < FB; ++k) {
+                const int idx = warp_base + (k0 + k) * 32 + lane;
+                int key = 0, slot = 0;
+                if (idx < n) {
+                    key = morton_key(xv[k], yv[k], f);
+                    slot = atomicAdd(&s_global[(unsigned)key >> BUCKET_SHIFT], 1);
+                }
+                item[k0 + k] = ((unsigned long long)(unsigned)key << 32) | (unsigned)slot;
+            }
+        }
+        __syncthreads();
+        // the tile's slots in each bucket, one global claim per bucket
+        {
+            const int c = s_global[tid];
+            if (c) s_tile_start[tid] = fp.bucket_off[tid] + atomicAdd(&fp.bucket_fill[tid], c);
+        }
+        __syncthreads();
+        // each record with one 32-byte store (one whole DRAM sector), batches of FB loads first
+#pragma unroll
+        for (int k0 = 0; k0 < PS_ITEMS; k0 += FB) {
+            double xv[FB], yv[FB], vv[FB];
+#pragma unroll
+            for (int k = 0; k < FB; ++k) {
+                const int idx = warp_base + (k0 + k) * 32 + lane;
+                xv[k] = idx < n ? __ldg(fp.x + idx) : 0.0;
+                yv[k] = idx < n ? __ldg(fp.y + idx) : 0.0;
+                vv[k] = idx < n ? __ldg(fp.v + idx) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < FB; ++k) {
+                const int idx = warp_base + (k0 + k) * 32 + lane;
+                if (idx >= n) continue;
+                const unsigned key = (unsigned)(item[k0 + k] >> 32);
+                const int pos = s_tile_start[key >> BUCKET_SHIFT] + (int)(unsigned)item[k0 + k];
+                if ((unsigned)pos >= (unsigned)n) {
+                    atomicOr(err, DEVERR_BOUNDS);
+                    continue;
+                }
+                st_global_v4(fp.rec + 2 * (size_t)pos, xv[k], yv[k], vv[k],
+                             __longlong_as_double((long long)idx));
+                item[k0 + k] = ((unsigned long long)key << 32) | (unsigned)pos;
+            }
+        }
+        __syncthreads();   // s_tile_start is reused below
+    } else {
+#pragma unroll
+        for (int k = 0; k < PS_ITEMS; ++k) {
+            const int idx = warp_base + k * 32 + lane;
+            item[k] = idx < n ? in[idx] : 0ull;
+        }
     }
     // Early counts: the tile's digit totals first (shared atomics), so that its aggregate is
     // published and the look-back done before the ranking, not after it.
@@ -488,15 +603,16 @@ __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
         if (warp_base + k * 32 + lane < n) atomicAdd(&s_count[(int)(item[k] >> shift) & 0xFF], 1);
     __syncthreads();
     const int total = s_count[d];
-    unsigned *mine = status + (size_t)tile * RS_RADIX + d;
-    const bool publish = tile != stall_tile;
+    // tile == stall_tile (a test setting): this tile publishes into `sink`, which no look-back
+    // reads, so the tiles after it wait until spin_limit
+    unsigned *mine = (STALL && tile == stall_tile ? sink : status + (size_t)tile * RS_RADIX) + d;
     int excl = 0;
     if (tile == 0) {
-        if (publish) atomicExch(mine, RS_FLAG_INC | (unsigned)total);
+        atomicExch(mine, RS_FLAG_INC | (unsigned)total);
     } else {
-        if (publish) atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
+        atomicExch(mine, RS_FLAG_AGG | (unsigned)total);
         excl = lookback(status, tile, d, err, spin_limit);
-        if (publish) atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
+        atomicExch(mine, RS_FLAG_INC | (unsigned)(excl + total));
     }
 
     const unsigned lt = lanemask_lt();
@@ -559,7 +675,10 @@ __global__ __launch_bounds__(PS_THREADS, 4) void k_onesweep_items(
 constexpr int GS_THREADS = 256;
 constexpr int GS_ITEMS = 8;
 
-template <bool KEYS>
+// KEYS: also the sorted keys and the permutation.  BUCKETED: the items carry record positions
+// and the records the sources' indices (the resident-values path); otherwise the items carry
+// the indices and the records are in input order.
+template <bool KEYS, bool BUCKETED = false>
 __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
     const unsigned long long *__restrict__ items, const double2 *__restrict__ rec, int n,
     int *__restrict__ keys, int *__restrict__ perm, double *__restrict__ xs,
@@ -569,6 +688,7 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
         unsigned long long it[GS_ITEMS];
         double2 a[GS_ITEMS];
         double w[GS_ITEMS];
+        int src[GS_ITEMS];
 #pragma unroll
         for (int k = 0; k < GS_ITEMS; ++k) {
             const int i = base + k * GS_THREADS;
@@ -580,7 +700,14 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
             const unsigned id = (unsigned)it[k];
             if (i < n && id < (unsigned)n) {
                 a[k] = __ldg(rec + 2 * (size_t)id);
-                w[k] = __ldg(reinterpret_cast<const double *>(rec + 2 * (size_t)id + 1));
+                if (BUCKETED) {
+                    const double2 b = __ldg(rec + 2 * (size_t)id + 1);
+                    w[k] = b.x;
+                    src[k] = (int)__double_as_longlong(b.y);
+                } else {
+                    w[k] = __ldg(reinterpret_cast<const double *>(rec + 2 * (size_t)id + 1));
+                    src[k] = (int)id;
+                }
             }
         }
 #pragma unroll
@@ -594,7 +721,7 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
             }
             if (KEYS) {
                 keys[i] = (int)(it[k] >> 32);
-                perm[i] = (int)id;
+                perm[i] = src[k];
             }
             xs[i] = a[k].x;
             ys[i] = a[k].y;
@@ -622,6 +749,28 @@ __global__ __launch_bounds__(256) void k_items_split(const unsigned long long *_
         const unsigned long long it = items[i];
         keys[i] = (int)(it >> 32);
         perm[i] = (int)(unsigned)it;
+    }
+}
+
+// The allocation-free sort's gather: the sorted items sit in xs (as 8-byte words); each thread
+// reads item i and then overwrites xs[i] with the source's x, so no other buffer is needed.
+__global__ __launch_bounds__(256) void k_gather_items_inplace(
+    const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ v, int n,
+    int *__restrict__ keys, int *__restrict__ perm, double *xs, double *__restrict__ ys,
+    double *__restrict__ vs, unsigned *err) {
+    unsigned long long *items = reinterpret_cast<unsigned long long *>(xs);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long it = items[i];
+        const unsigned j = (unsigned)it;
+        if (j >= (unsigned)n) {
+            atomicOr(err, DEVERR_BOUNDS);
+            continue;
+        }
+        keys[i] = (int)(it >> 32);
+        perm[i] = (int)j;
+        xs[i] = x[j];
+        ys[i] = y[j];
+        vs[i] = v[j];
     }
 }
 
@@ -788,35 +937,48 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     unsigned *status;
     const int npasses = (2 * LMAX + 7) / 8;
     const int ntiles = (n + PS_TILE - 1) / PS_TILE;
+    // histograms and their scans: the four radix digits, then the buckets of the records
+    constexpr int NHIST = RS_MAX_PASSES + 1;
     if ((rc = ensure(c, S_ITEMS_A, n, &items_a)) || (rc = ensure(c, S_ITEMS_B, n, &items_b)) ||
         (rc = ensure(c, S_REC, 2 * (size_t)n, &rec)) ||
-        (rc = ensure(c, S_RS_HIST, 2 * RS_MAX_PASSES * RS_RADIX, &hist)) ||
-        (rc = ensure(c, S_RS_COUNTER, RS_MAX_PASSES, &counter)) ||
-        (rc = ensure(c, S_RS_STATUS, (size_t)RS_MAX_PASSES * ntiles * RS_RADIX, &status)))
+        (rc = ensure(c, S_RS_HIST, 2 * NHIST * RS_RADIX, &hist)) ||
+        (rc = ensure(c, S_RS_COUNTER, RS_MAX_PASSES + NB_BUCKETS, &counter)) ||
+        (rc = ensure(c, S_RS_STATUS, ((size_t)RS_MAX_PASSES * ntiles + 1) * RS_RADIX, &status)))
         return rc;
-    int *offsets = hist + RS_MAX_PASSES * RS_RADIX;
-    TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * RS_MAX_PASSES * RS_RADIX, c.stream));
-    TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * RS_MAX_PASSES, c.stream));
+    int *offsets = hist + NHIST * RS_RADIX;
+    unsigned *sink = status + (size_t)RS_MAX_PASSES * ntiles * RS_RADIX;   // after every pass
+    int *bucket_fill = counter + RS_MAX_PASSES;
+    TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * NHIST * RS_RADIX, c.stream));
+    TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * (RS_MAX_PASSES + NB_BUCKETS), c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
                                 c.stream));
-    if (values_ready)
+    // resident values: the records are written by the first pass, in buckets (see FirstPass);
+    // values that arrive later: items and records in input order (finish_sources)
+    const bool bucketed = values_ready == nullptr;
+    if (bucketed)
+        k_key_hist<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, npasses, hist);
+    else
         k_keys_pack<false><<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, nullptr, n, frame,
                                                                       items_a, nullptr, npasses,
                                                                       hist);
-    else
-        k_keys_pack<true><<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, v, n, frame, items_a,
-                                                                     rec, npasses, hist);
     TC_KERNEL_CHECK();
-    k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
+    k_hist_scan<<<NHIST, RS_RADIX, 0, c.stream>>>(hist, offsets);
     TC_KERNEL_CHECK();
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
+    const FirstPass fp = {x, y, v, frame, rec, offsets + RS_MAX_PASSES * RS_RADIX, bucket_fill};
     static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in items_a");
     for (int p = 0; p < npasses; ++p) {
         const bool odd = p & 1;
-        k_onesweep_items<<<ntiles, PS_THREADS, 0, c.stream>>>(
+        const int stall = p == 0 && c.test_stall == TC_STALL_SORT ? 0 : -1;
+        auto pass = p == 0 ? (bucketed ? (stall >= 0 ? k_onesweep_items<true, true>
+                                                   : k_onesweep_items<true, false>)
+                                       : (stall >= 0 ? k_onesweep_items<false, true>
+                                                     : k_onesweep_items<false, false>))
+                           : k_onesweep_items<false, false>;
+        pass<<<ntiles, PS_THREADS, 0, c.stream>>>(
             odd ? items_b : items_a, odd ? items_a : items_b, n, 32 + 8 * p,
             offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err,
-            c.spin_limit, p == 0 && c.test_stall == TC_STALL_SORT ? 0 : -1);
+            c.spin_limit, stall, sink, fp);
         TC_KERNEL_CHECK();
     }
     c.nsrc = n;
@@ -832,8 +994,10 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
         c.late_ready = values_ready;
         return TC_OK;
     }
-    k_gather_sources<true><<<grid_for(n, GS_THREADS * GS_ITEMS, 8), GS_THREADS, 0, c.stream>>>(
-        items_a, rec, n, keys, perm, xs, ys, vs, err);
+    // a window of the sorted order in flight at a time (4 CTAs per SM): its records come from
+    // a compact range of buckets, which stays in L2
+    k_gather_sources<true, true><<<grid_for(n, GS_THREADS * GS_ITEMS, 4), GS_THREADS, 0,
+                                    c.stream>>>(items_a, rec, n, keys, perm, xs, ys, vs, err);
     TC_KERNEL_CHECK();
     return TC_OK;
 }
@@ -865,24 +1029,24 @@ int target_keys(Context &c, const double *xt, const double *yt, int m, int *keys
 }
 
 // ---------------------------------------------------------------------------- allocation-free
-// Source sort for callers that cannot allocate device memory.  Everything the sort needs
-// besides the caller's inputs and outputs -- the second key/permutation buffer of the
-// ping-pong passes, the per-tile look-back words, the digit histograms, the tile counters,
-// the bounding-box partials and the error word -- lives in one static device array of fixed
-// size, so a call makes no cudaMalloc/cudaFree and no other allocating call.
+// Source sort for callers that cannot allocate device memory, on the kernels the host entry
+// points run (k_bbox, k_keys_pack, four k_onesweep_items passes).  The caller's output arrays
+// double as the passes' ping-pong buffers: the 8-byte items live in xsorted and ysorted until
+// the last pass, and the gather then overwrites them in place.  Everything else -- the
+// per-tile look-back words, the digit histograms and their scans, the tile counters, the
+// bounding-box partials and the error word -- lives in one static device array of fixed size,
+// so a call makes no cudaMalloc/cudaFree and no other allocating call.
 constexpr int NOALLOC_MAX_SOURCES = 1 << 20;
-constexpr int NA_MAX_TILES = (NOALLOC_MAX_SOURCES + RS_TILE - 1) / RS_TILE;
+constexpr int NA_MAX_TILES = (NOALLOC_MAX_SOURCES + PS_TILE - 1) / PS_TILE;
 constexpr int NA_MAX_BBOX_BLOCKS = 4096;
-constexpr size_t NA_OFF_KEYS = 0;
-constexpr size_t NA_OFF_PERM = NA_OFF_KEYS + sizeof(int) * NOALLOC_MAX_SOURCES;
-constexpr size_t NA_OFF_STATUS = NA_OFF_PERM + sizeof(int) * NOALLOC_MAX_SOURCES;
+constexpr size_t NA_OFF_STATUS = 0;
 constexpr size_t NA_OFF_HIST =
     NA_OFF_STATUS + sizeof(unsigned) * RS_MAX_PASSES * NA_MAX_TILES * RS_RADIX;
 constexpr size_t NA_OFF_CTR = NA_OFF_HIST + sizeof(int) * 2 * RS_MAX_PASSES * RS_RADIX;
 constexpr size_t NA_OFF_ERR = NA_OFF_CTR + 256;
 constexpr size_t NA_OFF_DONE = NA_OFF_ERR + 256;
 constexpr size_t NA_OFF_PARTIALS = NA_OFF_DONE + 256;
-constexpr size_t NA_BYTES = NA_OFF_PARTIALS + sizeof(double4) * NA_MAX_BBOX_BLOCKS;  // ~9.2 MB
+constexpr size_t NA_BYTES = NA_OFF_PARTIALS + sizeof(double4) * NA_MAX_BBOX_BLOCKS;  // ~1.5 MB
 
 // One copy per device that loads the library, held until the process exits.  In host code
 // the name is only a host-side handle: kernels get the device address from
@@ -909,10 +1073,15 @@ static unsigned char *noalloc_scratch_base(int device) {
 }
 
 void kernels_sort(KernelList &v) {
-    v.insert(v.end(), {(const void *)k_bbox, (const void *)k_keys, (const void *)k_target_keys,
-                       (const void *)k_gather3, (const void *)k_hist, (const void *)k_hist_scan,
+    v.insert(v.end(), {(const void *)k_bbox, (const void *)k_target_keys,
+                       (const void *)k_gather_items_inplace, (const void *)k_hist,
+                       (const void *)k_hist_scan,
                        (const void *)k_onesweep, (const void *)k_keys_pack<true>,
-                       (const void *)k_keys_pack<false>, (const void *)k_onesweep_items,
+                       (const void *)k_keys_pack<false>, (const void *)k_onesweep_items<true>,
+                       (const void *)k_onesweep_items<false>, (const void *)k_key_hist,
+                       (const void *)k_onesweep_items<true, true>,
+                       (const void *)k_onesweep_items<false, true>,
+                       (const void *)k_gather_sources<true, true>,
                        (const void *)k_gather_sources<true>, (const void *)k_gather_sources<false>,
                        (const void *)k_pack_rec, (const void *)k_items_split,
                        (const void *)k_scan_reduce, (const void *)k_scan_blocks,
@@ -950,8 +1119,6 @@ extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const doub
         return treecode_last_status();
     }
     cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
-    int *keys_tmp = reinterpret_cast<int *>(base + NA_OFF_KEYS);
-    int *perm_tmp = reinterpret_cast<int *>(base + NA_OFF_PERM);
     unsigned *status = reinterpret_cast<unsigned *>(base + NA_OFF_STATUS);
     int *hist = reinterpret_cast<int *>(base + NA_OFF_HIST);
     int *offsets = hist + RS_MAX_PASSES * RS_RADIX;
@@ -960,10 +1127,13 @@ extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const doub
     unsigned *done = reinterpret_cast<unsigned *>(base + NA_OFF_DONE);
     double4 *partials = reinterpret_cast<double4 *>(base + NA_OFF_PARTIALS);
     Frame *fr = reinterpret_cast<Frame *>(frame);
+    // the passes' ping-pong buffers: the caller's xsorted / ysorted, as 8-byte items
+    unsigned long long *items_a = reinterpret_cast<unsigned long long *>(xsorted);
+    unsigned long long *items_b = reinterpret_cast<unsigned long long *>(ysorted);
 
     // The array keeps the previous call's contents: clear what has to start at zero.
     const int npasses = (2 * LMAX + 7) / 8;
-    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    const int ntiles = (n + PS_TILE - 1) / PS_TILE;
     TC_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned), s));
     TC_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned), s));
     TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * RS_MAX_PASSES * RS_RADIX, s));
@@ -973,27 +1143,23 @@ extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const doub
     const int gb = std::min(grid_for(n, BBOX_THREADS, 8), NA_MAX_BBOX_BLOCKS);
     k_bbox<<<gb, BBOX_THREADS, 0, s>>>(xsources, ysources, n, partials, done, fr);
     TC_KERNEL_CHECK();
-    k_keys<<<grid_for(n, 256), 256, 0, s>>>(xsources, ysources, n, fr, keys);
-    TC_KERNEL_CHECK();
-    k_hist<<<grid_for(n, 256, 4), 256, 0, s>>>(keys, n, npasses, hist);
+    k_keys_pack<false><<<grid_for(n, 256, 8), 256, 0, s>>>(xsources, ysources, nullptr, n, fr,
+                                                           items_a, nullptr, npasses, hist);
     TC_KERNEL_CHECK();
     k_hist_scan<<<npasses, RS_RADIX, 0, s>>>(hist, offsets);
     TC_KERNEL_CHECK();
-    // keys -> tmp -> keys -> tmp -> keys: four passes end in the caller's arrays
-    const int *ki = keys, *vi = nullptr;
+    static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in items_a");
     for (int p = 0; p < npasses; ++p) {
-        int *ko = (p & 1) ? keys : keys_tmp;
-        int *vo = (p & 1) ? perm : perm_tmp;
-        k_onesweep<<<ntiles, RS_THREADS, 0, s>>>(ki, vi, ko, vo, n, 8 * p, offsets + p * RS_RADIX,
-                                                  status + (size_t)p * ntiles * RS_RADIX,
-                                                  counter + p, err);
+        const bool odd = p & 1;
+        k_onesweep_items<false><<<ntiles, PS_THREADS, 0, s>>>(
+            odd ? items_b : items_a, odd ? items_a : items_b, n, 32 + 8 * p,
+            offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err,
+            RS_SPIN_LIMIT, -1, nullptr, FirstPass{});
         TC_KERNEL_CHECK();
-        ki = ko;
-        vi = vo;
     }
-    static_assert((2 * LMAX + 7) / 8 % 2 == 0, "an even number of passes ends in keys/perm");
-    k_gather3<<<grid_for(n, 256), 256, 0, s>>>(xsources, ysources, sourcevalues, perm, n,
-                                                xsorted, ysorted, vsorted, err);
+    k_gather_items_inplace<<<grid_for(n, 256), 256, 0, s>>>(xsources, ysources, sourcevalues, n,
+                                                             keys, perm, xsorted, ysorted,
+                                                             vsorted, err);
     TC_KERNEL_CHECK();
     unsigned h_err = 0;
     TC_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));

@@ -51,7 +51,7 @@ struct LevelOffsets {
 };
 
 struct PhaseTimes {
-    float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms, eval_kernel_ms;
+    float sort_ms, tree_ms, upward_ms, lists_ms, eval_ms, total_ms, eval_kernel_ms, far_kernel_ms;
 };
 
 struct Counts {
@@ -130,6 +130,7 @@ struct Context {
     cudaEvent_t ev_chunk[4] = {};        // force output runs ready for their host copy
     cudaEvent_t ev_leafset = nullptr;     // leaf moments written (main stream)
     cudaEvent_t ev_moments = nullptr;     // parent moments written (auxiliary stream)
+    cudaEvent_t ev_near = nullptr;        // force near field written (auxiliary stream)
     bool host_copied = false;
     // a source sort whose values arrive late (sort_sources / finish_sources)
     const double *late_x = nullptr, *late_y = nullptr, *late_v = nullptr;
@@ -153,7 +154,10 @@ struct Context {
     int spin_limit = DEFAULT_SPIN_LIMIT;
     int stack_limit = 0;
     bool timing = false;
-    cudaEvent_t ev[8] = {};
+    // phase events: 0-5 the phases, 6/7 the evaluation kernel (the far field of a force
+    // solve), 9/10 the force's near field on the auxiliary stream
+    cudaEvent_t ev[11] = {};
+    bool near_marked = false;             // ev[9], ev[10] recorded in this solve
     PhaseTimes times = {};
     Counts counts = {};
 

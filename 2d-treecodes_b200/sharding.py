@@ -1,10 +1,13 @@
-"""One force_mrag problem split over ranks by blocks.
+"""One treecode problem split over ranks: force_mrag by blocks, potential by targets.
 
-The blocks of a force_mrag solve are independent: every output element has one owner, so ranks
-need no exchange while they evaluate.  Each rank builds the whole tree from all the sources
-(the tree is replicated) and evaluates a contiguous run of the blocks in Morton order of their
-origins, so that a rank's blocks are close together and touch a compact part of the tree.
-Gathering the shards is needed only by a caller that wants every output on one rank.
+The blocks of a force_mrag solve are independent, and so are the targets of a potential solve
+(drivers/treecode-force.cpp:219-225 and drivers/treecode-potential.cpp:101-102 of the reference
+loop over them with no dependence between iterations): every output element has one owner, so
+ranks need no exchange while they evaluate.  Each rank builds the whole tree from all the
+sources (the tree is replicated) and evaluates a contiguous run of the blocks, or targets, in
+Morton order of their positions, so that a rank's share is close together and touches a compact
+part of the tree.  Gathering the shards is needed only by a caller that wants every output on
+one rank.
 """
 from __future__ import annotations
 
@@ -20,11 +23,11 @@ def _spread(v):
     return (v | (v << 1)) & 0x55555555
 
 
-def block_order(x0s, y0s):
-    """Block indices in Morton order of their origins (15 bits per axis over the origins'
-    bounding square; ties keep index order)."""
-    x0s = np.asarray(x0s, dtype=np.float64)
-    y0s = np.asarray(y0s, dtype=np.float64)
+def morton_order(x, y):
+    """Indices of the points (x, y) in Morton order (15 bits per axis over their bounding
+    square; ties keep index order)."""
+    x0s = np.asarray(x, dtype=np.float64)
+    y0s = np.asarray(y, dtype=np.float64)
     if len(x0s) == 0:
         return np.zeros(0, dtype=np.int64)
     lo_x, lo_y = x0s.min(), y0s.min()
@@ -36,14 +39,29 @@ def block_order(x0s, y0s):
     return np.argsort(keys, kind="stable")
 
 
+def block_order(x0s, y0s):
+    """Block indices in Morton order of their origins."""
+    return morton_order(x0s, y0s)
+
+
+def _run(order, rank, world):
+    """The rank-th of `world` near-equal contiguous runs of `order`."""
+    if not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside a world of {world}")
+    bounds = np.linspace(0, len(order), world + 1).round().astype(np.int64)
+    return order[bounds[rank]:bounds[rank + 1]]
+
+
 def block_shard(x0s, y0s, rank, world):
     """The blocks rank `rank` of `world` evaluates: the rank-th of `world` near-equal contiguous
     runs of the Morton order (every block in exactly one shard)."""
-    if not 0 <= rank < world:
-        raise ValueError(f"rank {rank} outside a world of {world}")
-    order = block_order(x0s, y0s)
-    bounds = np.linspace(0, len(order), world + 1).round().astype(np.int64)
-    return order[bounds[rank]:bounds[rank + 1]]
+    return _run(block_order(x0s, y0s), rank, world)
+
+
+def target_shard(xt, yt, rank, world):
+    """The targets rank `rank` of `world` evaluates in a potential solve: the rank-th of
+    `world` near-equal contiguous runs of the targets' Morton order."""
+    return _run(morton_order(xt, yt), rank, world)
 
 
 def solve_shard(ctx, theta, xs, ys, vs, x0s, y0s, hs, rank, world, blocksize=T.BLOCKSIZE):
@@ -72,3 +90,25 @@ def assemble(parts, nblocks, blocksize=T.BLOCKSIZE):
     if not seen.all():
         raise ValueError("a block is owned by no shard")
     return xo, yo
+
+
+def solve_potential_shard(ctx, theta, xs, ys, vs, xt, yt, rank, world):
+    """This rank's part of a potential solve on `ctx`: (target indices, potentials there)."""
+    idx = target_shard(xt, yt, rank, world)
+    xt, yt = (np.asarray(a, dtype=np.float64)[idx] for a in (xt, yt))
+    return idx, ctx.potential_host(theta, xs, ys, vs, xt, yt)
+
+
+def assemble_potential(parts, ntargets):
+    """Full potential output from every rank's (target indices, values)."""
+    out = np.empty(ntargets)
+    seen = np.zeros(ntargets, dtype=bool)
+    for idx, vals in parts:
+        idx = np.asarray(idx)
+        if seen[idx].any():
+            raise ValueError("a target is owned by two shards")
+        seen[idx] = True
+        out[idx] = vals
+    if not seen.all():
+        raise ValueError("a target is owned by no shard")
+    return out

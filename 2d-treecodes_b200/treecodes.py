@@ -117,7 +117,8 @@ class Stats(ctypes.Structure):
                 ("n_p2p", ctypes.c_longlong), ("p2p_pairs", ctypes.c_longlong),
                 ("e2p_pairs", ctypes.c_longlong), ("e2l_pairs", ctypes.c_longlong),
                 ("l2p_targets", ctypes.c_longlong), ("launches", ctypes.c_longlong),
-                ("eval_kernel_ms", ctypes.c_float), ("list_walks", ctypes.c_int)]
+                ("eval_kernel_ms", ctypes.c_float), ("list_walks", ctypes.c_int),
+                ("far_kernel_ms", ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -48,9 +48,9 @@ import workloads  # noqa: E402
 
 METRIC = "Mtargets/s at stated err vs FP64 direct: mixed vs FP64 GPU; serve p50/p99 ms"
 ORDER_FORCE = 24
-PHASES = ("sort_ms", "tree_ms", "upward_ms", "lists_ms", "eval_ms", "total_ms", "eval_kernel_ms")
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_force_eval.vortex_sheet_force.txt")
-PROFILE_TRAFFIC_MIXED = os.path.join(ROOT, "profiles", "k_force_eval.mixed.vortex_sheet_force.txt")
+PHASES = ("sort_ms", "tree_ms", "upward_ms", "lists_ms", "eval_ms", "total_ms", "eval_kernel_ms",
+          "far_kernel_ms")
+PROFILES = os.path.join(ROOT, "profiles")
 L2_BYTES = 126 << 20
 
 
@@ -68,20 +68,33 @@ def parse_args():
                    help="only `warmup` + `steps` device solves and a timing line (for profilers)")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     p.add_argument("--theta", type=float, default=None, help="override the workload's theta")
+    p.add_argument("--sources", type=int, default=None,
+                   help="override the workload's source count (reduced cases for profilers)")
+    p.add_argument("--blocks-per-side", type=int, default=None,
+                   help="override a force workload's MRAG grid (h = 1 / (32 x blocks per side))")
     p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the serving stream")
     p.add_argument("--serving-rate", type=float, default=200.0, help="Poisson arrival rate, 1/s")
     p.add_argument("--serving-slots", type=int, default=4)
     p.add_argument("--serving-budget-gb", type=float, default=40.0)
     p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                   help="weak: every rank solves its own copy of the workload; strong: the ranks "
+                        "split one problem (force blocks / potential targets in Morton order, "
+                        "the tree built by every rank)")
     return p.parse_args()
 
 
-def make_workload(name, seed_offset=0, theta=None):
+def make_workload(name, seed_offset=0, theta=None, sources=None, blocks_per_side=None):
     fn = workloads.WORKLOADS[name]
     import inspect
     seed = inspect.signature(fn).parameters["seed"].default + seed_offset
-    w = fn(seed=seed)
+    kw = {}
+    if sources is not None:
+        kw["n"] = sources
+    if blocks_per_side is not None:
+        kw["blocks_per_side"] = blocks_per_side
+    w = fn(seed=seed, **kw)
     if theta is not None:
         w["theta"] = float(theta)
         w["name"] += f"_theta{theta:g}"
@@ -182,23 +195,26 @@ class ClockSampler:
 
 # ------------------------------------------------------------------------------- roofline
 def algorithmic_flops(stats, kind="force"):
-    """Per-solve flops of the evaluation kernel with fixed per-unit weights.  force_mrag (p=24):
-    P2P 11 per pair (1 division), E2P 16p+8 per (target, cell), E2L 4p^2+20p per (brick, cell),
-    L2P 10p per target.  potential (p=12): P2P 8 per pair (1 log), E2P 10p+8 per (target,
-    cell)."""
+    """Per-solve flops of the evaluation with fixed per-unit weights, by kernel.  force_mrag
+    (p=24): far field (k_force_far) E2L 4p^2+20p per (brick, cell), L2P 10p per target, E2P
+    16p+8 per (target, cell); near field (k_force_near) P2P 11 per pair (1 division).
+    potential (p=12, one kernel, k_potential_eval): P2P 8 per pair (1 log), E2P 10p+8 per
+    (target, cell)."""
     if kind == "potential":
         p = 12
-        return 8.0 * stats["p2p_pairs"] + (10 * p + 8) * stats["e2p_pairs"]
+        return {"k_potential_eval": 8.0 * stats["p2p_pairs"] + (10 * p + 8) * stats["e2p_pairs"]}
     p = ORDER_FORCE
-    return (11.0 * stats["p2p_pairs"] + (16 * p + 8) * stats["e2p_pairs"]
-            + (4 * p * p + 20 * p) * stats["e2l_pairs"] + 10.0 * p * stats["l2p_targets"])
+    return {"k_force_far": (16 * p + 8) * stats["e2p_pairs"] + (4 * p * p + 20 * p) * stats["e2l_pairs"]
+            + 10.0 * p * stats["l2p_targets"],
+            "k_force_near": 11.0 * stats["p2p_pairs"]}
 
 
-def read_profile_traffic(mixed):
-    """DRAM bytes per launch of k_force_eval (the form that was timed) from the committed ncu
-    summary of the same workload, or None."""
+def read_profile_traffic(kernel, mixed, workload):
+    """DRAM bytes per launch of `kernel` (the form that was timed) from the committed ncu
+    summary of the same workload (profiles/<kernel>[.mixed].<workload>.txt), or None."""
+    name = f"{kernel}{'.mixed' if mixed else ''}.{workload}.txt"
     try:
-        with open(PROFILE_TRAFFIC_MIXED if mixed else PROFILE_TRAFFIC) as f:
+        with open(os.path.join(PROFILES, name)) as f:
             for line in f:
                 if line.startswith("dram_bytes_per_launch:"):
                     return float(line.split(":", 1)[1].split()[0])
@@ -295,7 +311,8 @@ def l2_desc(w):
 def run_reference(args, ws, rank):
     if rank != 0:
         return 0
-    w = make_workload(args.workload, theta=args.theta)
+    w = make_workload(args.workload, theta=args.theta, sources=args.sources,
+                      blocks_per_side=args.blocks_per_side)
     cores = os.cpu_count()
     for _ in range(args.warmup):
         cpu_reference_step(w)
@@ -331,8 +348,23 @@ def run_b200(args, ws, rank, local):
         raise SystemExit("bench.py needs a CUDA GPU")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    w = make_workload(args.workload, seed_offset=rank, theta=args.theta)
+    strong = args.scaling == "strong"
+    w = make_workload(args.workload, seed_offset=0 if strong else rank, theta=args.theta,
+                      sources=args.sources, blocks_per_side=args.blocks_per_side)
     kind = w["kind"]
+    # targets of the whole job: every rank's own problem (weak) or the one split problem (strong)
+    job_m = n_targets(w) * (1 if strong else ws)
+    if strong and ws > 1:
+        import sharding
+        w = dict(w)
+        if kind == "force":
+            idx = sharding.block_shard(w["x0s"], w["y0s"], rank, ws)
+            for k in ("x0s", "y0s", "hs"):
+                w[k] = np.ascontiguousarray(w[k][idx])
+        else:
+            idx = sharding.target_shard(w["xt"], w["yt"], rank, ws)
+            for k in ("xt", "yt"):
+                w[k] = np.ascontiguousarray(w[k][idx])
     mixed = args.precision == "mixed"
     ctx = T.Context(device=local, precision=1 if mixed else 0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -445,28 +477,47 @@ def run_b200(args, ws, rank, local):
 
     prec = 1 if mixed else 0
     ms, launches, clocks = timed(prec, args.steps, sample_clocks=True)
-    value = ws * m / (ms * 1e-3) / 1e6
+    value = job_m / (ms * 1e-3) / 1e6
     st = phases(prec)
     acc = accuracy(prec)
     other = None
     if mixed:   # the plain FP64 form on the same inputs, for the mixed-vs-FP64 ratio
         ms64, _, _ = timed(0, args.steps)
-        other = {"precision": "fp64", "value": ws * m / (ms64 * 1e-3) / 1e6, "unit": "Mtargets/s",
+        other = {"precision": "fp64", "value": job_m / (ms64 * 1e-3) / 1e6, "unit": "Mtargets/s",
                  "ms_per_step": ms64, "accuracy": accuracy(0),
                  "phase_ms": {k: v for k, v in phases(0).items() if k.endswith("_ms")}}
     ctx.set_precision(prec)
 
-    # ---- dominant kernel: the evaluation launch, timed by events on the library's stream
+    # ---- dominant kernel: the evaluation launches, timed by events on the library's stream
+    # (force: the far-field and near-field kernels separately; the longer one is the headline)
     flops = algorithmic_flops(st, kind)
     peak = T.measure_fma_peak(not mixed)
-    achieved = flops / (st["eval_kernel_ms"] * 1e-3) / 1e12
-    roofline = {"kernel": "k_force_eval" if kind == "force" else "k_potential_eval",
-                "bound": "fp32" if mixed else "fp64",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": read_profile_traffic(mixed) if w["name"].startswith("vortex_sheet_force") else None,
+    if kind == "force":
+        times = {"k_force_far": st["far_kernel_ms"],
+                 "k_force_near": st["eval_kernel_ms"] - st["far_kernel_ms"]}
+    else:
+        times = {"k_potential_eval": st["eval_kernel_ms"]}
+    wl = w["name"].split("_N")[0]
+    kernels = {}
+    for kname, kms in times.items():
+        ach = flops[kname] / (kms * 1e-3) / 1e12 if kms > 0 else None
+        kernels[kname] = {"achieved": ach, "frac": ach / peak if ach else None, "launch_ms": kms,
+                          "algorithmic_flops_per_launch": flops[kname],
+                          "traffic": read_profile_traffic(kname, mixed, wl)}
+    top = max(times, key=times.get)
+    tot_flops = sum(flops.values())
+    roofline = {"kernel": top, "bound": "fp32" if mixed else "fp64",
+                "achieved": kernels[top]["achieved"], "peak": peak, "unit": "TFLOP/s",
+                "frac": kernels[top]["frac"], "traffic": kernels[top]["traffic"],
                 "peak_source": ("measured %s FMA throughput of this GPU (tc_measure_fma_peak)"
                                 % ("FP32" if mixed else "FP64")),
-                "algorithmic_flops_per_launch": flops, "launch_ms": st["eval_kernel_ms"],
+                "algorithmic_flops_per_launch": kernels[top]["algorithmic_flops_per_launch"],
+                "launch_ms": kernels[top]["launch_ms"],
+                "kernels": kernels,
+                "evaluation": {"achieved": tot_flops / (st["eval_kernel_ms"] * 1e-3) / 1e12,
+                               "frac": tot_flops / (st["eval_kernel_ms"] * 1e-3) / 1e12 / peak,
+                               "launch_ms": st["eval_kernel_ms"],
+                               "algorithmic_flops_per_launch": tot_flops},
                 "phase_ms": {k: st[k] for k in PHASES}}
 
     # ---- end to end through the C ABI with pinned host buffers (host -> device copies and the
@@ -514,16 +565,16 @@ def run_b200(args, ws, rank, local):
     d2h = sum(t.numel() * 8 for t in hout)
     e2e_ms = wall(solve_host_ctx)
     e2e_ref_ms = wall(solve_host_ref)
-    e2e = {"value": ws * m / (e2e_ms * 1e-3) / 1e6, "unit": "Mtargets/s", "ms_per_step": e2e_ms,
+    e2e = {"value": job_m / (e2e_ms * 1e-3) / 1e6, "unit": "Mtargets/s", "ms_per_step": e2e_ms,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "api": ("tc_force_mrag_host" if kind == "force" else "tc_potential_host")
            + " (C ABI, host pointers, %s)" % args.precision,
            "reference_entry_point": {
                "api": ("treecode_force_mrag" if kind == "force" else "treecode_potential")
                + " (C ABI, host pointers, FP64)",
-               "value": ws * m / (e2e_ref_ms * 1e-3) / 1e6, "ms_per_step": e2e_ref_ms}}
+               "value": job_m / (e2e_ref_ms * 1e-3) / 1e6, "ms_per_step": e2e_ref_ms}}
 
-    e2e_fp64 = {"value": ws * m / (e2e_ref_ms * 1e-3) / 1e6, "unit": "Mtargets/s",
+    e2e_fp64 = {"value": job_m / (e2e_ref_ms * 1e-3) / 1e6, "unit": "Mtargets/s",
                 "ms_per_step": e2e_ref_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": e2e["reference_entry_point"]["api"],
                 "note": "plain FP64 through the reference-compatible entry point: the "
@@ -552,11 +603,12 @@ def run_b200(args, ws, rank, local):
         line = {
             "metric": METRIC, "value": value, "unit": "Mtargets/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "f32+f64" if mixed else "f64",
             "data": "synthetic (seeded PCG64; the reference's datasets are not available)",
             "config": bench_config(w, args.precision, l2_desc(w)),
-            "parallelism": f"{ws} independent solves (one per GPU)",
+            "parallelism": (f"{ws} independent solves (one per GPU)" if not strong else
+                            f"one problem split over {ws} GPUs (tree built on every GPU)"),
             "accuracy": acc,
             "plain_fp64": other,
             "e2e": e2e,

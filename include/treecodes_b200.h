@@ -95,6 +95,9 @@ typedef struct {
     float eval_kernel_ms;            /* the evaluation kernel alone (timing enabled) */
     int list_walks;                  /* tree walks that built the lists: 1, or 2 when the
                                         one-walk build outgrew its scratch (which then grows) */
+    float far_kernel_ms;             /* force: the far-field kernel alone; eval_kernel_ms is
+                                        it plus the near-field kernel, which runs beside the
+                                        upward pass (timing enabled; 0 otherwise) */
 } tc_stats;
 
 /* device < 0 selects the current device; stream may be NULL (the context creates one). */
@@ -196,11 +199,14 @@ TC_API int tc_log_probe_device(tc_context *ctx, const double *x, int n, double *
  * point runs the first stage
  * of the solve -- padded bounding square, 30-bit Morton keys, stable radix sort, gather of
  * x/y/value into Morton order, as drivers/sort-sources.cpp:23-132 of the reference defines it
- * -- with all of its scratch memory in one fixed, statically allocated device array.
+ * -- with all of its scratch memory in one fixed, statically allocated device array.  It runs the
+ * same kernels as the library's host entry points.
  *
  *   nsources <= TC_NOALLOC_MAX_SOURCES (1,048,576); larger inputs are rejected with
- *   TC_ERR_INVALID and a message naming the limit.  The scratch array is about 9.2 MB, held by
- *   every GPU that loads the library until the process exits.
+ *   TC_ERR_INVALID and a message naming the limit.  The scratch array is about 1.5 MB, held by
+ *   every GPU that loads the library until the process exits.  During the call xsorted and
+ *   ysorted also serve as the radix passes' working buffers (they hold the final results when
+ *   the call returns).
  *   All arrays are device pointers supplied by the caller: inputs xsources/ysources/
  *   sourcevalues; outputs keys and perm (nsources ints: sorted keys and, for each sorted
  *   position, the input index), xsorted/ysorted/vsorted (nsources doubles) and frame

@@ -58,11 +58,15 @@ def test_gloo_barrier_and_max_over_ranks():
 
 
 class _OracleContext:
-    """A stand-in with the library context's force_mrag_host, computed by the CPU oracle."""
+    """A stand-in with the library context's host entry points, computed by the CPU oracle."""
 
     def force_mrag_host(self, theta, xs, ys, vs, x0s, y0s, hs):
         import oracle as O
         return O.force_mrag(theta, xs, ys, vs, x0s, y0s, hs)
+
+    def potential_host(self, theta, xs, ys, vs, xt, yt):
+        import oracle as O
+        return O.potential(theta, xs, ys, vs, xt, yt)
 
 
 def _shard_rank_main(rank, ws, port, out):
@@ -140,3 +144,64 @@ def test_reference_arm_under_torchrun():
     line = lines[0]
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "reference"
+
+
+def _potential_shard_rank_main(rank, ws, port, out):
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(ws))
+    sys.path[:0] = [os.path.join(ROOT, "2d-treecodes_b200"), os.path.join(ROOT, "oracle")]
+    import sharding
+    import workloads as W
+    dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+    try:
+        w = W.gaussian_mixture_potential(n=20000, seed=7)
+        part = sharding.solve_potential_shard(_OracleContext(), w["theta"], w["xs"], w["ys"],
+                                              w["vs"], w["xt"], w["yt"], rank, ws)
+        parts = [None] * ws
+        dist.all_gather_object(parts, part)
+        if rank == 0:
+            got = sharding.assemble_potential(parts, len(w["xt"]))
+            ref = _OracleContext().potential_host(w["theta"], w["xs"], w["ys"], w["vs"],
+                                                  w["xt"], w["yt"])
+            out.put((np.array_equal(got, ref), [len(p[0]) for p in parts]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_potential_exact64.so")),
+                    reason="oracle not built")
+def test_sharded_potential_solve_on_two_gloo_ranks():
+    """One potential problem split by targets over two ranks in Morton order (tree replicated,
+    no exchange while evaluating): the gathered shards equal the unsplit solve bit for bit."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_potential_shard_rank_main, args=(r, 2, port, q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    equal, sizes = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert equal and sorted(sizes) == [10000, 10000]
+
+
+def test_target_shards_partition_in_morton_order():
+    sys.path.insert(0, os.path.join(ROOT, "2d-treecodes_b200"))
+    import sharding
+    r = np.random.default_rng(3)
+    xt, yt = r.random(1001), r.random(1001)
+    order = sharding.morton_order(xt, yt)
+    for ws in (1, 2, 5, 1001, 1002):
+        shards = [sharding.target_shard(xt, yt, k, ws) for k in range(ws)]
+        allidx = np.concatenate(shards)
+        assert np.array_equal(allidx, order)
+        assert max(map(len, shards)) - min(map(len, shards)) <= 1
+    with pytest.raises(ValueError):
+        sharding.target_shard(xt, yt, -1, 2)
+    with pytest.raises(ValueError):
+        sharding.assemble_potential([(np.array([0, 1]), np.zeros(2))], 3)

@@ -112,16 +112,16 @@ def test_bench_flop_model_and_profile_parse(tmp_path):
     import bench
     st = dict(p2p_pairs=10, e2p_pairs=2, e2l_pairs=3, l2p_targets=64)
     p = 24
-    assert bench.algorithmic_flops(st) == 110 + 2 * (16 * p + 8) + 3 * (4 * p * p + 20 * p) + 64 * 10 * p
-    f = tmp_path / "x.txt"
-    f.write_text("kernel: k_force_eval\ndram_bytes_per_launch: 123456 (read + write)\n")
-    old = bench.PROFILE_TRAFFIC, bench.PROFILE_TRAFFIC_MIXED
-    bench.PROFILE_TRAFFIC = str(f)
-    bench.PROFILE_TRAFFIC_MIXED = str(tmp_path / "missing.txt")
+    fl = bench.algorithmic_flops(st)
+    assert fl["k_force_near"] == 110
+    assert fl["k_force_far"] == 2 * (16 * p + 8) + 3 * (4 * p * p + 20 * p) + 64 * 10 * p
+    assert bench.algorithmic_flops(st, "potential") == {"k_potential_eval": 80 + 2 * (10 * 12 + 8)}
+    (tmp_path / "k_force_far.vortex_sheet_force.txt").write_text(
+        "kernel: k_force_far\ndram_bytes_per_launch: 123456 (read + write)\n")
+    old = bench.PROFILES
+    bench.PROFILES = str(tmp_path)
     try:
-        assert bench.read_profile_traffic(False) == 123456.0
-        assert bench.read_profile_traffic(True) is None
+        assert bench.read_profile_traffic("k_force_far", False, "vortex_sheet_force") == 123456.0
+        assert bench.read_profile_traffic("k_force_far", True, "vortex_sheet_force") is None
     finally:
-        bench.PROFILE_TRAFFIC, bench.PROFILE_TRAFFIC_MIXED = old
-    # the committed summaries of both forms carry the traffic line
-    assert bench.read_profile_traffic(False) > 0 and bench.read_profile_traffic(True) > 0
+        bench.PROFILES = old
