@@ -256,7 +256,11 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
         c.stream = stream;
         c.own_stream = false;
     } else {
-        TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        // the solve's critical path (sort, tree, expansions, far field) runs on this stream at
+        // the highest priority; the auxiliary stream's work (lists, near field) fills the gaps
+        int least = 0, greatest = 0;
+        TC_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        TC_CUDA_TRY(cudaStreamCreateWithPriority(&c.stream, cudaStreamNonBlocking, greatest));
         c.own_stream = true;
     }
     // freed pool blocks stay cached in the process for the next allocation (the default release
@@ -278,6 +282,7 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_leafset, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_moments, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_near, cudaEventDisableTiming));
+    TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_serial, cudaEventDisableTiming));
     c.h_pinned = pinned_area();
     if (!c.h_pinned) {
         set_error(TC_ERR_ALLOC, "page-locked host allocation failed");
@@ -310,7 +315,7 @@ static void context_free(Context &c) {
     for (auto &ev : c.ev)
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : {c.ev_fork, c.ev_totals, c.ev_join, c.ev_inputs, c.ev_leafset, c.ev_moments,
-                           c.ev_near})
+                           c.ev_near, c.ev_serial})
         if (ev) cudaEventDestroy(ev);
     for (auto &ev : c.ev_chunk)
         if (ev) cudaEventDestroy(ev);
@@ -708,8 +713,9 @@ TC_API int tc_supported_orders(int *orders, int capacity) {
 }
 
 TC_API int tc_set_timing(tc_context *ctx, int enabled) {
-    if (!ctx) return TC_ERR_INVALID;
+    if (!ctx || enabled < 0 || enabled > 2) return TC_ERR_INVALID;
     ctx->c.timing = enabled != 0;
+    ctx->c.serial_eval = enabled == 2;
     return TC_OK;
 }
 

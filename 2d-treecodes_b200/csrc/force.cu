@@ -280,16 +280,16 @@ __device__ __forceinline__ float2 cpowf_int(float2 z, int e) {
 
 // Near-field source tile.  Plain form: the sources' x, y, v.  Mixed form: for each source k of
 // the tile its offsets from the brick's 8 target columns (dx[c][k]) and 8 target rows
-// (dy[r][k]) as floats, and its value; rows padded to 34 words so that the 8 columns (4 rows) a
-// warp reads at once fall in distinct banks.
-constexpr int NEAR_ROW = EV_CHUNK + 2;
+// (dy[r][k]) as floats, and its value; read four sources at a time (16-byte loads), rows padded
+// to 36 words so that the 8 columns (4 rows) a warp reads at once fall in distinct banks.
+constexpr int NEAR_ROW = EV_CHUNK + 4;
 template <bool MIXED>
 struct NearShared {
     double2 sxy[EV_CHUNK];
     double sv[EV_CHUNK];
 };
 template <>
-struct NearShared<true> {
+struct __align__(16) NearShared<true> {
     float dx[TILE][NEAR_ROW];
     float dy[TILE][NEAR_ROW];
     float v[EV_CHUNK];
@@ -355,7 +355,7 @@ __global__ __launch_bounds__(EV_WARPS * 32, MIXED ? 5 : 4) void k_force_far(
         int brick = 0;
         if (lane == 0) brick = brick_lo + atomicAdd(brick_ctr, 1);
         brick = __shfl_sync(FULL_MASK, brick, 0);
-        if (brick >= brick_hi) break;
+        if (brick < brick_lo || brick >= brick_hi) break;   // (a counter not reset: no access)
         int blk, bx, by;
         brick_of(L, brick, blk, bx, by);
         const double h = hs[blk];
@@ -609,13 +609,13 @@ __global__ __launch_bounds__(EV_WARPS * 32, MIXED ? 5 : 4) void k_force_far(
             }
         }
 
-        // added to the near field that k_force_near (and k_force_gather_parts) wrote
+        // the far field alone, in the output layout; k_add_far adds it to the near field
         const size_t o0 = target_index(L, blk, bx, by, tx, ty);
         const size_t o1 = o0 + ((size_t)4 << L.lbs);
-        xout[o0] += ax0;
-        yout[o0] += ay0;
-        xout[o1] += ax1;
-        yout[o1] += ay1;
+        xout[o0] = ax0;
+        yout[o0] = ay0;
+        xout[o1] = ax1;
+        yout[o1] = ay1;
         __syncwarp();
     }
 }
@@ -651,7 +651,7 @@ __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
         int task = 0;
         if (lane == 0) task = task_lo + atomicAdd(task_ctr, 1);
         task = __shfl_sync(FULL_MASK, task, 0);
-        if (task >= task_hi) break;
+        if (task < task_lo || task >= task_hi) break;
         const int brick = task_brick[task];
         const int part = task - (toff[brick] - tbase);
         const int nparts = toff[brick + 1] - toff[brick];
@@ -727,15 +727,12 @@ __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
                     py = ys[t0 + lane];
                     pv = vs[t0 + lane];
                 }
-                const float2 *dxr = reinterpret_cast<const float2 *>(sh.dx[tx]);
-                const float2 *dyr0 = reinterpret_cast<const float2 *>(sh.dy[ty]);
-                const float2 *dyr1 = reinterpret_cast<const float2 *>(sh.dy[ty + 4]);
-                const float2 *vr2 = reinterpret_cast<const float2 *>(sh.v);
+                const float4 *dxr = reinterpret_cast<const float4 *>(sh.dx[tx]);
+                const float4 *dyr0 = reinterpret_cast<const float4 *>(sh.dy[ty]);
+                const float4 *dyr1 = reinterpret_cast<const float4 *>(sh.dy[ty + 4]);
+                const float4 *vr4 = reinterpret_cast<const float4 *>(sh.v);
                 float2 fx0 = make_float2(0.f, 0.f), fy0 = fx0, fx1 = fx0, fy1 = fx0;
-                const int npair = (cnt + 1) >> 1;
-#pragma unroll 4
-                for (int k = 0; k < npair; ++k) {
-                    const float2 dx = dxr[k], dy0 = dyr0[k], dy1 = dyr1[k], v = vr2[k];
+                auto pairs = [&](float2 dx, float2 dy0, float2 dy1, float2 v) {
                     const float2 dx2e = __ffma2_rn(dx, dx, eps2);
                     const float2 d0 = __ffma2_rn(dy0, dy0, dx2e);
                     const float2 d1 = __ffma2_rn(dy1, dy1, dx2e);
@@ -747,6 +744,15 @@ __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
                     fy0 = __ffma2_rn(dy0, f0, fy0);
                     fx1 = __ffma2_rn(dx, f1, fx1);
                     fy1 = __ffma2_rn(dy1, f1, fy1);
+                };
+                const int nquad = (cnt + 3) >> 2;
+#pragma unroll 2
+                for (int k = 0; k < nquad; ++k) {
+                    const float4 dx = dxr[k], dy0 = dyr0[k], dy1 = dyr1[k], v = vr4[k];
+                    pairs(make_float2(dx.x, dx.y), make_float2(dy0.x, dy0.y),
+                          make_float2(dy1.x, dy1.y), make_float2(v.x, v.y));
+                    pairs(make_float2(dx.z, dx.w), make_float2(dy0.z, dy0.w),
+                          make_float2(dy1.z, dy1.w), make_float2(v.z, v.w));
                 }
                 two_sum_acc(hx0, lx0, fx0.x + fx0.y);
                 two_sum_acc(hy0, ly0, fy0.x + fy0.y);
@@ -805,6 +811,20 @@ __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
             pp[96 + lane] = ay1;
         }
         __syncwarp();
+    }
+}
+
+// out += far over [begin, begin + count) of both output arrays (the near field plus the far
+// field; the two kernels write separate buffers so that they need not wait for each other).
+__global__ __launch_bounds__(256) void k_add_far(double *__restrict__ xout,
+                                                 double *__restrict__ yout,
+                                                 const double *__restrict__ xfar,
+                                                 const double *__restrict__ yfar, size_t begin,
+                                                 size_t count) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        xout[begin + i] += xfar[begin + i];
+        yout[begin + i] += yfar[begin + i];
     }
 }
 
@@ -964,19 +984,24 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         TC_CUDA_TRY(cudaEventRecord(c.ev_join, c.stream));
     }
     // The near field reads the sources and the P2P lists only, not the expansions: it runs on
-    // the auxiliary stream as soon as the lists are in place, while the upward pass may still be
-    // forming expansions on the main stream.  It writes the outputs (near field only); the far
-    // field, on the main stream, waits for it and adds its part.
+    // the auxiliary stream as soon as the lists are in place, while the upward pass forms the
+    // expansions and the far field is evaluated on the main stream (which has the higher
+    // priority: it carries the critical path).  The near field writes the outputs, the far
+    // field buffers of its own, and k_add_far adds the two once both are done.
     int *brick_ctr, *task_brick;
+    // (measurement mode: the near field waits for the upward pass, the far field for it)
+    if (c.serial_eval) TC_CUDA_TRY(cudaEventRecord(c.ev_serial, c.stream));
     {
         AuxScope on_aux(c);
+        if (c.serial_eval) TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_serial, 0));
+        // everything the near field uses is allocated and written on this stream (the far
+        // field's work counters are the main stream's own, S_FAR_CTR)
         double *partial;
-        if ((rc = ensure(c, S_BRICK_CTR, FORCE_CHUNKS + 1, &brick_ctr)) ||
+        if ((rc = ensure(c, S_BRICK_CTR, 1, &brick_ctr)) ||
             (rc = ensure(c, S_FPART, (size_t)ntasks * 4 * 32, &partial)) ||
             (rc = ensure(c, S_TASKMAP, (size_t)ntasks, &task_brick)))
             return rc;
-        // work counters: far-field runs [0, FORCE_CHUNKS), the near field FORCE_CHUNKS
-        TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, (FORCE_CHUNKS + 1) * sizeof(int), c.stream));
+        TC_CUDA_TRY(cudaMemsetAsync(brick_ctr, 0, sizeof(int), c.stream));
         k_task_map<<<(int)std::min<long long>((nbricks + 255) / 256, (long long)sm_count() * 8),
                      256, 0, c.stream>>>(nbricks, offs, task_brick);
         TC_KERNEL_CHECK();
@@ -993,7 +1018,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
         near<<<neargrid, EV_WARPS * 32, 0, c.stream>>>(
             nbricks, L, x0s, y0s, hs, slot_ptr<int2>(c, S_RANGE), slot_ptr<double>(c, S_XS),
             slot_ptr<double>(c, S_YS), slot_ptr<double>(c, S_VS), offs, lists, xout, yout,
-            partial, 0, nbricks, brick_ctr + FORCE_CHUNKS, task_brick);
+            partial, 0, nbricks, brick_ctr, task_brick);
         TC_KERNEL_CHECK();
         if (ntasks > nbricks) {
             k_force_gather_parts<<<(int)std::min<long long>((nbricks + 7) / 8,
@@ -1033,18 +1058,24 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
                                   : blocks_per_sm<k_force_far<P, false, LBS32>>(EV_WARPS * 32, 0);
         const int fargrid = (int)std::min<long long>((nbricks + EV_WARPS - 1) / EV_WARPS,
                                                      (long long)sm_count() * occ_far);
-        // the far field adds to the near field's outputs
-        TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_near, 0));
         // With host outputs of 2^21 targets or more (a copy of >= 32 MB, ~0.6 ms over PCIe) the
         // blocks are evaluated in FORCE_CHUNKS runs, each copied to the host on the auxiliary
         // stream while the next one is evaluated; below that the runs' tails cost more than
         // the overlap gains (measured: 16M sheet e2e 11.07 -> 10.67 ms, 1M vortex 2.01 ->
         // 2.27 ms if split).
         const size_t per_block = (size_t)1 << (2 * L.lbs);
+        const size_t nt_all = (size_t)nblocks * per_block;
+        double *xfar, *yfar;
+        int *far_ctr;
+        if ((rc2 = ensure(c, S_FARX, nt_all, &xfar)) || (rc2 = ensure(c, S_FARY, nt_all, &yfar)) ||
+            (rc2 = ensure(c, S_FAR_CTR, FORCE_CHUNKS, &far_ctr)))
+            return rc2;
+        TC_CUDA_TRY(cudaMemsetAsync(far_ctr, 0, FORCE_CHUNKS * sizeof(int), c.stream));
         const int nchunks =
             host_x && (size_t)nblocks * per_block >= ((size_t)1 << 21) && nblocks >= FORCE_CHUNKS
                 ? FORCE_CHUNKS
                 : 1;
+        if (c.serial_eval) TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_near, 0));
         phase_mark(c, 6);
         for (int k = 0; k < nchunks; ++k) {
             const int blk0 = (int)((long long)nblocks * k / nchunks);
@@ -1052,12 +1083,17 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
             const int b0 = blk0 << (2 * L.lbps), b1 = blk1 << (2 * L.lbps);
             far<<<fargrid, EV_WARPS * 32, 0, c.stream>>>(
                 nbricks, L, x0s, y0s, hs, tnode, slot_ptr<double>(c, S_MASS),
-                slot_ptr<double>(c, S_EXPS), offs, lists, xout, yout, b0, b1, brick_ctr + k, sexp,
+                slot_ptr<double>(c, S_EXPS), offs, lists, xfar, yfar, b0, b1, far_ctr + k, sexp,
                 sscale);
             TC_KERNEL_CHECK();
             if (k == nchunks - 1) phase_mark(c, 7);
+            const size_t o = blk0 * per_block, cnt = (size_t)(blk1 - blk0) * per_block;
+            if (k == 0) TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_near, 0));
+            k_add_far<<<(int)std::min<long long>((long long)(cnt + 255) / 256,
+                                                 (long long)sm_count() * 8),
+                        256, 0, c.stream>>>(xout, yout, xfar, yfar, o, cnt);
+            TC_KERNEL_CHECK();
             if (nchunks > 1) {
-                const size_t o = blk0 * per_block, cnt = (size_t)(blk1 - blk0) * per_block;
                 TC_CUDA_TRY(cudaEventRecord(c.ev_chunk[k], c.stream));
                 TC_CUDA_TRY(cudaStreamWaitEvent(c.aux, c.ev_chunk[k], 0));
                 TC_CUDA_TRY(cudaMemcpyAsync(host_x + o, xout + o, sizeof(double) * cnt,
@@ -1076,6 +1112,7 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
 void kernels_force(KernelList &v) {
     v.insert(v.end(), {(const void *)k_force_lists<1>, (const void *)k_force_lists<2>,
                        (const void *)k_force_lists_copy, (const void *)k_task_map,
+                       (const void *)k_add_far,
                        (const void *)k_force_gather_parts, (const void *)k_force_near<true, 5>,
                        (const void *)k_force_near<true, 0>, (const void *)k_force_near<false, 5>,
                        (const void *)k_force_near<false, 0>});

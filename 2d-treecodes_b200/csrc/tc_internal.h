@@ -36,7 +36,7 @@ enum Slot {
     S_TNODE, S_RANGE, S_CELL, S_MASS, S_W, S_WX, S_WY, S_EXPS, S_UPCNT,
     // force traversal / lists
     S_FCOUNT, S_FOFF, S_E2L, S_E2P, S_P2P, S_BRICK_CTR, S_FPART, S_SEXP, S_SSCALE, S_TASKMAP,
-    S_LSTART, S_LMETA,
+    S_LSTART, S_LMETA, S_FARX, S_FARY, S_FAR_CTR,
     // potential targets / lists
     S_TKEYS, S_TPERM, S_TKEYS2, S_TPERM2, S_PCOUNT, S_POFF, S_PE2P, S_PP2P,
     // misc
@@ -131,6 +131,7 @@ struct Context {
     cudaEvent_t ev_leafset = nullptr;     // leaf moments written (main stream)
     cudaEvent_t ev_moments = nullptr;     // parent moments written (auxiliary stream)
     cudaEvent_t ev_near = nullptr;        // force near field written (auxiliary stream)
+    cudaEvent_t ev_serial = nullptr;      // main stream's work so far (serial_eval)
     bool host_copied = false;
     // a source sort whose values arrive late (sort_sources / finish_sources)
     const double *late_x = nullptr, *late_y = nullptr, *late_v = nullptr;
@@ -154,6 +155,9 @@ struct Context {
     int spin_limit = DEFAULT_SPIN_LIMIT;
     int stack_limit = 0;
     bool timing = false;
+    // a measurement mode: the force's near- and far-field kernels run one after the other,
+    // after the upward pass, each alone on the GPU, so their events time each kernel by itself
+    bool serial_eval = false;
     // phase events: 0-5 the phases, 6/7 the evaluation kernel (the far field of a force
     // solve), 9/10 the force's near field on the auxiliary stream
     cudaEvent_t ev[11] = {};

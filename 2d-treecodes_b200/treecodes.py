@@ -273,7 +273,9 @@ class Context:
         self.blocksize = int(blocksize)
 
     def set_timing(self, on=True):
-        self.lib.tc_set_timing(self.h, 1 if on else 0)
+        """True / 1: phase times in stats(); 2: also the force's near- and far-field kernels
+        run one after the other, each alone on the GPU (per-kernel times); False / 0: off."""
+        _check(self.lib.tc_set_timing(self.h, int(on)))
 
     def stats(self):
         s = Stats()

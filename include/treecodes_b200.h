@@ -136,6 +136,10 @@ TC_API int tc_supported_orders(int *orders, int capacity);
  * default and for treecode_force_mrag).  Outputs hold nblocks * blocksize^2 values, target
  * (ix, iy) of block ib at ix + blocksize * (iy + blocksize * ib). */
 TC_API int tc_set_blocksize(tc_context *ctx, int blocksize);
+/* 1: record phase times (tc_get_stats); 2: also run the force evaluation's near- and far-field
+ * kernels one after the other, after the upward pass, each alone on the GPU, so that their
+ * times measure each kernel by itself (a measurement mode: the solve is slower, results are
+ * the same); 0: off. */
 TC_API int tc_set_timing(tc_context *ctx, int enabled);
 TC_API int tc_get_stats(tc_context *ctx, tc_stats *out);
 TC_API void *tc_get_stream(tc_context *ctx);

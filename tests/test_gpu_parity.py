@@ -266,3 +266,27 @@ def test_force_host_outputs_copied_in_runs(gpu_ctx):
         finally:
             gpu_ctx.set_precision(0)
         assert np.array_equal(hx, dx) and np.array_equal(hy, dy)
+
+
+def test_timing_modes_give_the_same_results(gpu_ctx):
+    """Phase timing (mode 1) and the per-kernel measurement mode (2, the force's near and far
+    field one after the other) change the scheduling only: the outputs are bit-identical."""
+    w = W.lamb_oseen_force(n=120000, blocks_per_side=4, h=1.0 / 128, seed=36)
+    ref = {}
+    for precision in (0, 1):
+        gpu_ctx.set_precision(precision)
+        try:
+            for mode in (0, 1, 2):
+                gpu_ctx.set_timing(mode)
+                got = gpu_force(gpu_ctx, w)
+                if mode == 0:
+                    ref[precision] = got
+                else:
+                    assert np.array_equal(got[0], ref[precision][0])
+                    assert np.array_equal(got[1], ref[precision][1])
+                if mode == 2:
+                    st = gpu_ctx.stats()
+                    assert 0 < st["far_kernel_ms"] < st["eval_kernel_ms"]
+        finally:
+            gpu_ctx.set_timing(0)
+            gpu_ctx.set_precision(0)
