@@ -985,9 +985,8 @@ int force_mrag(Context &c, double theta, const double *x0s, const double *y0s, c
     }
     // The near field reads the sources and the P2P lists only, not the expansions: it runs on
     // the auxiliary stream as soon as the lists are in place, while the upward pass forms the
-    // expansions and the far field is evaluated on the main stream (which has the higher
-    // priority: it carries the critical path).  The near field writes the outputs, the far
-    // field buffers of its own, and k_add_far adds the two once both are done.
+    // expansions and the far field is evaluated on the main stream.  The near field writes the
+    // outputs, the far field buffers of its own, and k_add_far adds the two once both are done.
     int *brick_ctr, *task_brick;
     // (measurement mode: the near field waits for the upward pass, the far field for it)
     if (c.serial_eval) TC_CUDA_TRY(cudaEventRecord(c.ev_serial, c.stream));

@@ -174,3 +174,45 @@ def test_trimmed_memory_stays_cached_until_released():
     finally:
         ctx.close()
         keep.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_concurrent_contexts_equal_solo(precision):
+    """Four threads, each with its own context, solve half-million-source force problems at
+    once, repeatedly: every result equals the problem solved alone, bit for bit.  Each solve
+    runs work on two streams of its context (the auxiliary one at the lower priority), so this
+    exercises the ordering between them under load from the other contexts."""
+    import threading
+    import workloads as W
+    ws = [W.lamb_oseen_force(n=1 << 19, blocks_per_side=8, h=1.0 / 256, seed=50 + i)
+          for i in range(4)]
+    args = [(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"], w["hs"]) for w in ws]
+    refs = []
+    for a in args:
+        ctx = T.Context(device=0, precision=precision)
+        try:
+            refs.append(ctx.force_mrag_host(*a))
+        finally:
+            ctx.close()
+    results = [None] * len(args)
+    errors = []
+
+    def run(i):
+        try:
+            ctx = T.Context(device=0, precision=precision)
+            try:
+                results[i] = [ctx.force_mrag_host(*args[i]) for _ in range(4)]
+            finally:
+                ctx.close()
+        except Exception as exc:   # reported below, on the test's thread
+            errors.append((i, exc))
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(len(args))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not errors, errors
+    for i, outs in enumerate(results):
+        for xo, yo in outs:
+            assert np.array_equal(xo, refs[i][0]) and np.array_equal(yo, refs[i][1]), i

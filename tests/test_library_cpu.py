@@ -125,3 +125,7 @@ def test_bench_flop_model_and_profile_parse(tmp_path):
         assert bench.read_profile_traffic("k_force_far", True, "vortex_sheet_force") is None
     finally:
         bench.PROFILES = old
+    # the committed summaries of both kernels and both forms carry the traffic line
+    for kernel in ("k_force_far", "k_force_near"):
+        for mixed in (False, True):
+            assert bench.read_profile_traffic(kernel, mixed, "vortex_sheet_force") > 0
