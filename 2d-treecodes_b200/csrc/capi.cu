@@ -201,6 +201,23 @@ static cudaError_t release_pool_cache(int device) {
     return e == cudaSuccess ? cudaMemPoolTrimTo(pool, 0) : e;
 }
 
+// Freed pool blocks stay cached in the process for the next allocation (the default release
+// threshold of 0 would hand them back to the driver at every synchronisation); set once per
+// device.
+static cudaError_t keep_pool_cache(int device) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), device) != done.end()) return cudaSuccess;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, device);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e == cudaSuccess) done.push_back(device);
+    return e;
+}
+
 // Live contexts per device.  Freed buffers stay cached in the device's pool while any context
 // lives, for the next allocation of any of them: a trim at every context's end (a request
 // server evicting idle clients) handed the memory back only for the next solve to map it anew.
@@ -264,16 +281,7 @@ static int context_init(Context &c, int device, cudaStream_t stream) {
         TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
     }
-    // freed pool blocks stay cached in the process for the next allocation (the default release
-    // threshold of 0 would hand them back to the driver at every synchronisation)
-    static const cudaError_t pool_rc = [device] {
-        cudaMemPool_t pool;
-        cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, device);
-        if (e != cudaSuccess) return e;
-        uint64_t keep = UINT64_MAX;
-        return cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }();
-    TC_CUDA_TRY(pool_rc);
+    TC_CUDA_TRY(keep_pool_cache(device));
     TC_CUDA_TRY(cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     TC_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_totals, cudaEventDisableTiming));
@@ -744,6 +752,32 @@ TC_API int tc_context_trim(tc_context *ctx) {
     }
     TC_CUDA_TRY(cudaStreamSynchronize(c.stream));
     c.nnodes = c.nsrc = 0;
+    return TC_OK;
+}
+
+TC_API int tc_reserve_cached_memory(int device, size_t bytes) {
+    clear_error();
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) return TC_ERR_NO_DEVICE;
+    TC_CUDA_TRY(cudaSetDevice(device));
+    TC_CUDA_TRY(keep_pool_cache(device));
+    size_t free_b = 0, total_b = 0;
+    TC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const size_t margin = (size_t)2 << 30;   // left to the driver and to other allocators
+    bytes = std::min(bytes, free_b > margin ? free_b - margin : 0);
+    if (bytes == 0) return TC_OK;
+    cudaStream_t s;
+    TC_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, s);
+    const cudaError_t es = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess || es != cudaSuccess) {
+        cudaGetLastError();
+        set_error(TC_ERR_ALLOC, "reserving %zu bytes in the device pool failed: %s", bytes,
+                  cudaGetErrorString(e != cudaSuccess ? e : es));
+        return TC_ERR_ALLOC;
+    }
     return TC_OK;
 }
 

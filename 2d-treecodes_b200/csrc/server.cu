@@ -26,6 +26,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <ctime>
 #include <deque>
 #include <list>
 #include <mutex>
@@ -42,6 +43,13 @@ using Clock = std::chrono::steady_clock;
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// Seconds on CLOCK_MONOTONIC (the clock of Python's time.perf_counter() on Linux).
+double monotonic_s() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
 
 struct Job {
@@ -74,6 +82,7 @@ struct tc_server {
     std::condition_variable cv_done;   // a job finished
     std::deque<Job *> queue;
     std::unordered_map<long long, Job *> jobs;
+    std::deque<long long> done_order;  // finished tickets in completion order (for wait_any)
     std::unordered_map<long long, Client> clients;
     std::list<long long> lru;          // idle clients, least recently used first
     std::vector<tc_context *> pool;    // one pooled context per slot (one-off requests)
@@ -216,7 +225,9 @@ Job *tc_server::pick(int slot, size_t *reserve, tc_context **ctx) {
             j->result.status = TC_ERR_CAPACITY;
             j->result.slot = slot;
             j->admitted = j->finished = Clock::now();
+            j->result.finished_s = monotonic_s();
             j->done = true;
+        done_order.push_back(j->ticket);
             ++failed;
             ++completed;
             cv_done.notify_all();
@@ -238,7 +249,9 @@ Job *tc_server::pick(int slot, size_t *reserve, tc_context **ctx) {
                     j->result.status = TC_ERR_CUDA;
                     j->result.slot = slot;
                     j->admitted = j->finished = Clock::now();
+                    j->result.finished_s = monotonic_s();
                     j->done = true;
+                    done_order.push_back(j->ticket);
                     ++failed;
                     ++completed;
                     cv_done.notify_all();
@@ -309,9 +322,11 @@ void tc_server::worker(int slot) {
         }
         peak = std::max(peak, charged);
         j->finished = Clock::now();
+        j->result.finished_s = monotonic_s();
         j->result.status = rc;
         j->result.slot = slot;
         j->done = true;
+        done_order.push_back(j->ticket);
         ++completed;
         if (rc) ++failed;
         cv_done.notify_all();
@@ -348,6 +363,9 @@ TC_API int tc_server_create(tc_server **srv, int device, int slots, size_t hbm_b
             return rc;
         }
     }
+    // the budget mapped into the device pool now, not while other requests' solves run (best
+    // effort: a server whose budget exceeds the free memory still works, with a smaller pool)
+    tc_reserve_cached_memory(device, hbm_budget_bytes);
     for (int i = 0; i < slots; ++i) s->workers.emplace_back(&tc_server::worker, s, i);
     *srv = s;
     return TC_OK;
@@ -401,6 +419,24 @@ TC_API int tc_server_submit(tc_server *srv, const tc_request *req, long long *ti
     return TC_OK;
 }
 
+namespace {
+
+// Hands a finished job's result to the caller and forgets the job (under the server lock).
+int collect_locked(tc_server *srv, Job *j, tc_request_result *result) {
+    j->result.queue_ms = ms_between(j->submitted, j->admitted);
+    j->result.service_ms = ms_between(j->admitted, j->finished);
+    j->result.latency_ms = ms_between(j->submitted, j->finished);
+    if (result) *result = j->result;
+    const int status = j->result.status;
+    srv->jobs.erase(j->ticket);
+    delete j;
+    // a wait_any blocked on the last outstanding ticket, which this call took, must return
+    srv->cv_done.notify_all();
+    return status;
+}
+
+}  // namespace
+
 TC_API int tc_server_wait(tc_server *srv, long long ticket, tc_request_result *result) {
     if (!srv) return TC_ERR_INVALID;
     std::unique_lock<std::mutex> lock(srv->mu);
@@ -408,14 +444,28 @@ TC_API int tc_server_wait(tc_server *srv, long long ticket, tc_request_result *r
     if (it == srv->jobs.end()) return TC_ERR_INVALID;
     Job *j = it->second;
     srv->cv_done.wait(lock, [&] { return j->done; });
-    j->result.queue_ms = ms_between(j->submitted, j->admitted);
-    j->result.service_ms = ms_between(j->admitted, j->finished);
-    j->result.latency_ms = ms_between(j->submitted, j->finished);
-    if (result) *result = j->result;
-    const int status = j->result.status;
-    srv->jobs.erase(it);
-    delete j;
-    return status;
+    return collect_locked(srv, j, result);
+}
+
+TC_API int tc_server_wait_any(tc_server *srv, long long *ticket, tc_request_result *result) {
+    if (!srv || !ticket) return TC_ERR_INVALID;
+    std::unique_lock<std::mutex> lock(srv->mu);
+    for (;;) {
+        // the oldest completion not yet collected (tickets that tc_server_wait took are skipped)
+        while (!srv->done_order.empty()) {
+            const long long t = srv->done_order.front();
+            srv->done_order.pop_front();
+            auto it = srv->jobs.find(t);
+            if (it == srv->jobs.end()) continue;
+            *ticket = t;
+            return collect_locked(srv, it->second, result);
+        }
+        if (srv->jobs.empty()) {   // nothing submitted and uncollected: nothing to wait for
+            *ticket = 0;
+            return TC_ERR_INVALID;
+        }
+        srv->cv_done.wait(lock);
+    }
 }
 
 TC_API int tc_server_release_client(tc_server *srv, long long client) {

@@ -42,11 +42,13 @@ def pinned_empty(n):
         return np.empty(int(n))
 
 
-def warm_pinned_cache(max_bytes=1 << 25, per_class=12):
+def warm_pinned_cache(max_bytes=1 << 25, per_class=32):
     """Fills torch's page-locked block cache: `per_class` blocks of every power-of-two size
     class from 4 KB to `max_bytes`, allocated and released at once.  The cache keeps freed blocks
     by class, so later `pinned_empty` calls reuse them; an empty class instead calls the driver's
-    page-locked allocation, which may synchronise the device and stall every solve in flight."""
+    page-locked allocation, which stalls every solve in flight: on the GPU hosts measured, single
+    allocations took up to 0.37 s, and the 2000-request stream with 12 blocks per class made
+    225 of them, each stall holding more outputs live and so causing the next (p99 0.6-1.2 s)."""
     held, total, b = [], 0, 4096
     try:
         import torch
@@ -168,30 +170,38 @@ def submit(server, spec, data, precision):
 
 def run_stream(server, specs, precision, materialise, keep_outputs=False):
     """Open-loop replay of `specs` on `server`.  Returns a summary dict (p50/p99 latency from
-    scheduled arrival, aggregate Mtargets/s over the stream's span) and, if asked, outputs."""
-    pending = []
-    lock = threading.Condition()
-    done_flag = [False]
+    scheduled arrival to the server's completion stamp, aggregate Mtargets/s over the stream's
+    span) and, if asked, outputs.  Results are collected in completion order
+    (`Server.wait_any`), so each request's outputs are released as soon as it is done."""
+    index = {}                       # ticket -> (request number, submission time)
+    lock = threading.Lock()
+    permits = threading.Semaphore(0)   # one per submitted request, one more at the end
+    submitted = [None]               # the number submitted, once submission is over
     records = [None] * len(specs)
     outputs = [None] * len(specs) if keep_outputs else None
     errors = []
 
     def collector():
-        k = 0
+        collected = 0
         while True:
+            permits.acquire()
             with lock:
-                while k >= len(pending) and not done_flag[0]:
-                    lock.wait()
-                if k >= len(pending):
+                if submitted[0] is not None and collected >= submitted[0]:
                     return
-                i, ticket, t_sub = pending[k]
-            k += 1
+            collected += 1
             try:
-                outs, res = server.wait(ticket)
+                ticket, outs, res = server.wait_any()
             except T.TreecodeError as e:
+                with lock:
+                    i = index.pop(getattr(e, "ticket", None), (None,))[0]
                 errors.append((i, str(e)))
                 continue
-            t_done = time.perf_counter()
+            with lock:
+                i, t_sub = index.pop(ticket)
+            # the server's completion stamp (CLOCK_MONOTONIC, perf_counter's clock)
+            seen = time.perf_counter()
+            fin = res["finished_s"]
+            t_done = fin if t_sub <= fin <= seen else seen
             records[i] = dict(res, t_done=t_done, t_sub=t_sub)
             spec = specs[i]
             if spec["resident"] and spec["step"] == spec["last_step"]:
@@ -202,20 +212,24 @@ def run_stream(server, specs, precision, materialise, keep_outputs=False):
     th = threading.Thread(target=collector)
     th.start()
     t0 = time.perf_counter()
-    for i, spec in enumerate(specs):
-        data = materialise(spec)
-        now = time.perf_counter() - t0
-        if spec["t"] > now:
-            time.sleep(spec["t"] - now)
-        t_sub = time.perf_counter()
-        ticket = submit(server, spec, data, precision)
+    count = 0
+    try:
+        for i, spec in enumerate(specs):
+            data = materialise(spec)
+            now = time.perf_counter() - t0
+            if spec["t"] > now:
+                time.sleep(spec["t"] - now)
+            t_sub = time.perf_counter()
+            with lock:   # the ticket is known to the collector before it can be collected
+                ticket = submit(server, spec, data, precision)
+                index[ticket] = (i, t_sub)
+            count += 1
+            permits.release()
+    finally:
         with lock:
-            pending.append((i, ticket, t_sub))
-            lock.notify()
-    with lock:
-        done_flag[0] = True
-        lock.notify()
-    th.join()
+            submitted[0] = count
+        permits.release()
+        th.join()
     if errors:
         raise T.TreecodeError(f"{len(errors)} requests failed, first: {errors[0]}")
     lat = np.array([(r["t_done"] - t0) * 1e3 - s["t"] * 1e3 for r, s in zip(records, specs)])
@@ -224,6 +238,7 @@ def run_stream(server, specs, precision, materialise, keep_outputs=False):
     targets = sum(s["n"] if s["kind"] == "potential" else
                   max(1, int(round(math.sqrt(s["n"] / 2048.0)))) ** 2 * 1024 for s in specs)
     span = max(r["t_done"] for r in records) - t0 - specs[0]["t"]
+    slow = np.argsort(-lat)[:5]
     summary = dict(requests=len(specs), precision="mixed" if precision else "fp64",
                    p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
                    mean_ms=float(lat.mean()), max_ms=float(lat.max()),
@@ -231,5 +246,9 @@ def run_stream(server, specs, precision, materialise, keep_outputs=False):
                    queue_p99_ms=float(np.percentile(queue, 99)),
                    mtargets_per_s=targets / span / 1e6, span_s=span,
                    offered_rate_hz=len(specs) / specs[-1]["t"] if specs[-1]["t"] > 0 else None,
+                   slowest=[dict(request=int(i), kind=specs[i]["kind"], n=specs[i]["n"],
+                                 arrival_s=round(specs[i]["t"], 4), latency_ms=float(lat[i]),
+                                 queue_ms=float(queue[i]), service_ms=float(service[i]))
+                            for i in slow],
                    server=server.stats())
     return summary, outputs

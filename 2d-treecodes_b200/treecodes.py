@@ -43,6 +43,7 @@ SIGNATURES = {
     "tc_set_host_waits": (_i, [_vp, _i]),
     "tc_set_wait_test": (_i, [_vp, _i, _i, _i]),
     "tc_release_cached_memory": (_i, [_i]),
+    "tc_reserve_cached_memory": (_i, [_i, ctypes.c_size_t]),
     "tc_set_orders": (_i, [_vp, _i, _i]),
     "tc_supported_orders": (_i, [ctypes.POINTER(ctypes.c_int), _i]),
     "tc_set_blocksize": (_i, [_vp, _i]),
@@ -66,6 +67,7 @@ SIGNATURES = {
     "tc_server_destroy": (None, [_vp]),
     "tc_server_submit": (_i, [_vp, _vp, ctypes.POINTER(ctypes.c_longlong)]),
     "tc_server_wait": (_i, [_vp, ctypes.c_longlong, _vp]),
+    "tc_server_wait_any": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong), _vp]),
     "tc_server_release_client": (_i, [_vp, ctypes.c_longlong]),
     "tc_server_get_stats": (_i, [_vp, _vp]),
     "tc_request_footprint": (ctypes.c_size_t, [_i, _i, _i, _i, _i]),
@@ -86,7 +88,7 @@ class Request(ctypes.Structure):
 
 class RequestResult(ctypes.Structure):
     _fields_ = [("status", _i), ("slot", _i), ("queue_ms", _d), ("service_ms", _d),
-                ("latency_ms", _d), ("footprint_bytes", ctypes.c_size_t)]
+                ("latency_ms", _d), ("footprint_bytes", ctypes.c_size_t), ("finished_s", _d)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -199,6 +201,12 @@ def release_cached_memory(device=-1):
     """Hands the device's cached, unused pool memory back to the driver (destroyed and trimmed
     contexts leave their memory cached while another context of the device lives)."""
     _check(load().tc_release_cached_memory(int(device)))
+
+
+def reserve_cached_memory(nbytes, device=-1):
+    """Maps up to `nbytes` of device memory into the device's pool ahead of the solves (at
+    most the free memory less 2 GB); a request server does this for its budget."""
+    _check(load().tc_reserve_cached_memory(int(device), int(nbytes)))
 
 
 def measure_fma_peak(fp64=True):
@@ -421,6 +429,22 @@ class Server:
         if rc != 0:
             raise TreecodeError(f"request {ticket} failed with status {rc}")
         return outs, res.as_dict()
+
+    def wait_any(self):
+        """(ticket, outputs tuple, result dict) of the earliest completed request not yet
+        collected; raises if that solve failed (the exception carries the ticket) or if no
+        request is outstanding."""
+        res = RequestResult()
+        t = ctypes.c_longlong()
+        rc = self.lib.tc_server_wait_any(self.h, ctypes.byref(t), ctypes.byref(res))
+        if t.value == 0:
+            raise TreecodeError(f"no request outstanding (status {rc})")
+        _, _, outs = self._live.pop(t.value)
+        if rc != 0:
+            err = TreecodeError(f"request {t.value} failed with status {rc}")
+            err.ticket = t.value
+            raise err
+        return t.value, outs, res.as_dict()
 
     def release_client(self, client):
         _check(self.lib.tc_server_release_client(self.h, ctypes.c_longlong(client)))

@@ -13,9 +13,10 @@ form measured on the same inputs (`plain_fp64`), so the mixed-vs-FP64 ratio is i
   e2e       the same metric through the C ABI with pinned host buffers (host->device copies and
             the result read-back timed): tc_force_mrag_host at the run's precision, and the
             reference-compatible treecode_force_mrag (FP64) beside it
-  roofline  the evaluation kernel (k_force_eval): algorithmic flops per launch / its event time,
-            against the measured FMA throughput of this GPU (FP64, or FP32 for the mixed form);
-            DRAM traffic per launch from the committed ncu capture
+  roofline  the evaluation kernels (k_force_far: E2L, L2P, E2P; k_force_near: P2P), each timed
+            alone in the library's serialised timing mode: algorithmic flops per launch / its
+            event time, against the measured FMA throughput of this GPU (FP64, or FP32 for the
+            mixed form); DRAM traffic per launch from the committed ncu captures
   e2e_fp64  the plain FP64 form through the reference-compatible treecode_force_mrag, host
             buffers: the matched-precision figure against the reference arm
   cpu_baseline  the reference's drivers (oracle/_ref) on the host cores: whole calls, measured
@@ -639,6 +640,16 @@ def run_b200(args, ws, rank, local):
     return 0
 
 
+def host_pinned_allocs():
+    import torch
+    return int(torch.cuda.host_memory_stats().get("num_host_alloc", 0))
+
+
+def device_free_bytes():
+    import torch
+    return int(torch.cuda.mem_get_info()[0])
+
+
 def run_serving(args, T):
     """The serving stream on a request server: p50/p99 latency from arrival and aggregate
     Mtargets/s, mixed and plain FP64 on the same seeded stream.  Inputs and outputs live in
@@ -651,7 +662,8 @@ def run_serving(args, T):
                       "followup_share": 0.2, "theta": list(S.THETAS),
                       "distributions": list(S.DISTRIBUTIONS), "host_memory": "page-locked",
                       "warm_up": "60 requests of another seed in each form, not counted",
-                      "latency": "scheduled arrival to completion (host clock)"}}
+                      "latency": "scheduled arrival to the server's completion stamp "
+                                 "(host monotonic clock)"}}
     m = S.Materialiser()
     srv = T.Server(slots=args.serving_slots,
                    hbm_budget_bytes=int(args.serving_budget_gb * (1 << 30)),
@@ -663,7 +675,12 @@ def run_serving(args, T):
             S.run_stream(srv, warm, precision, m)
         for precision, name in ((1, "mixed"), (0, "fp64")):
             m.state.clear()
+            host0, free0 = host_pinned_allocs(), device_free_bytes()
             summary, _ = S.run_stream(srv, specs, precision, m)
+            # stalls outside the solves: page-locked blocks the host allocator had to add, and
+            # device memory the stream-ordered pool had to map, during the stream
+            summary["host_pinned_allocs"] = host_pinned_allocs() - host0
+            summary["device_free_drop_gb"] = (free0 - device_free_bytes()) / 1e9
             out[name] = summary
     finally:
         srv.close()

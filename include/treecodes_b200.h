@@ -237,6 +237,11 @@ TC_API size_t tc_context_device_bytes(tc_context *ctx);
 TC_API int tc_context_trim(tc_context *ctx);
 /* Hands the device's cached, unused pool memory back to the driver (device < 0: current). */
 TC_API int tc_release_cached_memory(int device);
+/* Maps up to `bytes` of device memory into the device's stream-ordered pool and leaves it there
+ * unused (at most the free memory less 2 GB), so that later context allocations are carved from
+ * it instead of growing the pool while solves run; growing it mapped new memory in the middle of
+ * other contexts' work.  The memory returns to the driver as described for tc_context_trim. */
+TC_API int tc_reserve_cached_memory(int device, size_t bytes);
 
 /* ---- serving loop ---------------------------------------------------------------------
  * A request server on one GPU: solves submitted from any thread are queued, admitted in
@@ -275,6 +280,10 @@ typedef struct {
     double service_ms;              /* admission to completion */
     double latency_ms;              /* submission to completion */
     size_t footprint_bytes;         /* device memory charged at admission */
+    double finished_s;              /* completion instant, seconds on CLOCK_MONOTONIC (the
+                                       clock of Python's time.perf_counter() on Linux), so
+                                       that a caller can time a request from its own
+                                       arrival stamp whatever order it collects results in */
 } tc_request_result;
 
 typedef struct {
@@ -283,13 +292,20 @@ typedef struct {
     int slots, max_in_service, resident_clients;
 } tc_server_stats;
 
-/* slots: concurrent solves (>= 1); hbm_budget_bytes: device memory the server may hold. */
+/* slots: concurrent solves (>= 1); hbm_budget_bytes: device memory the server may hold, which
+ * it maps into the device's pool at creation (tc_reserve_cached_memory). */
 TC_API int tc_server_create(tc_server **srv, int device, int slots, size_t hbm_budget_bytes);
 /* Waits for all submitted requests, then frees every context. */
 TC_API void tc_server_destroy(tc_server *srv);
 TC_API int tc_server_submit(tc_server *srv, const tc_request *req, long long *ticket);
 /* Blocks until the request has completed; each ticket is waited for once. */
 TC_API int tc_server_wait(tc_server *srv, long long ticket, tc_request_result *result);
+/* Blocks until any submitted, not yet collected request has completed and collects it: *ticket
+   receives its ticket, the return value its status (the earliest completion first).  Returns
+   TC_ERR_INVALID with *ticket = 0 when no request is outstanding.  A caller that collects in
+   completion order releases each result's buffers as soon as it is done, instead of holding
+   them behind a longer solve submitted earlier. */
+TC_API int tc_server_wait_any(tc_server *srv, long long *ticket, tc_request_result *result);
 /* Releases a resident client's device memory once its queued requests are done. */
 TC_API int tc_server_release_client(tc_server *srv, long long client);
 TC_API int tc_server_get_stats(tc_server *srv, tc_server_stats *out);

@@ -41,6 +41,7 @@ int tc_set_precision(tc_context *c, int p) {
     return 0;
 }
 size_t tc_context_device_bytes(tc_context *c) { return c ? c->bytes : 0; }
+int tc_reserve_cached_memory(int, size_t) { return 0; }
 int tc_context_trim(tc_context *c) {
     c->bytes = 0;
     return 0;

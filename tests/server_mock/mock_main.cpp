@@ -60,11 +60,44 @@ int main(int argc, char **argv) {
             tickets.push_back(t);
             if (rng() % 4 == 0) std::this_thread::sleep_for(std::chrono::microseconds(rng() % 300));
         }
-        for (int i = 0; i < nreq; ++i) {
+        if (trial % 2 == 0) {
+            for (int i = 0; i < nreq; ++i) {
+                tc_request_result res;
+                if (tc_server_wait(s, tickets[i], &res) != 0) ++failures;
+                for (double v : out[i])
+                    if (v != marker[i]) ++failures;
+            }
+        } else {
+            // one ticket by tc_server_wait, the rest in completion order by tc_server_wait_any:
+            // every ticket exactly once, completion stamps non-decreasing, then nothing left
+            std::map<long long, int> index;
+            for (int i = 0; i < nreq; ++i) index[tickets[i]] = i;
+            const int mid = nreq / 2;
             tc_request_result res;
-            if (tc_server_wait(s, tickets[i], &res) != 0) ++failures;
-            for (double v : out[i])
-                if (v != marker[i]) ++failures;
+            if (tc_server_wait(s, tickets[mid], &res) != 0) ++failures;
+            index.erase(tickets[mid]);
+            for (double v : out[mid])
+                if (v != marker[mid]) ++failures;
+            double last = -1.0;
+            for (int k = 0; k + 1 < nreq; ++k) {
+                long long t = 0;
+                const int rc = tc_server_wait_any(s, &t, &res);
+                auto it = index.find(t);
+                if (rc != 0 || it == index.end()) {
+                    fprintf(stderr, "trial %d: wait_any gave ticket %lld (status %d)\n", trial, t, rc);
+                    ++failures;
+                    continue;
+                }
+                const int i = it->second;
+                index.erase(it);
+                if (res.finished_s < last) ++failures;
+                last = res.finished_s;
+                for (double v : out[i])
+                    if (v != marker[i]) ++failures;
+            }
+            long long t = -1;
+            if (tc_server_wait_any(s, &t, nullptr) != TC_ERR_INVALID || t != 0) ++failures;
+            if (!index.empty()) ++failures;
         }
         tc_server_stats st;
         tc_server_get_stats(s, &st);

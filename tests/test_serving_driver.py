@@ -3,6 +3,7 @@ server: the stream's composition, the open-loop replay, the follow-up advection,
 sessions (a resident client is released once, after its last step completes; one-off requests
 run on client 0 and are never released)."""
 import threading
+import time
 
 import numpy as np
 
@@ -10,7 +11,10 @@ import serving as S
 
 
 class FakeServer:
-    """Records what the driver asks of a request server; solves complete in submission order."""
+    """Records what the driver asks of a request server.  `wait_any` completes the newest
+    outstanding request whose client has no earlier one outstanding (one client's steps stay in
+    order, as on the real server), so the driver must cope with completions out of submission
+    order."""
 
     def __init__(self):
         self.lock = threading.Lock()
@@ -18,6 +22,7 @@ class FakeServer:
         self.completed = set()
         self.released = []       # (client, tickets completed at the time)
         self.inputs = {}
+        self.order = []          # tickets in the order wait_any completed them
 
     def _submit(self, kind, client, xs, ys, vs):
         with self.lock:
@@ -37,7 +42,22 @@ class FakeServer:
     def wait(self, ticket):
         with self.lock:
             self.completed.add(ticket)
-        return (np.zeros(1),), {"status": 0, "slot": 0, "queue_ms": 0.0, "service_ms": 0.1}
+        return (np.zeros(1),), {"status": 0, "slot": 0, "queue_ms": 0.0, "service_ms": 0.1,
+                                "finished_s": time.perf_counter()}
+
+    def wait_any(self):
+        with self.lock:
+            out = [(t, c) for t, _, c, _ in self.submitted if t not in self.completed]
+            assert out, "wait_any with nothing outstanding"
+            first = {}
+            for t, c in out:
+                first.setdefault(c, t)
+            ready = [t for t, c in out if c == 0 or first[c] == t]
+            t = max(ready)
+            self.completed.add(t)
+            self.order.append(t)
+        return t, (np.zeros(1),), {"status": 0, "slot": 0, "queue_ms": 0.0, "service_ms": 0.1,
+                                   "finished_s": time.perf_counter()}
 
     def release_client(self, client):
         with self.lock:
@@ -89,6 +109,16 @@ def test_clients_released_once_after_their_last_step():
             last_ticket[s["client"]] = t
     for client, done in srv.released:
         assert last_ticket[client] in done                 # after its last step completed
+
+
+def test_results_collected_in_completion_order():
+    specs = small_stream(300, 13)
+    m = S.Materialiser(log2_max=12, seed=3)
+    srv = FakeServer()
+    summary, outs = S.run_stream(srv, specs, 1, m, keep_outputs=True)
+    assert sorted(srv.order) == list(range(len(specs)))   # every request exactly once
+    assert all(o is not None for o in outs)
+    assert summary["p50_ms"] >= 0 and np.isfinite(summary["p99_ms"])
 
 
 def test_followups_advect_the_previous_step():
