@@ -317,9 +317,10 @@ __device__ __forceinline__ void split_f32(double v, float &hi, float &lo) {
     lo = (float)(v - (double)hi);
 }
 
-// MIXED = false: plain FP64.  MIXED = true: E2P in FP32 on scaled multipole coefficients with
-// compensated per-target sums, the two targets of a lane side by side in paired-FP32 (f32x2)
-// registers; the local expansion (E2L, L2P) stays FP64.
+// MIXED = false: plain FP64.  MIXED = true: E2L, L2P and E2P in FP32 on power-of-two scaled
+// quantities (scaled multipole coefficients, scaled local coefficients, offsets over the
+// brick's scale), the two targets of a lane side by side in paired-FP32 (f32x2) registers,
+// E2P's per-cell terms in compensated FP32 sums per target.
 // LBS > 0: the block layout of side 2^LBS fixed at compile time (the default side 32 has its
 // own instances: the layout arithmetic on kernel arguments measured 3% slower); LBS = 0: the
 // layout L given at run time.
