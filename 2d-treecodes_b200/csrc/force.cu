@@ -622,11 +622,15 @@ __global__ __launch_bounds__(EV_WARPS * 32, MIXED ? 5 : 4) void k_force_far(
 }
 
 // P2P (force-kernels.m4:15-55): sum v (xr, yr) / (xr^2 + yr^2 + eps) over the sources of a
-// task's segment.  MIXED = true: FP32 pairs on offsets from the brick corner (each source's
-// offset to every target column and row formed once per tile from float hi + lo parts, so the
-// separation keeps a few float ulps of itself), two sources per step in f32x2 registers, one
-// reciprocal per source for both of the lane's targets (1/d0 = d1 / (d0 d1)), FP32 sums per
-// tile added into compensated per-target sums.
+// task's segment.  Both forms take one reciprocal per source for both of the lane's targets,
+// 1/d0 = d1 / (d0 d1).
+//  * MIXED = false: FP64, the reciprocal refined by two Newton steps (the squared separations
+//    are at least eps and, for coordinates below ~1e70, their product stays far from the
+//    double range's ends).
+//  * MIXED = true: FP32 pairs on offsets from the brick corner (each source's offset to every
+//    target column and row formed once per tile from float hi + lo parts, so the separation
+//    keeps a few float ulps of itself), two sources per step in f32x2 registers, FP32 sums per
+//    tile added into compensated per-target sums.
 template <bool MIXED, int LBS>
 __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
     int nbricks, BlockLayout L_arg, const double *__restrict__ x0s, const double *__restrict__ y0s,
@@ -707,17 +711,27 @@ __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
                 __syncwarp();
                 {
                     // offsets of source `lane` from every target column / row: (c h - q) with
-                    // q = source - corner, both as float hi + lo; slots past the tile get a
-                    // zero value (and unit offsets), so steps may take two sources at a time
+                    // q = source - corner, both as float hi + lo, two columns (rows) per f32x2
+                    // instruction; slots past the tile get a zero value (their offsets, of an
+                    // earlier source or of the origin, stay finite and their separations at
+                    // least eps), so steps may take two sources at a time
                     float qxh, qxl, qyh, qyl;
                     split_f32(px - b.xlo, qxh, qxl);
                     split_f32(py - b.ylo, qyh, qyl);
                     const bool live = lane < cnt;
+                    const float2 nqxh = make_float2(-qxh, -qxh), nqxl = make_float2(-qxl, -qxl);
+                    const float2 nqyh = make_float2(-qyh, -qyh), nqyl = make_float2(-qyl, -qyl);
+                    const float2 *ch2 = reinterpret_cast<const float2 *>(sh.ch);
+                    const float2 *cl2 = reinterpret_cast<const float2 *>(sh.cl);
 #pragma unroll
-                    for (int c = 0; c < TILE; ++c) {
-                        const float ch = sh.ch[c], cl = sh.cl[c];
-                        sh.dx[c][lane] = live ? (ch - qxh) + (cl - qxl) : 1.f;
-                        sh.dy[c][lane] = live ? (ch - qyh) + (cl - qyl) : 1.f;
+                    for (int c = 0; c < TILE; c += 2) {
+                        const float2 ch = ch2[c >> 1], cl = cl2[c >> 1];
+                        const float2 dx = __fadd2_rn(__fadd2_rn(ch, nqxh), __fadd2_rn(cl, nqxl));
+                        const float2 dy = __fadd2_rn(__fadd2_rn(ch, nqyh), __fadd2_rn(cl, nqyl));
+                        sh.dx[c][lane] = dx.x;
+                        sh.dx[c + 1][lane] = dx.y;
+                        sh.dy[c][lane] = dy.x;
+                        sh.dy[c + 1][lane] = dy.y;
                     }
                     sh.v[lane] = live ? (float)pv : 0.f;
                 }
@@ -786,8 +800,9 @@ __global__ __launch_bounds__(EV_WARPS * 32, NEAR_MIN_BLOCKS) void k_force_near(
                     const double xr = xt - sp.x;
                     const double xr2e = fma(xr, xr, eps);
                     const double yr0 = yt0 - sp.y, yr1 = yt1 - sp.y;
-                    const double f0 = v * rcp_nr(fma(yr0, yr0, xr2e));
-                    const double f1 = v * rcp_nr(fma(yr1, yr1, xr2e));
+                    const double d0 = fma(yr0, yr0, xr2e), d1 = fma(yr1, yr1, xr2e);
+                    const double vr = v * rcp_nr(d0 * d1);
+                    const double f0 = vr * d1, f1 = vr * d0;
                     ax0 = fma(xr, f0, ax0);
                     ay0 = fma(yr0, f0, ay0);
                     ax1 = fma(xr, f1, ax1);

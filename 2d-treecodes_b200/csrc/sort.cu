@@ -1,14 +1,21 @@
 // sort.cu -- bounding square, Morton keys, LSD radix sort with a stable permutation, and the
 // sorted source arrays.  Restates drivers/sort-sources.cpp:23-132 of the reference.
 //
-// Data flow per solve (N sources, all FP64 SoA in HBM):
+// Data flow per solve (N sources, all FP64 SoA in HBM), with the values resident (the device
+// entry points):
 //   k_bbox            x, y        -> Frame (xmin, ymin, ext, scale)          16 B/src read
-//   k_keys_pack       x, y, v     -> items (key << 32 | index), records      24 B read, 40 B written
-//                                    (x, y, v, 0), digit histograms
-//   k_onesweep_items  items       -> items sorted by one 8-bit key digit     8 B read, 8 B written
-//                                    (4 passes)
-//   k_gather_sources  items, recs -> sorted keys, permutation, x, y, v       8 B + one 32-byte
-//                                                                            record read, 32 B written
+//   k_key_hist        x, y        -> histograms of the 4 key digits and of   16 B read
+//                                    the 256 spatial buckets (top 8 key bits)
+//   k_onesweep_items  x, y, v     -> 32-byte records (x, y, v, index) in     24 B read, 40 B written
+//     (first pass)                   their buckets, items (key << 32 | slot)
+//                                    sorted by the first digit
+//   k_onesweep_items  items       -> items sorted by the next 8-bit digit    8 B read, 8 B written
+//                                    (3 passes)
+//   k_gather_sources  items, recs -> sorted keys, permutation, x, y, v       8 B + one record
+//                                                                            read, 32 B written
+// With values that arrive after x and y (the host entry points): k_keys_pack writes the items
+// (key << 32 | index) and the histograms, four passes sort them, k_items_split writes keys and
+// permutation, k_gather_xy the sorted x and y, and k_gather_v the sorted v once it is in.
 //
 // The radix sort is a one-pass-per-digit ("onesweep") LSD sort: every CTA counts the digits of
 // a tile of items, finds its global digit offsets by a decoupled look-back over the tiles
@@ -345,23 +352,16 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
 }
 
 // ---------------------------------------------------------------------------- source sort
-// The sources are sorted as 8-byte items (key << 32 | index) and gathered once at the end:
-//   * k_keys_pack reads x, y, v once and writes the Morton keys' digit histograms, the items
-//     in input order and a 32-byte record (x, y, v, 0) per source (k_keys_pack<false> and
-//     k_pack_rec split this in two when the values arrive later, see sort_sources);
-//   * four onesweep passes over the items (8-bit digits of the key half; 16 B of traffic per
-//     item and pass);
-//   * k_gather_sources reads each sorted item's record (one 32-byte DRAM sector) and writes
-//     the sorted keys, permutation, x, y and v.
-// Ties keep input order, so the result is the (key, index) lexicographic order.
-template <bool PACK>
+// The sources are sorted as 8-byte items key << 32 | payload by four onesweep passes (8-bit
+// digits of the key half, 16 B of traffic per item and pass).  Ties keep input order, so the
+// result is the (key, index) lexicographic order.
+// k_keys_pack: the items (key << 32 | index) in input order and the histograms of the four
+// digits (the late-values path and the allocation-free sort).
 __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
-                                                   const double *__restrict__ y,
-                                                   const double *__restrict__ v, int n,
+                                                   const double *__restrict__ y, int n,
                                                    const Frame *__restrict__ frame,
                                                    unsigned long long *__restrict__ items,
-                                                   double2 *__restrict__ rec, int npasses,
-                                                   int *__restrict__ hist) {
+                                                   int npasses, int *__restrict__ hist) {
     __shared__ int s[RS_MAX_PASSES][RS_RADIX];
     for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
     __syncthreads();
@@ -374,40 +374,21 @@ __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
     };
     const int gid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) |
-          reinterpret_cast<uintptr_t>(items) | (PACK ? reinterpret_cast<uintptr_t>(v) : 0)) &
-         15) == 0) {
+          reinterpret_cast<uintptr_t>(items)) & 15) == 0) {
         // 16-byte loads and stores: two sources per thread and step
         const double2 *x2 = reinterpret_cast<const double2 *>(x);
         const double2 *y2 = reinterpret_cast<const double2 *>(y);
-        const double2 *v2 = reinterpret_cast<const double2 *>(v);
         ulonglong2 *it2 = reinterpret_cast<ulonglong2 *>(items);
         for (int i = gid; i < n / 2; i += stride) {
             const double2 a = x2[i], b = y2[i];
             it2[i] = make_ulonglong2(item_of(a.x, b.x, 2 * i), item_of(a.y, b.y, 2 * i + 1));
-            if (PACK) {
-                const double2 w = v2[i];
-                rec[4 * i + 0] = make_double2(a.x, b.x);
-                rec[4 * i + 1] = make_double2(w.x, 0.0);
-                rec[4 * i + 2] = make_double2(a.y, b.y);
-                rec[4 * i + 3] = make_double2(w.y, 0.0);
-            }
         }
         if ((n & 1) && gid == 0) {
             const int i = n - 1;
             items[i] = item_of(x[i], y[i], i);
-            if (PACK) {
-                rec[2 * i] = make_double2(x[i], y[i]);
-                rec[2 * i + 1] = make_double2(v[i], 0.0);
-            }
         }
     } else {
-        for (int i = gid; i < n; i += stride) {
-            items[i] = item_of(x[i], y[i], i);
-            if (PACK) {
-                rec[2 * i] = make_double2(x[i], y[i]);
-                rec[2 * i + 1] = make_double2(v[i], 0.0);
-            }
-        }
+        for (int i = gid; i < n; i += stride) items[i] = item_of(x[i], y[i], i);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < npasses * RS_RADIX; i += blockDim.x) {
@@ -675,10 +656,8 @@ __global__ __launch_bounds__(PS_THREADS, FIRST ? 3 : 4) void k_onesweep_items(
 constexpr int GS_THREADS = 256;
 constexpr int GS_ITEMS = 8;
 
-// KEYS: also the sorted keys and the permutation.  BUCKETED: the items carry record positions
-// and the records the sources' indices (the resident-values path); otherwise the items carry
-// the indices and the records are in input order.
-template <bool KEYS, bool BUCKETED = false>
+// The sorted sources from the sorted items (key << 32 | record slot) and the bucketed records
+// (x, y, v, index): the sorted keys, the permutation (the records' indices) and x, y, v.
 __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
     const unsigned long long *__restrict__ items, const double2 *__restrict__ rec, int n,
     int *__restrict__ keys, int *__restrict__ perm, double *__restrict__ xs,
@@ -686,9 +665,7 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
     const int stride = gridDim.x * GS_THREADS * GS_ITEMS;
     for (int base = blockIdx.x * GS_THREADS * GS_ITEMS + threadIdx.x; base < n; base += stride) {
         unsigned long long it[GS_ITEMS];
-        double2 a[GS_ITEMS];
-        double w[GS_ITEMS];
-        int src[GS_ITEMS];
+        double2 a[GS_ITEMS], b[GS_ITEMS];
 #pragma unroll
         for (int k = 0; k < GS_ITEMS; ++k) {
             const int i = base + k * GS_THREADS;
@@ -700,44 +677,51 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
             const unsigned id = (unsigned)it[k];
             if (i < n && id < (unsigned)n) {
                 a[k] = __ldg(rec + 2 * (size_t)id);
-                if (BUCKETED) {
-                    const double2 b = __ldg(rec + 2 * (size_t)id + 1);
-                    w[k] = b.x;
-                    src[k] = (int)__double_as_longlong(b.y);
-                } else {
-                    w[k] = __ldg(reinterpret_cast<const double *>(rec + 2 * (size_t)id + 1));
-                    src[k] = (int)id;
-                }
+                b[k] = __ldg(rec + 2 * (size_t)id + 1);
             }
         }
 #pragma unroll
         for (int k = 0; k < GS_ITEMS; ++k) {
             const int i = base + k * GS_THREADS;
             if (i >= n) continue;
-            const unsigned id = (unsigned)it[k];
-            if (id >= (unsigned)n) {
+            if ((unsigned)it[k] >= (unsigned)n) {
                 atomicOr(err, DEVERR_BOUNDS);
                 continue;
             }
-            if (KEYS) {
-                keys[i] = (int)(it[k] >> 32);
-                perm[i] = src[k];
-            }
+            keys[i] = (int)(it[k] >> 32);
+            perm[i] = (int)__double_as_longlong(b[k].y);
             xs[i] = a[k].x;
             ys[i] = a[k].y;
-            vs[i] = w[k];
+            vs[i] = b[k].x;
         }
     }
 }
 
-// The records (x, y, v, 0) in input order, when the values arrive after the sort has started.
-__global__ __launch_bounds__(256) void k_pack_rec(const double *__restrict__ x,
-                                                  const double *__restrict__ y,
-                                                  const double *__restrict__ v, int n,
-                                                  double2 *__restrict__ rec) {
+// Late values, before they arrive: x and y in sorted order, gathered by the permutation from
+// the input arrays (off the critical path, while v is still being copied in).
+__global__ __launch_bounds__(256) void k_gather_xy(const int *__restrict__ perm,
+                                                   const double *__restrict__ x,
+                                                   const double *__restrict__ y, int n,
+                                                   double *__restrict__ xs,
+                                                   double *__restrict__ ys, unsigned *err) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        rec[2 * i] = make_double2(x[i], y[i]);
-        rec[2 * i + 1] = make_double2(v[i], 0.0);
+        const unsigned j = (unsigned)perm[i];
+        if (j >= (unsigned)n) {
+            atomicOr(err, DEVERR_BOUNDS);
+            continue;
+        }
+        xs[i] = __ldg(x + j);
+        ys[i] = __ldg(y + j);
+    }
+}
+
+// Late values, once they are in: v in sorted order (the one gather left after their arrival).
+__global__ __launch_bounds__(256) void k_gather_v(const int *__restrict__ perm,
+                                                  const double *__restrict__ v, int n,
+                                                  double *__restrict__ vs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned j = (unsigned)perm[i];
+        if (j < (unsigned)n) vs[i] = __ldg(v + j);
     }
 }
 
@@ -953,14 +937,14 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
                                 c.stream));
     // resident values: the records are written by the first pass, in buckets (see FirstPass);
-    // values that arrive later: items and records in input order (finish_sources)
+    // values that arrive later: items in input order; x, y, v gathered by the permutation
+    // in finish_sources
     const bool bucketed = values_ready == nullptr;
     if (bucketed)
         k_key_hist<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, npasses, hist);
     else
-        k_keys_pack<false><<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, nullptr, n, frame,
-                                                                      items_a, nullptr, npasses,
-                                                                      hist);
+        k_keys_pack<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, items_a, npasses,
+                                                               hist);
     TC_KERNEL_CHECK();
     k_hist_scan<<<NHIST, RS_RADIX, 0, c.stream>>>(hist, offsets);
     TC_KERNEL_CHECK();
@@ -985,7 +969,7 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     // a test stall leaves the passes' output unordered: report it before anything reads it
     if (c.test_stall == TC_STALL_SORT && (rc = check_device_errors(c, "source sort"))) return rc;
     if (values_ready) {
-        // the keys now (the tree needs nothing else); x/y/v in finish_sources
+        // the keys now (the tree needs nothing else); x, y, v in finish_sources
         k_items_split<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(items_a, n, keys, perm);
         TC_KERNEL_CHECK();
         c.late_x = x;
@@ -996,7 +980,7 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     }
     // a window of the sorted order in flight at a time (4 CTAs per SM): its records come from
     // a compact range of buckets, which stays in L2
-    k_gather_sources<true, true><<<grid_for(n, GS_THREADS * GS_ITEMS, 4), GS_THREADS, 0,
+    k_gather_sources<<<grid_for(n, GS_THREADS * GS_ITEMS, 4), GS_THREADS, 0,
                                     c.stream>>>(items_a, rec, n, keys, perm, xs, ys, vs, err);
     TC_KERNEL_CHECK();
     return TC_OK;
@@ -1005,15 +989,16 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
 int finish_sources(Context &c) {
     if (!c.late_ready) return TC_OK;
     const int n = c.nsrc;
+    const int *perm = slot_ptr<int>(c, S_PERM);
+    k_gather_xy<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(perm, c.late_x, c.late_y, n,
+                                                          slot_ptr<double>(c, S_XS),
+                                                          slot_ptr<double>(c, S_YS),
+                                                          slot_ptr<unsigned>(c, S_ERR));
+    TC_KERNEL_CHECK();
     TC_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.late_ready, 0));
     c.late_ready = nullptr;
-    double2 *rec = slot_ptr<double2>(c, S_REC);
-    k_pack_rec<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(c.late_x, c.late_y, c.late_v, n, rec);
-    TC_KERNEL_CHECK();
-    k_gather_sources<false><<<grid_for(n, GS_THREADS * GS_ITEMS, 8), GS_THREADS, 0, c.stream>>>(
-        slot_ptr<unsigned long long>(c, S_ITEMS_A), rec, n, nullptr, nullptr,
-        slot_ptr<double>(c, S_XS), slot_ptr<double>(c, S_YS), slot_ptr<double>(c, S_VS),
-        slot_ptr<unsigned>(c, S_ERR));
+    k_gather_v<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(perm, c.late_v, n,
+                                                         slot_ptr<double>(c, S_VS));
     TC_KERNEL_CHECK();
     return TC_OK;
 }
@@ -1076,14 +1061,13 @@ void kernels_sort(KernelList &v) {
     v.insert(v.end(), {(const void *)k_bbox, (const void *)k_target_keys,
                        (const void *)k_gather_items_inplace, (const void *)k_hist,
                        (const void *)k_hist_scan,
-                       (const void *)k_onesweep, (const void *)k_keys_pack<true>,
-                       (const void *)k_keys_pack<false>, (const void *)k_onesweep_items<true>,
+                       (const void *)k_onesweep, (const void *)k_keys_pack,
+                       (const void *)k_onesweep_items<true>,
                        (const void *)k_onesweep_items<false>, (const void *)k_key_hist,
                        (const void *)k_onesweep_items<true, true>,
                        (const void *)k_onesweep_items<false, true>,
-                       (const void *)k_gather_sources<true, true>,
-                       (const void *)k_gather_sources<true>, (const void *)k_gather_sources<false>,
-                       (const void *)k_pack_rec, (const void *)k_items_split,
+                       (const void *)k_gather_sources, (const void *)k_gather_xy,
+                       (const void *)k_gather_v, (const void *)k_items_split,
                        (const void *)k_scan_reduce, (const void *)k_scan_blocks,
                        (const void *)k_scan_apply});
 }
@@ -1143,8 +1127,8 @@ extern "C" TC_API int tc_sort_sources_noalloc(const double *xsources, const doub
     const int gb = std::min(grid_for(n, BBOX_THREADS, 8), NA_MAX_BBOX_BLOCKS);
     k_bbox<<<gb, BBOX_THREADS, 0, s>>>(xsources, ysources, n, partials, done, fr);
     TC_KERNEL_CHECK();
-    k_keys_pack<false><<<grid_for(n, 256, 8), 256, 0, s>>>(xsources, ysources, nullptr, n, fr,
-                                                           items_a, nullptr, npasses, hist);
+    k_keys_pack<<<grid_for(n, 256, 8), 256, 0, s>>>(xsources, ysources, n, fr, items_a, npasses,
+                                                    hist);
     TC_KERNEL_CHECK();
     k_hist_scan<<<npasses, RS_RADIX, 0, s>>>(hist, offsets);
     TC_KERNEL_CHECK();
