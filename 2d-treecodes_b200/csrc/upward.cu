@@ -6,7 +6,7 @@
 // node's mass, weights, com and radius level by level, deepest first (upward.cpp:95-218).
 // Expansions: k_leaf_p2e (one warp per leaf, lanes over sources, FP32 lane sums in the
 // mixed-precision form; kernels/upward-kernels.m4:18-93), then E2E deepest level first
-// (upward-kernels.m4:95-149): k_upward_wide (thread per inner node, cp.async staging) on wide
+// (upward-kernels.m4:95-149): k_upward_wide (four threads per inner node, one per child) on wide
 // levels, k_upward_level (warp per inner node) on narrow ones, k_upward_top (one block) on the
 // small top levels.  Inner node r of level l is addressed structurally (its children are
 // off[l+1] + 4r .. +3, its id is their cell's parent), so the E2E does not depend on the child
@@ -49,8 +49,7 @@ __device__ const BinomTable g_binom_up = make_binom_table();   // per-lane indic
 constexpr int UP_WARPS = 4;          // warps per block of the leaf and per-level merge kernels
 constexpr int UP_TOP_WARPS = 16;     // warps of the single-block launch over the top levels
 constexpr int UP_TOP_MAX_NODES = 64;     // a level this small joins the single-block launch
-constexpr int UP_WIDE_MIN_NODES = 2048;  // a level with this many inner nodes: thread per node
-constexpr int UP_WIDE_WARPS = 1;         // warps per block of the thread-per-node kernel
+constexpr int UP_WIDE_MIN_NODES = 2048;  // a level with this many inner nodes: k_upward_wide
 
 
 __device__ __forceinline__ bool is_leaf(int2 rg, int4 cl, int leafcap) {
@@ -525,55 +524,31 @@ __global__ __launch_bounds__(UP_WARPS * 32, 5) void k_upward_level(
     }
 }
 
-// Wide levels: one thread per inner node.  Inner node r of level l owns the children
-// off[l+1] + 4r .. +3 and is their common parent cell[off[l+1] + 4r].w.  A warp takes 32
-// consecutive inner nodes; child c of all 32 is staged through shared memory (coalesced runs of
-// 2P coefficients), transposed to one column per node, and every thread then shifts its own
-// child with the binomial sums fully unrolled (uniform constant-bank operands).
+// Wide levels, four threads per inner node (thread 4j + c shifts child c of the warp's j-th
+// node): 8 inner nodes per warp.  The warp's 32 children are consecutive (children of inner
+// node r are off[l+1] + 4r .. +3), so their coefficients are staged with coalesced loads; each
+// thread then holds its own child's scaled coefficients in registers, forms that child's
+// contribution to every coefficient of the parent with the binomial sums fully unrolled
+// (uniform constant-bank operands), and the four contributions are added through shared
+// memory.  A thread per node (all four children, the parent's coefficients accumulated in
+// shared memory) held 250 registers and 38 KB of shared memory per warp, 5 warps per SM; this
+// form holds 168 and 12.5 KB, 12 warps per SM.
+constexpr int UP_WIDE_MIN_BLOCKS = 12;
 template <int P>
 struct WideShared {
-    double a[2][2 * P][33];   // a[b][t][j]: coefficient t of node j's child, two buffers
-    double o[2 * P][33];      // o[t][j]: coefficient t of node j's result
-    int parent[32];
+    double c[32][2 * P + 1];   // row t: thread t's child coefficients, then its contribution
 };
 
-// 8-byte asynchronous global -> shared copies (no register staging), grouped per child.
-__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// Child c of the warp's 32 inner nodes r0.. into buf[t][j] (node j's 2P coefficients, column j).
 template <int P>
-__device__ __forceinline__ void stage_children(double (*buf)[33], const double *exps, int cbase,
-                                               int r0, int ninner, int c) {
-    for (int idx = lane_id(); idx < 32 * 2 * P; idx += 32) {
-        const int j = idx / (2 * P), t = idx - j * (2 * P);
-        if (r0 + j < ninner)
-            cp_async8(&buf[t][j], exps + (size_t)(cbase + 4 * (r0 + j) + c) * 2 * P + t);
-        else
-            buf[t][j] = 0.0;
-    }
-    cp_async_commit();
-}
-
-template <int P>
-__global__ __launch_bounds__(UP_WIDE_WARPS * 32, 8) void k_upward_wide(
+__global__ __launch_bounds__(32, UP_WIDE_MIN_BLOCKS) void k_upward_wide(
     int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
     const double *mass, const double *wgt, double *exps, unsigned *err) {
-    __shared__ WideShared<P> shared[UP_WIDE_WARPS];
-    WideShared<P> &st = shared[threadIdx.x >> 5];
-    const int lane = lane_id();
+    __shared__ WideShared<P> st;
+    const int lane = lane_id(), j = lane >> 2, c = lane & 3;
     const int cbase = lo.off[l + 1];
     const int ninner = (lo.off[l + 2] - cbase) / 4;
-    for (int r0 = (blockIdx.x * UP_WIDE_WARPS + (threadIdx.x >> 5)) * 32; r0 < ninner;
-         r0 += gridDim.x * UP_WIDE_WARPS * 32) {
-        const int r = r0 + lane;
+    for (int r0 = blockIdx.x * 8; r0 < ninner; r0 += gridDim.x * 8) {
+        const int r = r0 + j;
         const int cb = cbase + 4 * r;
         bool act = r < ninner;
         int parent = -1;
@@ -584,85 +559,69 @@ __global__ __launch_bounds__(UP_WIDE_WARPS * 32, 8) void k_upward_wide(
                 act = false;
             }
         }
-        st.parent[lane] = act ? parent : -1;
-        double cm[4], cw[4], cxc[4], cyc[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int id = act ? cb + c : 0;
-            cm[c] = mass[id];
-            cw[c] = wgt[id];
-            cxc[c] = tnode[id].xcom;
-            cyc[c] = tnode[id].ycom;
-        }
-        // the parent's com comes from the moments pass
+        const int id = act ? cb + c : 0;
+        const double m = mass[id], w = wgt[id];
+        const double cx = tnode[id].xcom, cy = tnode[id].ycom;
         const double px = act ? tnode[parent].xcom : 0.0, py = act ? tnode[parent].ycom : 0.0;
-        int zcount = 0, nz = 0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const bool negl = fabs(cw[c]) < 1.1e-16;
-            zcount += negl;
-            if (!negl) nz = c;
-        }
+        // the node's negligible children (its four threads' bits of the ballot)
+        const unsigned negl = __ballot_sync(FULL_MASK, act && fabs(w) < 1.1e-16);
+        const unsigned g = (negl >> (4 * j)) & 0xFu;
+        const int zcount = __popc(g);
+        const int nz = 31 - __clz((~g & 0xFu) | 1u);   // the last non-negligible child
         const bool shift = act && zcount <= 2;
-#pragma unroll
-        for (int k = 0; k < 2 * P; ++k) st.o[k][lane] = 0.0;
+        const bool copy = act && zcount == 3 && c == nz;
+        // the warp's 32 children, coalesced (zeros past the level)
         __syncwarp();
-        stage_children<P>(st.a[0], exps, cbase, r0, ninner, 0);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            double (*a)[33] = st.a[c & 1];
-            // the next child's copies run while this one is shifted
-            if (c < 3) {
-                stage_children<P>(st.a[(c + 1) & 1], exps, cbase, r0, ninner, c + 1);
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
+        {
+            const size_t first = (size_t)(cbase + 4 * r0) * 2 * P;
+            const int nchild = min(32, 4 * (ninner - r0));
+            for (int idx = lane; idx < 32 * 2 * P; idx += 32) {
+                const int ch = idx / (2 * P), t = idx - ch * (2 * P);
+                st.c[ch][t] = ch < nchild ? exps[first + idx] : 0.0;
             }
-            __syncwarp();
-            if (act && zcount == 3 && c == nz)
-#pragma unroll
-                for (int k = 0; k < 2 * P; ++k) st.o[k][lane] = a[k][lane];
-            if (shift) {
-                // C_k = a_{k-1} z0^-k in place, then
-                // out_l += z0^l (-m/l + sum_{k<=l} C(l-1, k-1) C_k)
-                const double x0 = cxc[c] - px, y0 = cyc[c] - py;
-                const double r2z0 = x0 * x0 + y0 * y0;
-                const cplx zinv = {x0 / r2z0, -y0 / r2z0};
-                cplx zp = zinv;
-#pragma unroll
-                for (int k = 0; k < P; ++k) {
-                    const cplx v = cmul({a[k][lane], a[P + k][lane]}, zp);
-                    a[k][lane] = v.re;
-                    a[P + k][lane] = v.im;
-                    zp = cmul(zp, zinv);
-                }
-                const cplx z0 = {x0, y0};
-                cplx zl = z0;
-#pragma unroll
-                for (int L = 1; L <= P; ++L) {
-                    double tr = L == 1 ? -cm[c] : cm[c] * (-1.0 / L), ti = 0.0;
-#pragma unroll
-                    for (int k = 1; k <= L; ++k) {
-                        const double b = c_binom_up.c[L - 1][k - 1];
-                        tr = fma(b, a[k - 1][lane], tr);
-                        ti = fma(b, a[P + k - 1][lane], ti);
-                    }
-                    const cplx o = cfma({tr, ti}, zl, {st.o[L - 1][lane], st.o[P + L - 1][lane]});
-                    st.o[L - 1][lane] = o.re;
-                    st.o[P + L - 1][lane] = o.im;
-                    zl = cmul(zl, z0);
-                }
-            }
-            // this buffer is restaged two children later: all lanes must be done with it
-            __syncwarp();
         }
-        // results written as runs of 2P per parent
         __syncwarp();
-        for (int idx = lane; idx < 32 * 2 * P; idx += 32) {
-            const int j = idx / (2 * P), t = idx - j * (2 * P);
-            const int pj = st.parent[j];
-            if (pj >= 0) exps[(size_t)pj * 2 * P + t] = st.o[t][j];
+        // C_k = a_{k-1} z0^-k of this thread's child
+        const double x0 = cx - px, y0 = cy - py;
+        double cr[P], ci[P];
+        {
+            const double r2z0 = x0 * x0 + y0 * y0;
+            const cplx zinv = shift ? cplx{x0 / r2z0, -y0 / r2z0} : cplx{0.0, 0.0};
+            cplx zp = zinv;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const cplx v = cmul({st.c[lane][k], st.c[lane][P + k]}, zp);
+                cr[k] = v.re;
+                ci[k] = v.im;
+                zp = cmul(zp, zinv);
+            }
         }
+        // this child's part of parent coefficient L: z0^L (-m/L + sum_{k<=L} C(L-1, k-1) C_k)
+        const cplx z0 = {x0, y0};
+        cplx zl = z0;
+#pragma unroll
+        for (int L = 1; L <= P; ++L) {
+            double tr = L == 1 ? -m : m * (-1.0 / L), ti = 0.0;
+#pragma unroll
+            for (int k = 1; k <= L; ++k) {
+                const double b = c_binom_up.c[L - 1][k - 1];
+                tr = fma(b, cr[k - 1], tr);
+                ti = fma(b, ci[k - 1], ti);
+            }
+            const cplx o = cmul({tr, ti}, zl);
+            zl = cmul(zl, z0);
+            // three negligible children: the fourth's coefficients unshifted; four: zero
+            const double a_re = st.c[lane][L - 1], a_im = st.c[lane][P + L - 1];
+            st.c[lane][L - 1] = shift ? o.re : (copy ? a_re : 0.0);
+            st.c[lane][P + L - 1] = shift ? o.im : (copy ? a_im : 0.0);
+        }
+        __syncwarp();
+        // the parent's coefficients t = c, c + 4, ...: its four children's parts in order
+        if (act)
+            for (int t = c; t < 2 * P; t += 4)
+                exps[(size_t)parent * 2 * P + t] =
+                    ((st.c[4 * j][t] + st.c[4 * j + 1][t]) + st.c[4 * j + 2][t]) +
+                    st.c[4 * j + 3][t];
     }
 }
 
@@ -788,10 +747,9 @@ static int run_expansions(Context &c) {
         const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
         if (ninner <= 0) continue;
         if (ninner >= UP_WIDE_MIN_NODES) {
-            const int g = (int)std::min<long long>(
-                (ninner + UP_WIDE_WARPS * 32 - 1) / (UP_WIDE_WARPS * 32), (long long)sms * 8);
-            k_upward_wide<P><<<g, UP_WIDE_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass,
-                                                                     w, exps, err);
+            const int g = (int)std::min<long long>((ninner + 7) / 8,
+                                                   (long long)sms * UP_WIDE_MIN_BLOCKS);
+            k_upward_wide<P><<<g, 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w, exps, err);
         } else {
             const int g = (int)std::min<long long>((ninner + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
             k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
