@@ -59,6 +59,34 @@ def test_stream_results_equal_solo(precision):
     assert summary["p99_ms"] >= summary["p50_ms"] > 0
 
 
+def test_wait_any_collects_each_request_once_in_completion_order():
+    """tc_server_wait_any: every ticket exactly once, completion stamps (CLOCK_MONOTONIC, the
+    clock of time.perf_counter) non-decreasing and within the call, each result equal to the
+    request solved alone; with nothing outstanding it reports so at once."""
+    import time
+    specs = S.make_stream(nreq=24, rate_hz=5000.0, seed=57, log2_min=10, log2_max=LOG2_MAX,
+                          followup_share=0.0)
+    m = S.Materialiser(log2_max=LOG2_MAX, seed=77)
+    datas = [m(s) for s in specs]
+    srv = T.Server(slots=4, hbm_budget_bytes=8 << 30, device=0)
+    try:
+        t0 = time.perf_counter()
+        tickets = [S.submit(srv, s, d, 1) for s, d in zip(specs, datas)]
+        got, stamps = {}, []
+        for _ in tickets:
+            t, outs, res = srv.wait_any()
+            assert t in tickets and t not in got
+            got[t] = outs
+            stamps.append(res["finished_s"])
+        t1 = time.perf_counter()
+        with pytest.raises(T.TreecodeError, match="no request outstanding"):
+            srv.wait_any()
+    finally:
+        srv.close()
+    assert stamps == sorted(stamps) and t0 <= stamps[0] and stamps[-1] <= t1
+    assert_same([got[t] for t in tickets], [solo(s, d, 1) for s, d in zip(specs, datas)])
+
+
 def test_budget_limits_concurrency_and_evicts():
     specs = S.make_stream(nreq=24, rate_hz=5000.0, seed=41, log2_min=14, log2_max=LOG2_MAX,
                           followup_share=0.4)
