@@ -294,12 +294,12 @@ def cpu_reference_step(w, sample_targets=1 << 19):
     return wall, desc
 
 
-def bench_config(w, precision, flush_desc):
-    """The `config` object of both arms: the same keys, only `precision` differs."""
+def bench_config(w, flush_desc):
+    """The `config` object of both arms: the workload alone, identical in both (the arithmetic
+    is in each line's `dtype` and `precision`)."""
     return {"workload": w["name"], "theta": w["theta"],
             "order": ORDER_FORCE if w["kind"] == "force" else 12,
-            "sources": len(w["xs"]), "targets": n_targets(w), "precision": precision,
-            "l2": flush_desc}
+            "sources": len(w["xs"]), "targets": n_targets(w), "l2": flush_desc}
 
 
 def l2_desc(w):
@@ -329,7 +329,8 @@ def run_reference(args, ws, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded PCG64; the reference's datasets are not available)",
-        "config": bench_config(w, "fp64", l2_desc(w)),
+        "precision": "fp64",
+        "config": bench_config(w, l2_desc(w)),
         "cpu_baseline": {"value": val, "unit": "Mtargets/s", "cores": cores, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": val, "unit": "Mtargets/s", "h2d_bytes_per_step": 0,
@@ -622,7 +623,8 @@ def run_b200(args, ws, rank, local):
             "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "f32+f64" if mixed else "f64",
             "data": "synthetic (seeded PCG64; the reference's datasets are not available)",
-            "config": bench_config(w, args.precision, l2_desc(w)),
+            "precision": args.precision,
+            "config": bench_config(w, l2_desc(w)),
             "parallelism": (f"{ws} independent solves (one per GPU)" if not strong else
                             f"one problem split over {ws} GPUs (tree built on every GPU)"),
             "accuracy": acc,
