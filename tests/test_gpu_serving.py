@@ -204,12 +204,39 @@ def test_trimmed_memory_stays_cached_until_released():
         keep.close()
 
 
+def test_reserved_memory_serves_later_solves():
+    """tc_reserve_cached_memory maps memory into the device pool ahead of the solves: device
+    free memory drops by about the amount, a solve afterwards is carved from it (free memory
+    does not drop again), and tc_release_cached_memory hands the unused part back."""
+    import torch
+    import workloads as W
+    w = W.lamb_oseen_force(n=1 << 20, blocks_per_side=4, h=1.0 / 128)
+    free = lambda: torch.cuda.mem_get_info(0)[0]
+    keep = T.Context(device=0)   # a live context: the pool keeps what is freed into it
+    ctx = T.Context(device=0)
+    try:
+        T.release_cached_memory(0)
+        f0 = free()
+        T.reserve_cached_memory(2 << 30, 0)
+        f1 = free()
+        assert f0 - f1 >= (2 << 30) * 9 // 10, (f0, f1)
+        ctx.force_mrag_host(w["theta"], w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"], w["hs"])
+        assert 0 < ctx.device_bytes() < 1 << 30
+        f2 = free()
+        assert f1 - f2 < 64 << 20, (f1, f2, ctx.device_bytes())
+        T.release_cached_memory(0)
+        assert free() - f2 >= 1 << 30
+    finally:
+        ctx.close()
+        keep.close()
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_concurrent_contexts_equal_solo(precision):
     """Four threads, each with its own context, solve half-million-source force problems at
     once, repeatedly: every result equals the problem solved alone, bit for bit.  Each solve
-    runs work on two streams of its context (the auxiliary one at the lower priority), so this
-    exercises the ordering between them under load from the other contexts."""
+    runs work on two streams of its context, so this exercises the ordering between them under
+    load from the other contexts."""
     import threading
     import workloads as W
     ws = [W.lamb_oseen_force(n=1 << 19, blocks_per_side=8, h=1.0 / 256, seed=50 + i)
