@@ -128,6 +128,25 @@ def test_small_source_counts(gpu_ctx, n):
     assert rel_l2(np.r_[xo, yo], np.r_[rx, ry]) < TOL
 
 
+@pytest.mark.parametrize("n", [2047, 2049, 3071, 3072, 3073, 6145, 16385])
+def test_sort_tile_boundaries_and_host_path(gpu_ctx, n):
+    """Source counts at the radix passes' tile edges (3072 items) and the gather's (2048):
+    keys, sorted sources, permutation and tree bit-exact with the oracle (device path, values
+    resident); the host entry point, whose sort gathers x and y before v arrives, gives the
+    device path's outputs bit for bit."""
+    r = np.random.default_rng(n)
+    w = dict(xs=r.random(n), ys=r.random(n), vs=r.uniform(-1, 1, n))
+    live_tree_check(gpu_ctx, "potential", w)
+    w["xt"], w["yt"] = r.random(300), r.random(300)
+    out = gpu_potential(gpu_ctx, w, 0.5)
+    assert np.array_equal(gpu_ctx.potential_host(0.5, w["xs"], w["ys"], w["vs"], w["xt"],
+                                                 w["yt"]), out)
+    w.update(x0s=np.array([0.1, 0.5]), y0s=np.array([0.2, 0.6]), hs=np.array([0.01, 0.005]))
+    xo, yo = gpu_force(gpu_ctx, w, 0.5)
+    hx, hy = gpu_ctx.force_mrag_host(0.5, w["xs"], w["ys"], w["vs"], w["x0s"], w["y0s"], w["hs"])
+    assert np.array_equal(hx, xo) and np.array_equal(hy, yo)
+
+
 def test_zero_sources_give_zero_output(gpu_ctx):
     e = np.zeros(0)
     out = gpu_ctx.potential_host(0.5, e, e, e, np.array([0.1, 0.2]), np.array([0.3, 0.4]))
