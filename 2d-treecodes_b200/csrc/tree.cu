@@ -274,9 +274,11 @@ __global__ void k_tree_root(int n, int leafcap, TNode *tnode, int2 *range, int4 
     if (n <= leafcap) tnode[0].child = -1;
 }
 
-// One thread per inner cell: the r-th inner cell of level l is started by list entry
-// inv[l][r] (source s = lpos[j]).  Its children's ranges come from searches for the child key
-// boundaries inside [s, e), e the first key past the cell; its own id from its parent's rank.
+// Four threads per inner cell: the r-th inner cell of level l is started by list entry
+// inv[l][r] (source s = lpos[j]); its own id comes from its parent's rank.  Thread q of the four
+// finds the end of child q (the key boundary of child q + 1, or of the cell's end for q = 3) by
+// a search from s; the four searches run at once instead of one after another (each boundary
+// lies inside [s, e), since the keys are sorted), and thread q writes child q.
 __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap,
                                 const int *__restrict__ lpos,
                                 const unsigned short *__restrict__ lmask,
@@ -284,8 +286,12 @@ __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap
                                 int stride, int ninner, LevelOffsets lo, int nnodes,
                                 TNode *__restrict__ tnode, int2 *__restrict__ range,
                                 int4 *__restrict__ cell, unsigned *err) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ninner; t += gridDim.x * blockDim.x) {
-        // level of inner cell t: the inner cells are numbered level by level
+    const int q = threadIdx.x & 3;
+    const unsigned gmask = 0xFu << (lane_id() & ~3);   // the cell's four lanes
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < ninner;
+         t += (gridDim.x * blockDim.x) >> 2) {
+        // level of inner cell t: the inner cells are numbered level by level (the four threads
+        // compute the same values, so they branch together)
         int l = 0, r = t;
         while (l < LMAX - 1 && r >= (lo.off[l + 2] - lo.off[l + 1]) / 4) {
             r -= (lo.off[l + 2] - lo.off[l + 1]) / 4;
@@ -295,13 +301,12 @@ __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap
         const int s = lpos[j];
         const unsigned mj = lmask[j];
         if (!((mj >> l) & 1u)) {
-            atomicOr(err, DEVERR_TREE);
+            if (q == 0) atomicOr(err, DEVERR_TREE);
             continue;
         }
         const int key = keys[s];
         const int shift = 2 * (LMAX - l);
         const int P = l == 0 ? 0 : (key >> shift);
-        const int e = l == 0 ? n : gallop_lower_bound(keys, s, n, (P + 1) << shift);
         int id = 0;
         if (l > 0) {
             // The parent is the inner cell of level l-1 that holds source s: the last list
@@ -309,32 +314,34 @@ __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap
             // before s).  Its rank is the count of such entries up to j, minus one.
             const int prank = rank[(size_t)(l - 1) * stride + j] + (int)((mj >> (l - 1)) & 1u) - 1;
             if (prank < 0) {
-                atomicOr(err, DEVERR_TREE);
+                if (q == 0) atomicOr(err, DEVERR_TREE);
                 continue;
             }
             id = lo.off[l] + 4 * prank + (P & 3);
         }
         const int base = lo.off[l + 1] + 4 * r;
         if (id < 0 || id >= nnodes || base < 0 || base + 4 > nnodes) {
-            atomicOr(err, DEVERR_BOUNDS);
+            if (q == 0) atomicOr(err, DEVERR_BOUNDS);
             continue;
         }
-        tnode[id].child = base;
+        if (q == 0) tnode[id].child = base;
         const int cshift = shift - 2;
-        int b[5];
-        b[0] = s;
-        b[4] = e;
-        for (int c = 1; c < 4; ++c) b[c] = gallop_lower_bound(keys, b[c - 1], e, ((P << 2) | c) << cshift);
+        // the end of child q: the first key of child q + 1, or past the cell for q = 3
+        int end_q;
+        if (q < 3)
+            end_q = gallop_lower_bound(keys, s, n, ((P << 2) | (q + 1)) << cshift);
+        else
+            end_q = l == 0 ? n : gallop_lower_bound(keys, s, n, (P + 1) << shift);
+        int beg_q = __shfl_up_sync(gmask, end_q, 1, 4);
+        if (q == 0) beg_q = s;
         const int cx = compact_bits(P), cy = compact_bits(P >> 1);
-        for (int c = 0; c < 4; ++c) {
-            const int cid = base + c;
-            const int cnt = b[c + 1] - b[c];
-            range[cid] = make_int2(b[c], b[c + 1]);
-            cell[cid] = make_int4(l + 1, 2 * cx + (c & 1), 2 * cy + (c >> 1), id);
-            tnode[cid].count = cnt;
-            const bool inner = cnt > leafcap && l + 1 < LMAX;
-            if (!inner) tnode[cid].child = -1;
-        }
+        const int cid = base + q;
+        const int cnt = end_q - beg_q;
+        range[cid] = make_int2(beg_q, end_q);
+        cell[cid] = make_int4(l + 1, 2 * cx + (q & 1), 2 * cy + (q >> 1), id);
+        tnode[cid].count = cnt;
+        const bool inner = cnt > leafcap && l + 1 < LMAX;
+        if (!inner) tnode[cid].child = -1;
     }
 }
 
@@ -427,7 +434,7 @@ int build_topology(Context &c, int leafcap) {
     k_tree_root<<<1, 1, 0, c.stream>>>(n, leafcap, tnode, range, cell);
     TC_KERNEL_CHECK();
     if (ninner > 0) {
-        k_tree_children<<<grid_for_tree((int)ninner, 128), 128, 0, c.stream>>>(
+        k_tree_children<<<grid_for_tree(4 * (int)ninner, 128), 128, 0, c.stream>>>(
             keys, n, leafcap, lpos, lmask, rank, rinv, cap, (int)ninner, lo, c.nnodes, tnode, range,
             cell, slot_ptr<unsigned>(c, S_ERR));
         TC_KERNEL_CHECK();
