@@ -9,6 +9,9 @@
 // that arrive while others are on the GPU start as soon as a slot and memory are free
 // (continuous batching of independent solves).
 //
+// Slots: with three or more, the last one is an express slot for requests of at most 2^17
+// sources; the others take any request.
+//
 // Admission (under the server lock):
 //   * a request of client k is admissible only when no earlier request of k is queued or in
 //     service, so one client's steps run in submission order on its resident buffers;
@@ -104,6 +107,10 @@ struct tc_server {
 };
 
 namespace {
+
+// With three slots or more, the last slot takes only requests of at most this many sources, so
+// that small requests do not queue behind a burst of large ones that holds every slot.
+constexpr int EXPRESS_MAX_SOURCES = 1 << 17;
 
 size_t footprint_estimate(int kind, long long n, long long ntargets, long long nblocks,
                           int precision) {
@@ -212,6 +219,9 @@ Job *tc_server::pick(int slot, size_t *reserve, tc_context **ctx) {
             auto ci = clients.find(k);
             if (ci != clients.end() && ci->second.busy) continue;
         }
+        // the express slot leaves large requests to the others (after the client bookkeeping
+        // above, so that a later step of the same client cannot overtake a skipped one)
+        if (nslots >= 3 && slot == nslots - 1 && j->req.nsources > EXPRESS_MAX_SOURCES) continue;
         const size_t held = k > 0 ? (clients.count(k) ? clients[k].bytes : 0) : pool_bytes[slot];
         // the charge: the estimate scaled by the learned actual/estimate ratio, at most the
         // whole budget, so that admitting it never charges more than the budget

@@ -19,6 +19,7 @@ arrival to its completion, so a submitter that falls behind shows up as latency.
 """
 from __future__ import annotations
 
+import gc
 import math
 import threading
 import time
@@ -210,6 +211,11 @@ def run_stream(server, specs, precision, materialise, keep_outputs=False):
                 outputs[i] = outs
 
     th = threading.Thread(target=collector)
+    # no cyclic garbage collection while the stream runs: a full collection holds the
+    # interpreter lock, during which neither the submitting nor the collecting thread runs
+    gc.collect()
+    gc_was_on = gc.isenabled()
+    gc.disable()
     th.start()
     t0 = time.perf_counter()
     count = 0
@@ -230,6 +236,8 @@ def run_stream(server, specs, precision, materialise, keep_outputs=False):
             submitted[0] = count
         permits.release()
         th.join()
+        if gc_was_on:
+            gc.enable()
     if errors:
         raise T.TreecodeError(f"{len(errors)} requests failed, first: {errors[0]}")
     lat = np.array([(r["t_done"] - t0) * 1e3 - s["t"] * 1e3 for r, s in zip(records, specs)])

@@ -292,8 +292,10 @@ typedef struct {
     int slots, max_in_service, resident_clients;
 } tc_server_stats;
 
-/* slots: concurrent solves (>= 1); hbm_budget_bytes: device memory the server may hold, which
- * it maps into the device's pool at creation (tc_reserve_cached_memory). */
+/* slots: concurrent solves (>= 1); with 3 or more, the last slot serves only requests of at
+ * most 2^17 sources, so that small requests do not queue behind a burst of large ones.
+ * hbm_budget_bytes: device memory the server may hold, which it maps into the device's pool at
+ * creation (tc_reserve_cached_memory). */
 TC_API int tc_server_create(tc_server **srv, int device, int slots, size_t hbm_budget_bytes);
 /* Waits for all submitted requests, then frees every context. */
 TC_API void tc_server_destroy(tc_server *srv);
