@@ -27,7 +27,18 @@ int main(int argc, char **argv) {
     for (int trial = 0; trial < trials; ++trial) {
         const size_t budget = (size_t)(24 + rng() % 400) << 20;
         tc_server *s;
-        if (tc_server_create(&s, 0, 1 + rng() % 4, budget)) return 10;
+        const int nslots = 1 + rng() % 4;
+        if (tc_server_create(&s, 0, nslots, budget)) return 10;
+        // with 3 slots or more the last one (the express slot) runs only requests of at most
+        // 2^17 sources
+        auto check_slot = [&](const tc_request_result &res, int nsrc) {
+            if (nslots >= 3 && nsrc > (1 << 17) && res.slot == nslots - 1) {
+                fprintf(stderr, "trial %d: a request of %d sources ran on the express slot\n",
+                        trial, nsrc);
+                ++failures;
+            }
+        };
+        std::vector<int> nsrc_of;
         const int nreq = 40 + rng() % 40;
         std::vector<std::vector<double>> in(nreq), out(nreq);
         std::vector<long long> tickets;
@@ -40,6 +51,7 @@ int main(int argc, char **argv) {
             // client ids are unique to the trial (at most 8 per trial, below 1024 overall)
             r.client = (rng() % 3 == 0) ? 1 + (trial % 120) * 8 + rng() % 5 : 0;
             r.nsources = 1000 + rng() % 150000;
+            nsrc_of.push_back(r.nsources);
             in[i] = {(double)r.client, (double)(r.client > 0 ? ++seq[r.client] : 0)};
             r.xsources = r.ysources = r.sourcevalues = in[i].data();
             marker[i] = in[i][0] * 1e6 + in[i][1];
@@ -64,6 +76,7 @@ int main(int argc, char **argv) {
             for (int i = 0; i < nreq; ++i) {
                 tc_request_result res;
                 if (tc_server_wait(s, tickets[i], &res) != 0) ++failures;
+                check_slot(res, nsrc_of[i]);
                 for (double v : out[i])
                     if (v != marker[i]) ++failures;
             }
@@ -90,6 +103,7 @@ int main(int argc, char **argv) {
                 }
                 const int i = it->second;
                 index.erase(it);
+                check_slot(res, nsrc_of[i]);
                 if (res.finished_s < last) ++failures;
                 last = res.finished_s;
                 for (double v : out[i])
