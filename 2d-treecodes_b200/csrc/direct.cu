@@ -91,8 +91,10 @@ int direct_force(Context &c, const double *xs, const double *ys, const double *v
 // ---------------------------------------------------------------------------- log probe
 // out[2i] = log_pos(x[i]) (the potential kernels' logarithm), out[2i + 1] = the library log.
 __global__ void k_log_probe(const double *__restrict__ x, int n, double *__restrict__ out) {
+    __shared__ double s_neg_log_c[LOG_NTAB];
+    load_log_table(s_neg_log_c);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        out[2 * i] = log_pos(x[i]);
+        out[2 * i] = log_pos(x[i], s_neg_log_c);
         out[2 * i + 1] = log(x[i]);
     }
 }

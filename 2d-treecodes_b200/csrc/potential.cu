@@ -299,6 +299,8 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
     __shared__ float4 s_ny[PE_WARPS][PE_CHUNK / 2];
     __shared__ float2 s_v2[PE_WARPS][PE_CHUNK / 2];
     __shared__ double s_part[PE_WARPS][32];        // P2P lane partials of a sparse mask
+    __shared__ double s_neg_log_c[LOG_NTAB];       // log_pos's table
+    load_log_table(s_neg_log_c);
     const int lane = lane_id(), warp = threadIdx.x >> 5;
     const double eps = 10 * DBL_EPSILON;
     const int *toff = offs + 2 * ngroups;
@@ -394,14 +396,15 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                             qr2.x + fmaf(ur, qr2.y, -ui * qi2.y),
                             qi2.x + fmaf(ur, qi2.y, ui * qr2.y));
                         two_sum_add(sh, sl, ur * q.x - ui * q.y);
-                        far += mm * log_pos(r2) * 0.5;
+                        far += mm * log_pos(r2, s_neg_log_c) * 0.5;
                     } else {
                         const double inv = 1.0 / r2;
                         const cplx u = {rz * inv, -iz * inv};
                         cplx q = s_coef[warp][P - 1];
 #pragma unroll
                         for (int k = P - 2; k >= 0; --k) q = cfma(q, u, s_coef[warp][k]);
-                        far += mm * log_pos(r2) * 0.5 + (u.re * q.re - u.im * q.im);
+                        far += mm * log_pos(r2, s_neg_log_c) * 0.5 +
+                               (u.re * q.re - u.im * q.im);
                     }
                 }
             }
@@ -525,7 +528,8 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                             for (int q = 0; q < cnt; ++q) {
                                 const double2 sp = s_xy[warp][q];
                                 const double xr = x - sp.x, yr = y - sp.y;
-                                near += log_pos(xr * xr + yr * yr + eps) * s_v[warp][q];
+                                near += log_pos(fma(xr, xr, fma(yr, yr, eps)), s_neg_log_c) *
+                                        s_v[warp][q];
                             }
                         }
                     }
@@ -558,7 +562,8 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                             for (int q = lane / k; q < cnt; q += r) {
                                 const double2 sp = s_xy[warp][q];
                                 const double xr = qx - sp.x, yr = qy - sp.y;
-                                part += log_pos(xr * xr + yr * yr + eps) * s_v[warp][q];
+                                part += log_pos(fma(xr, xr, fma(yr, yr, eps)), s_neg_log_c) *
+                                        s_v[warp][q];
                             }
                     }
                     s_part[warp][lane] = part;

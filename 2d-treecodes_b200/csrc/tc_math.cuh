@@ -2,6 +2,7 @@
 #pragma once
 
 #include "tc_common.cuh"
+#include "tc_log_table.cuh"
 
 namespace tc {
 
@@ -23,40 +24,45 @@ constexpr BinomTable make_binom_table() {
 }
 
 // Natural logarithm of a positive normal double, for the potential kernels' log r^2 terms
-// (arguments r^2 + 10 eps or |z|^2 of a far cell, never zero, subnormal or infinite).  From the
-// mathematics: x = 2^e m with m in [sqrt(1/2), sqrt(2)), s = (m - 1) / (m + 1), and
-// log m = 2 atanh s = 2 s (1 + s^2 q(s^2)), q(z) = (atanh(sqrt z) / sqrt z - 1) / z; log x =
-// e ln 2 + log m, with ln 2 split into a head of 21 bits (e * head exact) and a tail.  q is the
-// degree-6 interpolant of it at the 7 first-kind Chebyshev nodes of z in [0, ((sqrt 2 - 1) /
-// (sqrt 2 + 1))^2] (error below 2e-16, which the factor z <= 0.0295 scales to under 2^-57 of
-// log m); fit_log_poly.py beside this file regenerates the coefficients.  The division is a refined reciprocal (rcp_nr).  About 25 instructions against the
-// library log's ~100; within a few ulp of it (tests/test_gpu_parity.py checks the bound on
-// 2^20 arguments).
-__device__ __forceinline__ double log_pos(double x) {
-    const int lo = __double2loint(x);
-    int hi = __double2hiint(x);
-    int e = (hi >> 20) - 1023;
-    int mh = (hi & 0x000fffff) | 0x3ff00000;   // m in [1, 2)
-    if (mh > 0x3ff6a09e) {                     // m above sqrt(2) (to 20 bits): halve it
-        mh -= 0x00100000;
-        ++e;
-    }
-    const double m = __hiloint2double(mh, lo);
-    const double f = m - 1.0;
-    const double s = f * rcp_nr(2.0 + f);
-    const double z = s * s;
-    double q = 0x1.2b584aae78a57p-4;
-    q = fma(q, z, 0x1.39fe606542ddep-4);
-    q = fma(q, z, 0x1.7462b4ab2ef6bp-4);
-    q = fma(q, z, 0x1.c71c62e5800a1p-4);
-    q = fma(q, z, 0x1.2492492df148dp-3);
-    q = fma(q, z, 0x1.99999999952e2p-3);
-    q = fma(q, z, 0x1.5555555555558p-2);
-    const double two_s = 2.0 * s;
-    const double logm = fma(two_s * z, q, two_s);
-    constexpr double LN2_HEAD = 0x1.62e42p-1, LN2_TAIL = 0x1.fdf473de6af28p-22;
-    const double de = (double)e;
-    return fma(de, LN2_HEAD, fma(de, LN2_TAIL, logm));
+// (arguments r^2 + 10 eps or |z|^2 of a far cell, never zero, subnormal or infinite).
+// Table-driven, after Tang's method (P. T. P. Tang, ACM TOMS 16(4), 1990): x = 2^e m with m in
+// [sqrt(1/2), sqrt(2)); c = the single-precision reciprocal of m (from its top 20 fraction bits)
+// rounded to 10 significant bits, so that r = m c - 1 is exact in one fma (m c has at most 62
+// significant bits and |r| <= 2^-10 (1 + 2^-7)); log x = e ln 2 - log c + log1p(r), log1p(r) =
+// r + r^2 q(r) with q of degree 3.  -log c comes from a table of LOG_NTAB doubles indexed by the
+// rounded float bits of c, which the caller keeps in shared memory (load_log_table); m is in
+// [sqrt(1/2), sqrt(2)) by construction, which puts the index in [20, 532] for any x.  The last
+// step, e ln 2 + (-log c + log1p r), rounds twice: for e = 0 only the sum, and for e != 0 the
+// result is at least ln 2 / 2 in size, so ln 2's own rounding (2^-55) stays below half an ulp of
+// it.  fit_log_table.py beside this file writes the table and q (tc_log_table.cuh).  8 FP64
+// operations, one single-precision reciprocal, one conversion and one shared load, against the
+// library log's ~100 instructions; within 2 ulp of the exact logarithm (tests/test_gpu_parity.py
+// checks 4 ulp against the library log on 2^20 arguments).
+__device__ __forceinline__ double log_pos(double x, const double *__restrict__ neg_log_c) {
+    const int ix = __double2hiint(x) - 0x3fe6a09f;   // high word of sqrt(1/2), rounded up
+    const int e = ix >> 20;
+    const int mf = ix & 0x000fffff;                 // fraction bits of m, offset
+    const double m = __hiloint2double(mf + 0x3fe6a09f, __double2loint(x));
+    const float mfl = __int_as_float((mf << 3) + (0x07e6a09f << 3));   // m to 20 bits, as float
+    float rc;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(mfl));
+    // round the reciprocal to 10 significant bits: key = its float bits >> LOG_KEY_SHIFT
+    const unsigned key = (__float_as_uint(rc) + (1u << (LOG_KEY_SHIFT - 1))) >> LOG_KEY_SHIFT;
+    const double c = __hiloint2double((int)(key << (LOG_KEY_SHIFT - 3)) + (896 << 20), 0);
+    const double r = fma(m, c, -1.0);
+    double q = LOG_Q3;
+    q = fma(q, r, LOG_Q2);
+    q = fma(q, r, LOG_Q1);
+    q = fma(q, r, LOG_Q0);
+    const double p = fma(r * r, q, r);
+    constexpr double LN2 = 0x1.62e42fefa39efp-1;
+    return fma((double)e, LN2, neg_log_c[(int)key - LOG_IDX_BASE] + p);
+}
+
+// Copies log_pos's table into the block's shared memory; every thread of the block calls it.
+__device__ __forceinline__ void load_log_table(double *s_neg_log_c) {
+    for (int i = threadIdx.x; i < LOG_NTAB; i += blockDim.x) s_neg_log_c[i] = LOG_NEG_LOG_C[i];
+    __syncthreads();
 }
 
 struct cplx {

@@ -251,7 +251,7 @@ def test_gpu_direct_sum_matches_cpu_direct_sum(gpu_ctx):
 
 
 def test_potential_log_within_a_few_ulp_of_the_library(gpu_ctx):
-    """The potential kernels' own logarithm (log_pos: atanh series on the reduced mantissa)
+    """The potential kernels' own logarithm (log_pos: table-driven reduction and log1p series)
     against CUDA's log on 2^20 arguments spanning the range the kernels feed it (r^2 + 10 eps
     from ~2e-15 up, far-cell |z|^2), plus arguments next to 1, to powers of two and to the
     sqrt(2) split of the reduction."""
