@@ -524,7 +524,7 @@ __global__ __launch_bounds__(PE_WARPS * 32) void k_potential_eval(
                             }
                             two_sum_add(nh, nl, (acc.x + acc.y) * ln2);
                         } else {
-#pragma unroll 2
+#pragma unroll 4
                             for (int q = 0; q < cnt; ++q) {
                                 const double2 sp = s_xy[warp][q];
                                 const double xr = x - sp.x, yr = y - sp.y;
