@@ -237,7 +237,7 @@ Job *tc_server::pick(int slot, size_t *reserve, tc_context **ctx) {
             j->admitted = j->finished = Clock::now();
             j->result.finished_s = monotonic_s();
             j->done = true;
-        done_order.push_back(j->ticket);
+            done_order.push_back(j->ticket);
             ++failed;
             ++completed;
             cv_done.notify_all();
