@@ -50,6 +50,7 @@ __global__ __launch_bounds__(BBOX_THREADS) void k_bbox(const double *__restrict_
                                                        const double *__restrict__ y, int n,
                                                        double4 *partials, unsigned *done,
                                                        Frame *frame) {
+    pdl_begin();
     double xmi = 1e13, xma = 0, ymi = 1e13, yma = 0;
     auto take = [&](double xv, double yv) {
         xmi = fmin(xmi, xv);
@@ -186,6 +187,7 @@ __global__ __launch_bounds__(256) void k_hist(const int *__restrict__ keys, int 
 
 __global__ __launch_bounds__(RS_RADIX) void k_hist_scan(const int *__restrict__ hist,
                                                         int *__restrict__ offsets) {
+    pdl_begin();
     const int p = blockIdx.x;
     const int v = hist[p * RS_RADIX + threadIdx.x];
     offsets[p * RS_RADIX + threadIdx.x] = block_exclusive_scan(v, nullptr);
@@ -362,6 +364,7 @@ __global__ __launch_bounds__(256) void k_keys_pack(const double *__restrict__ x,
                                                    const Frame *__restrict__ frame,
                                                    unsigned long long *__restrict__ items,
                                                    int npasses, int *__restrict__ hist) {
+    pdl_begin();
     __shared__ int s[RS_MAX_PASSES][RS_RADIX];
     for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
     __syncthreads();
@@ -423,6 +426,7 @@ __global__ __launch_bounds__(256) void k_key_hist(const double *__restrict__ x,
                                                   const double *__restrict__ y, int n,
                                                   const Frame *__restrict__ frame, int npasses,
                                                   int *__restrict__ hist) {
+    pdl_begin();
     __shared__ int s[RS_MAX_PASSES + 1][RS_RADIX];
     for (int i = threadIdx.x; i < (RS_MAX_PASSES + 1) * RS_RADIX; i += blockDim.x)
         (&s[0][0])[i] = 0;
@@ -489,6 +493,7 @@ __global__ __launch_bounds__(PS_THREADS, FIRST ? 3 : 4) void k_onesweep_items(
     const unsigned long long *__restrict__ in, unsigned long long *__restrict__ out, int n,
     int shift, const int *__restrict__ digit_offsets, unsigned *status, int *tile_counter,
     unsigned *err, int spin_limit, int stall_tile, unsigned *sink, FirstPass fp) {
+    pdl_begin();
     __shared__ unsigned long long s_items[PS_TILE];
     __shared__ int s_whist[PS_WARPS][RS_RADIX];
     __shared__ int s_count[RS_RADIX];
@@ -662,6 +667,7 @@ __global__ __launch_bounds__(GS_THREADS) void k_gather_sources(
     const unsigned long long *__restrict__ items, const double2 *__restrict__ rec, int n,
     int *__restrict__ keys, int *__restrict__ perm, double *__restrict__ xs,
     double *__restrict__ ys, double *__restrict__ vs, unsigned *err) {
+    pdl_begin();
     const int stride = gridDim.x * GS_THREADS * GS_ITEMS;
     for (int base = blockIdx.x * GS_THREADS * GS_ITEMS + threadIdx.x; base < n; base += stride) {
         unsigned long long it[GS_ITEMS];
@@ -729,6 +735,7 @@ __global__ __launch_bounds__(256) void k_gather_v(const int *__restrict__ perm,
 __global__ __launch_bounds__(256) void k_items_split(const unsigned long long *__restrict__ items,
                                                      int n, int *__restrict__ keys,
                                                      int *__restrict__ perm) {
+    pdl_begin();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const unsigned long long it = items[i];
         keys[i] = (int)(it >> 32);
@@ -906,9 +913,6 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
         return rc;
     partials = reinterpret_cast<double4 *>(reinterpret_cast<char *>(frame) + 64);
     unsigned *done = reinterpret_cast<unsigned *>(partials + gb);
-    TC_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned), c.stream));
-    k_bbox<<<gb, BBOX_THREADS, 0, c.stream>>>(x, y, n, partials, done, frame);
-    TC_KERNEL_CHECK();
 
     // four 8-bit passes over the (key, index) items, then one gather of the records
     if (n >= (1 << 30)) {
@@ -932,21 +936,27 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     int *offsets = hist + NHIST * RS_RADIX;
     unsigned *sink = status + (size_t)RS_MAX_PASSES * ntiles * RS_RADIX;   // after every pass
     int *bucket_fill = counter + RS_MAX_PASSES;
+    // every buffer and counter first, so that the sort's kernels follow each other directly on
+    // the stream (each may then be scheduled while the one before it drains, launch_pdl)
+    TC_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(unsigned), c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * NHIST * RS_RADIX, c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int) * (RS_MAX_PASSES + NB_BUCKETS), c.stream));
     TC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)npasses * ntiles * RS_RADIX,
                                 c.stream));
+    k_bbox<<<gb, BBOX_THREADS, 0, c.stream>>>(x, y, n, partials, done, frame);
+    TC_KERNEL_CHECK();
     // resident values: the records are written by the first pass, in buckets (see FirstPass);
     // values that arrive later: items in input order; x, y, v gathered by the permutation
     // in finish_sources
     const bool bucketed = values_ready == nullptr;
     if (bucketed)
-        k_key_hist<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, npasses, hist);
+        TC_CUDA_TRY(launch_pdl(k_key_hist, grid_for(n, 256, 8), 256, 0, c.stream, x, y, n,
+                               (const Frame *)frame, npasses, hist));
     else
-        k_keys_pack<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(x, y, n, frame, items_a, npasses,
-                                                               hist);
+        TC_CUDA_TRY(launch_pdl(k_keys_pack, grid_for(n, 256, 8), 256, 0, c.stream, x, y, n,
+                               (const Frame *)frame, items_a, npasses, hist));
     TC_KERNEL_CHECK();
-    k_hist_scan<<<NHIST, RS_RADIX, 0, c.stream>>>(hist, offsets);
+    TC_CUDA_TRY(launch_pdl(k_hist_scan, NHIST, RS_RADIX, 0, c.stream, (const int *)hist, offsets));
     TC_KERNEL_CHECK();
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     const FirstPass fp = {x, y, v, frame, rec, offsets + RS_MAX_PASSES * RS_RADIX, bucket_fill};
@@ -959,10 +969,12 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
                                        : (stall >= 0 ? k_onesweep_items<false, true>
                                                      : k_onesweep_items<false, false>))
                            : k_onesweep_items<false, false>;
-        pass<<<ntiles, PS_THREADS, 0, c.stream>>>(
-            odd ? items_b : items_a, odd ? items_a : items_b, n, 32 + 8 * p,
-            offsets + p * RS_RADIX, status + (size_t)p * ntiles * RS_RADIX, counter + p, err,
-            c.spin_limit, stall, sink, fp);
+        TC_CUDA_TRY(launch_pdl(pass, ntiles, PS_THREADS, 0, c.stream,
+                               (const unsigned long long *)(odd ? items_b : items_a),
+                               odd ? items_a : items_b, n, 32 + 8 * p,
+                               (const int *)(offsets + p * RS_RADIX),
+                               status + (size_t)p * ntiles * RS_RADIX, counter + p, err,
+                               c.spin_limit, stall, sink, fp));
         TC_KERNEL_CHECK();
     }
     c.nsrc = n;
@@ -970,7 +982,8 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     if (c.test_stall == TC_STALL_SORT && (rc = check_device_errors(c, "source sort"))) return rc;
     if (values_ready) {
         // the keys now (the tree needs nothing else); x, y, v in finish_sources
-        k_items_split<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(items_a, n, keys, perm);
+        TC_CUDA_TRY(launch_pdl(k_items_split, grid_for(n, 256, 8), 256, 0, c.stream,
+                               (const unsigned long long *)items_a, n, keys, perm));
         TC_KERNEL_CHECK();
         c.late_x = x;
         c.late_y = y;
@@ -980,8 +993,9 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     }
     // a window of the sorted order in flight at a time (4 CTAs per SM): its records come from
     // a compact range of buckets, which stays in L2
-    k_gather_sources<<<grid_for(n, GS_THREADS * GS_ITEMS, 4), GS_THREADS, 0,
-                                    c.stream>>>(items_a, rec, n, keys, perm, xs, ys, vs, err);
+    TC_CUDA_TRY(launch_pdl(k_gather_sources, grid_for(n, GS_THREADS * GS_ITEMS, 4), GS_THREADS, 0,
+                           c.stream, (const unsigned long long *)items_a, (const double2 *)rec, n,
+                           keys, perm, xs, ys, vs, err));
     TC_KERNEL_CHECK();
     return TC_OK;
 }

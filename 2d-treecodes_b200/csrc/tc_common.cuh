@@ -53,6 +53,15 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+// Programmatic dependent launch (launch_pdl): a kernel may be scheduled while the kernel before
+// it on its stream is still draining.  A kernel so launched calls this first: it waits until
+// that kernel has completed and its writes are visible (so stream order holds exactly), then
+// lets the kernel after it be scheduled in turn.  Both are no-ops without the launch attribute.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Approximate FP64 reciprocal from the SFU (PTX rcp.approx.ftz.f64), refined by two
 // Newton-Raphson steps y <- y + y (1 - d y); each step doubles the number of correct bits.
 __device__ __forceinline__ double rcp_nr(double d) {

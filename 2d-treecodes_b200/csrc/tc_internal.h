@@ -208,6 +208,25 @@ T *slot_ptr(Context &c, Slot s) { return static_cast<T *>(c.buf[s].p); }
 // Streaming multiprocessors of the current device (queried once; thread-safe).
 int device_sm_count();
 
+// Launches `kernel` on `s` with programmatic stream serialization: its blocks may be scheduled
+// while the previous kernel of `s` drains, and wait in pdl_begin() (the kernel's first
+// statement) until that kernel has completed.  Follow with TC_KERNEL_CHECK().
+template <class... P, class... A>
+cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       A &&...args) {
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 // Resident blocks per SM of a kernel at a block size and dynamic shared memory size, computed
 // once per kernel instance (thread-safe initialisation of a function-local static).
 template <auto Kernel>

@@ -73,6 +73,7 @@ __global__ __launch_bounds__(TL_THREADS) void k_tree_list(const int *__restrict_
                                                           unsigned short *__restrict__ lmask,
                                                           int *nlist_out, unsigned *err,
                                                           int spin_limit, int stall_tile) {
+    pdl_begin();
     __shared__ int s_tile, s_excl;
     // the tile's keys with one before and leafcap after, staged by coalesced loads; word q is
     // kept at q + q / 32 so that the 16-source runs of a warp's threads hit distinct banks
@@ -180,6 +181,7 @@ constexpr int RANK_THREADS = 1024;
 __global__ __launch_bounds__(RANK_THREADS) void k_rank_count(const unsigned short *__restrict__ lmask,
                                                              const int *__restrict__ d_nlist,
                                                              int *__restrict__ blk, int nblk) {
+    pdl_begin();
     __shared__ int s_cnt[LMAX];
     if (threadIdx.x < LMAX) s_cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -197,6 +199,7 @@ __global__ __launch_bounds__(RANK_THREADS) void k_rank_count(const unsigned shor
 // One CTA per level: exclusive scan over the blocks' counts; level total -> totals[l].
 __global__ __launch_bounds__(1024) void k_rank_scan(int *__restrict__ blk, int nblk,
                                                     int *__restrict__ totals) {
+    pdl_begin();
     __shared__ int s_part[1024];
     const int l = blockIdx.x;
     int *row = blk + (size_t)l * nblk;
@@ -234,6 +237,7 @@ __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned shor
                                                              const int *__restrict__ blk, int nblk,
                                                              int *__restrict__ rank,
                                                              int *__restrict__ inv, int stride) {
+    pdl_begin();
     __shared__ int s_w[LMAX][RANK_THREADS / 32];
     const int nlist = *d_nlist;
     const int j = blockIdx.x * RANK_THREADS + threadIdx.x;
@@ -268,6 +272,7 @@ __global__ __launch_bounds__(RANK_THREADS) void k_rank_apply(const unsigned shor
 
 
 __global__ void k_tree_root(int n, int leafcap, TNode *tnode, int2 *range, int4 *cell) {
+    pdl_begin();
     range[0] = make_int2(0, n);
     cell[0] = make_int4(0, 0, 0, -1);
     tnode[0].count = n;
@@ -286,6 +291,7 @@ __global__ void k_tree_children(const int *__restrict__ keys, int n, int leafcap
                                 int stride, int ninner, LevelOffsets lo, int nnodes,
                                 TNode *__restrict__ tnode, int2 *__restrict__ range,
                                 int4 *__restrict__ cell, unsigned *err) {
+    pdl_begin();
     const int q = threadIdx.x & 3;
     const unsigned gmask = 0xFu << (lane_id() & ~3);   // the cell's four lanes
     for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < ninner;
@@ -385,11 +391,15 @@ int build_topology(Context &c, int leafcap) {
     TC_KERNEL_CHECK();
     // a test stall leaves the list offsets wrong: report it before anything reads them
     if (c.test_stall == TC_STALL_TREE && (rc = check_device_errors(c, "tree build"))) return rc;
-    k_rank_count<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk);
+    // the rank kernels follow k_tree_list directly (launch_pdl)
+    TC_CUDA_TRY(launch_pdl(k_rank_count, nblk, RANK_THREADS, 0, c.stream,
+                           (const unsigned short *)lmask, (const int *)d_nlist, blkc, nblk));
     TC_KERNEL_CHECK();
-    k_rank_scan<<<LMAX, 1024, 0, c.stream>>>(blkc, nblk, totals);
+    TC_CUDA_TRY(launch_pdl(k_rank_scan, LMAX, 1024, 0, c.stream, blkc, nblk, totals));
     TC_KERNEL_CHECK();
-    k_rank_apply<<<nblk, RANK_THREADS, 0, c.stream>>>(lmask, d_nlist, blkc, nblk, rank, rinv, cap);
+    TC_CUDA_TRY(launch_pdl(k_rank_apply, nblk, RANK_THREADS, 0, c.stream,
+                           (const unsigned short *)lmask, (const int *)d_nlist, (const int *)blkc,
+                           nblk, rank, rinv, cap));
     TC_KERNEL_CHECK();
     // the level totals and the list length, in one read-back
     TC_CUDA_TRY(cudaMemcpyAsync(c.h_pinned, totals, sizeof(int) * (LMAX + 1),
@@ -434,9 +444,11 @@ int build_topology(Context &c, int leafcap) {
     k_tree_root<<<1, 1, 0, c.stream>>>(n, leafcap, tnode, range, cell);
     TC_KERNEL_CHECK();
     if (ninner > 0) {
-        k_tree_children<<<grid_for_tree(4 * (int)ninner, 128), 128, 0, c.stream>>>(
-            keys, n, leafcap, lpos, lmask, rank, rinv, cap, (int)ninner, lo, c.nnodes, tnode, range,
-            cell, slot_ptr<unsigned>(c, S_ERR));
+        TC_CUDA_TRY(launch_pdl(k_tree_children, grid_for_tree(4 * (int)ninner, 128), 128, 0,
+                               c.stream, keys, n, leafcap, (const int *)lpos,
+                               (const unsigned short *)lmask, (const int *)rank,
+                               (const int *)rinv, cap, (int)ninner, lo, c.nnodes, tnode, range,
+                               cell, slot_ptr<unsigned>(c, S_ERR)));
         TC_KERNEL_CHECK();
     }
     return TC_OK;

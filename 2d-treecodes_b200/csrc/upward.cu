@@ -64,6 +64,7 @@ __global__ __launch_bounds__(256) void k_leaf_setup(
     const double *__restrict__ vs, const int2 *__restrict__ range, const int4 *__restrict__ cell,
     TNode *tnode, double *mass, double *wgt, double *wxs, double *wys,
     const Frame *__restrict__ frame, unsigned *err) {
+    pdl_begin();
     const int lane = lane_id(), q = lane & 3, qbase = lane & ~3;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int node = (int)(tid >> 2);
@@ -154,6 +155,7 @@ __global__ __launch_bounds__(UP_WARPS * 32, MIXED ? 4 : 3) void k_leaf_p2e(
     int nnodes, int nsrc, int leafcap, const double *__restrict__ xs, const double *__restrict__ ys,
     const double *__restrict__ vs, const int2 *__restrict__ range, const int4 *__restrict__ cell,
     const TNode *__restrict__ tnode, double *exps, const Frame *__restrict__ frame) {
+    pdl_begin();
     using acc_t = typename std::conditional<MIXED, float, double>::type;
     constexpr int U = MIXED ? 4 : (P > 16 ? 6 : 4);   // sources per lane in flight
     extern __shared__ __align__(16) unsigned char leaf_smem[];
@@ -354,6 +356,7 @@ __global__ __launch_bounds__(256) void k_moments_level(int l, LevelOffsets lo, i
                                                        double *mass, double *wgt, double *wxs,
                                                        double *wys, const Frame *__restrict__ frame,
                                                        unsigned *err) {
+    pdl_begin();
     const int ninner = (lo.off[l + 2] - lo.off[l + 1]) / 4;
     const double ext = frame->ext;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < ninner; r += gridDim.x * blockDim.x) {
@@ -369,6 +372,7 @@ __global__ __launch_bounds__(1024) void k_moments_top(int ltop, LevelOffsets lo,
                                                       double *mass, double *wgt, double *wxs,
                                                       double *wys, const Frame *__restrict__ frame,
                                                       unsigned *err) {
+    pdl_begin();
     const double ext = frame->ext;
     for (int l = ltop; l >= 0; --l) {
         const int ninner = (lo.off[l + 2] - lo.off[l + 1]) / 4;
@@ -506,6 +510,7 @@ template <int P>
 __global__ __launch_bounds__(UP_WARPS * 32, 5) void k_upward_level(
     int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
     const double *mass, const double *wgt, double *exps, unsigned *err) {
+    pdl_begin();
     __shared__ MergeShared<P> shared[UP_WARPS];
     __shared__ BinomRows<P> bt;
     fill_binom_rows<P>(bt);
@@ -543,6 +548,7 @@ template <int P>
 __global__ __launch_bounds__(32, UP_WIDE_MIN_BLOCKS) void k_upward_wide(
     int l, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
     const double *mass, const double *wgt, double *exps, unsigned *err) {
+    pdl_begin();
     __shared__ WideShared<P> st;
     const int lane = lane_id(), j = lane >> 2, c = lane & 3;
     const int cbase = lo.off[l + 1];
@@ -631,6 +637,7 @@ template <int P>
 __global__ __launch_bounds__(UP_TOP_WARPS * 32) void k_upward_top(
     int ltop, LevelOffsets lo, int nnodes, const int4 *__restrict__ cell, const TNode *tnode,
     const double *mass, const double *wgt, double *exps, unsigned *err) {
+    pdl_begin();
     __shared__ MergeShared<P> shared[UP_TOP_WARPS];
     __shared__ BinomRows<P> bt;
     fill_binom_rows<P>(bt);
@@ -691,16 +698,28 @@ int upward_moments(Context &c) {
     // inner nodes exist on levels 0 .. LMAX-1, deepest first
     const LevelOffsets offs = level_offsets(c);
     const int ltop = small_top(c, MOM_TOP_MAX);
+    // the first launch follows the event wait; each later one follows a kernel (launch_pdl)
+    bool after_kernel = false;
     for (int l = LMAX - 1; l > ltop; --l) {
         const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
         if (ninner <= 0) continue;
-        k_moments_level<<<(ninner + 255) / 256, 256, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
-                                                                    wx, wy, frame, err);
+        if (after_kernel)
+            TC_CUDA_TRY(launch_pdl(k_moments_level, (ninner + 255) / 256, 256, 0, c.stream, l,
+                                   offs, nn, cell, tnode, mass, w, wx, wy, frame, err));
+        else
+            k_moments_level<<<(ninner + 255) / 256, 256, 0, c.stream>>>(l, offs, nn, cell, tnode,
+                                                                        mass, w, wx, wy, frame,
+                                                                        err);
         TC_KERNEL_CHECK();
+        after_kernel = true;
     }
     if (ltop >= 0) {
-        k_moments_top<<<1, MOM_TOP_MAX, 0, c.stream>>>(ltop, offs, nn, cell, tnode, mass, w, wx, wy,
-                                                       frame, err);
+        if (after_kernel)
+            TC_CUDA_TRY(launch_pdl(k_moments_top, 1, MOM_TOP_MAX, 0, c.stream, ltop, offs, nn, cell,
+                                   tnode, mass, w, wx, wy, frame, err));
+        else
+            k_moments_top<<<1, MOM_TOP_MAX, 0, c.stream>>>(ltop, offs, nn, cell, tnode, mass, w,
+                                                           wx, wy, frame, err);
         TC_KERNEL_CHECK();
     }
     TC_CUDA_TRY(cudaEventRecord(c.ev_moments, c.stream));
@@ -743,23 +762,39 @@ static int run_expansions(Context &c) {
     // small top levels in one single-block launch
     const LevelOffsets offs = level_offsets(c);
     const int ltop = small_top(c, UP_TOP_MAX_NODES);
+    // the first launch follows the event wait; each later one follows a kernel (launch_pdl)
+    bool after_kernel = false;
     for (int l = LMAX - 1; l > ltop; --l) {
         const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
         if (ninner <= 0) continue;
         if (ninner >= UP_WIDE_MIN_NODES) {
             const int g = (int)std::min<long long>((ninner + 7) / 8,
                                                    (long long)sms * UP_WIDE_MIN_BLOCKS);
-            k_upward_wide<P><<<g, 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w, exps, err);
+            if (after_kernel)
+                TC_CUDA_TRY(launch_pdl(k_upward_wide<P>, g, 32, 0, c.stream, l, offs, nn, cell,
+                                       (const TNode *)tnode, mass, w, exps, err));
+            else
+                k_upward_wide<P><<<g, 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w, exps,
+                                                         err);
         } else {
             const int g = (int)std::min<long long>((ninner + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
-            k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w,
-                                                                 exps, err);
+            if (after_kernel)
+                TC_CUDA_TRY(launch_pdl(k_upward_level<P>, g, UP_WARPS * 32, 0, c.stream, l, offs,
+                                       nn, cell, (const TNode *)tnode, mass, w, exps, err));
+            else
+                k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass,
+                                                                     w, exps, err);
         }
         TC_KERNEL_CHECK();
+        after_kernel = true;
     }
     if (ltop >= 0) {
-        k_upward_top<P><<<1, UP_TOP_WARPS * 32, 0, c.stream>>>(ltop, offs, nn, cell, tnode, mass, w,
-                                                               exps, err);
+        if (after_kernel)
+            TC_CUDA_TRY(launch_pdl(k_upward_top<P>, 1, UP_TOP_WARPS * 32, 0, c.stream, ltop, offs,
+                                   nn, cell, (const TNode *)tnode, mass, w, exps, err));
+        else
+            k_upward_top<P><<<1, UP_TOP_WARPS * 32, 0, c.stream>>>(ltop, offs, nn, cell, tnode,
+                                                                   mass, w, exps, err);
         TC_KERNEL_CHECK();
     }
     return TC_OK;
