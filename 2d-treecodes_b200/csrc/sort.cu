@@ -143,6 +143,7 @@ __device__ __forceinline__ int quantize(double v, double vmin, double scale) {
 // the sources' square).  Used only to group nearby targets; it does not affect results.
 __global__ void k_target_keys(const double *__restrict__ x, const double *__restrict__ y, int n,
                               const Frame *__restrict__ frame, int *__restrict__ keys) {
+    pdl_begin();
     const Frame f = *frame;
     const double hi = (double)((1 << LMAX) - 1);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -171,6 +172,7 @@ constexpr int RS_MAX_PASSES = 4;
 // Histograms of every 8-bit digit of the keys, in one read.
 __global__ __launch_bounds__(256) void k_hist(const int *__restrict__ keys, int n, int npasses,
                                               int *__restrict__ hist) {
+    pdl_begin();
     __shared__ int s[RS_MAX_PASSES][RS_RADIX];
     for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_RADIX; i += blockDim.x) (&s[0][0])[i] = 0;
     __syncthreads();
@@ -255,6 +257,7 @@ __global__ __launch_bounds__(RS_THREADS) void k_onesweep(
     const int *__restrict__ keys_in, const int *__restrict__ vals_in, int *__restrict__ keys_out,
     int *__restrict__ vals_out, int n, int shift, const int *__restrict__ digit_offsets,
     unsigned *status, int *tile_counter, unsigned *err) {
+    pdl_begin();
     __shared__ int s_keys[RS_TILE];
     __shared__ int s_vals[RS_TILE];
     __shared__ int s_whist[RS_WARPS][RS_RADIX];
@@ -710,6 +713,7 @@ __global__ __launch_bounds__(256) void k_gather_xy(const int *__restrict__ perm,
                                                    const double *__restrict__ y, int n,
                                                    double *__restrict__ xs,
                                                    double *__restrict__ ys, unsigned *err) {
+    pdl_begin();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const unsigned j = (unsigned)perm[i];
         if (j >= (unsigned)n) {
@@ -725,6 +729,7 @@ __global__ __launch_bounds__(256) void k_gather_xy(const int *__restrict__ perm,
 __global__ __launch_bounds__(256) void k_gather_v(const int *__restrict__ perm,
                                                   const double *__restrict__ v, int n,
                                                   double *__restrict__ vs) {
+    pdl_begin();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const unsigned j = (unsigned)perm[i];
         if (j < (unsigned)n) vs[i] = __ldg(v + j);
@@ -798,17 +803,17 @@ int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, 
                                 c.stream));
     k_hist<<<grid_for(n, 256, 4), 256, 0, c.stream>>>(keys_in, n, npasses, hist);
     TC_KERNEL_CHECK();
-    k_hist_scan<<<npasses, RS_RADIX, 0, c.stream>>>(hist, offsets);
+    // the kernels after k_hist follow each other directly (launch_pdl)
+    TC_CUDA_TRY(launch_pdl(k_hist_scan, npasses, RS_RADIX, 0, c.stream, (const int *)hist, offsets));
     TC_KERNEL_CHECK();
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
 
     const int *ki = keys_in, *vi = vals_in;
     int *ko = keys_a, *vo = vals_a;
     for (int p = 0; p < npasses; ++p) {
-        k_onesweep<<<ntiles, RS_THREADS, 0, c.stream>>>(ki, vi, ko, vo, n, 8 * p,
-                                                         offsets + p * RS_RADIX,
-                                                         status + (size_t)p * ntiles * RS_RADIX,
-                                                         counter + p, err);
+        TC_CUDA_TRY(launch_pdl(k_onesweep, ntiles, RS_THREADS, 0, c.stream, ki, vi, ko, vo, n,
+                               8 * p, (const int *)(offsets + p * RS_RADIX),
+                               status + (size_t)p * ntiles * RS_RADIX, counter + p, err));
         TC_KERNEL_CHECK();
         ki = ko;
         vi = vo;
@@ -827,6 +832,7 @@ constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
 __global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(const int *__restrict__ in, int n,
                                                              int *__restrict__ block_sums) {
+    pdl_begin();
     const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
     int s = 0;
 #pragma unroll
@@ -839,6 +845,7 @@ __global__ __launch_bounds__(SCAN_THREADS) void k_scan_reduce(const int *__restr
 
 __global__ __launch_bounds__(SCAN_THREADS) void k_scan_blocks(int *block_sums, int nb,
                                                              int *out_total) {
+    pdl_begin();
     // one CTA: each thread scans a contiguous chunk of the block sums
     const int per = (nb + SCAN_THREADS - 1) / SCAN_THREADS;
     const int b0 = threadIdx.x * per;
@@ -859,6 +866,7 @@ __global__ __launch_bounds__(SCAN_THREADS) void k_scan_blocks(int *block_sums, i
 __global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(const int *__restrict__ in, int n,
                                                             const int *__restrict__ block_offs,
                                                             int *__restrict__ out) {
+    pdl_begin();
     const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
     int v[SCAN_ITEMS];
     int s = 0;
@@ -887,9 +895,10 @@ int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
     }
     k_scan_reduce<<<nb, SCAN_THREADS, 0, c.stream>>>(d_in, n, bs);
     TC_KERNEL_CHECK();
-    k_scan_blocks<<<1, SCAN_THREADS, 0, c.stream>>>(bs, nb, d_out + n);
+    TC_CUDA_TRY(launch_pdl(k_scan_blocks, 1, SCAN_THREADS, 0, c.stream, bs, nb, d_out + n));
     TC_KERNEL_CHECK();
-    k_scan_apply<<<nb, SCAN_THREADS, 0, c.stream>>>(d_in, n, bs, d_out);
+    TC_CUDA_TRY(launch_pdl(k_scan_apply, nb, SCAN_THREADS, 0, c.stream, d_in, n,
+                           (const int *)bs, d_out));
     TC_KERNEL_CHECK();
     return TC_OK;
 }
