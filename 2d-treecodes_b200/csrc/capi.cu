@@ -672,6 +672,16 @@ TC_API int tc_set_host_waits(tc_context *ctx, int sleeping) {
     return TC_OK;
 }
 
+TC_API int tc_set_launch_overlap(tc_context *ctx, int on) {
+    clear_error();
+    if (!ctx || on < 0 || on > 1) {
+        set_error(TC_ERR_INVALID, "invalid launch overlap setting %d", on);
+        return TC_ERR_INVALID;
+    }
+    ctx->c.launch_overlap = on != 0;
+    return TC_OK;
+}
+
 TC_API int tc_set_wait_test(tc_context *ctx, int stall, int spin_limit, int stack_limit) {
     clear_error();
     if (!ctx || stall < TC_STALL_NONE || stall > TC_STALL_TREE) {

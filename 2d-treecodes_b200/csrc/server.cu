@@ -154,6 +154,10 @@ int run_request(tc_context *ctx, const tc_request &r) {
     // slot threads sleep while their solve runs instead of spinning on a host core
     int rc = tc_set_host_waits(ctx, 1);
     if (rc) return rc;
+    // plain launches: programmatic dependent launch in four contexts solving at once gave
+    // occasional stalls of tens of milliseconds
+    rc = tc_set_launch_overlap(ctx, 0);
+    if (rc) return rc;
     rc = tc_set_precision(ctx, r.precision);
     if (rc) return rc;
     if (r.kind == TC_REQUEST_POTENTIAL)

@@ -784,6 +784,7 @@ static int grid_for(int n, int threads, int per_sm = 8) {
 int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, int nbits,
                      int *keys_a, int *vals_a, int *keys_b, int *vals_b, int **keys_out,
                      int **vals_out) {
+    const bool ovl = c.launch_overlap;   // launch_pdl chains (tc_set_launch_overlap)
     if (n >= (1 << 30)) {
         set_error(TC_ERR_INVALID, "radix sort supports fewer than 2^30 keys (got %d)", n);
         return TC_ERR_INVALID;
@@ -804,14 +805,15 @@ int radix_sort_pairs(Context &c, const int *keys_in, const int *vals_in, int n, 
     k_hist<<<grid_for(n, 256, 4), 256, 0, c.stream>>>(keys_in, n, npasses, hist);
     TC_KERNEL_CHECK();
     // the kernels after k_hist follow each other directly (launch_pdl)
-    TC_CUDA_TRY(launch_pdl(k_hist_scan, npasses, RS_RADIX, 0, c.stream, (const int *)hist, offsets));
+    TC_CUDA_TRY(launch_pdl(ovl, k_hist_scan, npasses, RS_RADIX, 0, c.stream, (const int *)hist,
+                           offsets));
     TC_KERNEL_CHECK();
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
 
     const int *ki = keys_in, *vi = vals_in;
     int *ko = keys_a, *vo = vals_a;
     for (int p = 0; p < npasses; ++p) {
-        TC_CUDA_TRY(launch_pdl(k_onesweep, ntiles, RS_THREADS, 0, c.stream, ki, vi, ko, vo, n,
+        TC_CUDA_TRY(launch_pdl(ovl, k_onesweep, ntiles, RS_THREADS, 0, c.stream, ki, vi, ko, vo, n,
                                8 * p, (const int *)(offsets + p * RS_RADIX),
                                status + (size_t)p * ntiles * RS_RADIX, counter + p, err));
         TC_KERNEL_CHECK();
@@ -885,6 +887,7 @@ __global__ __launch_bounds__(SCAN_THREADS) void k_scan_apply(const int *__restri
 }
 
 int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
+    const bool ovl = c.launch_overlap;   // launch_pdl chains (tc_set_launch_overlap)
     const int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     int *bs;
     int rc;
@@ -895,9 +898,9 @@ int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
     }
     k_scan_reduce<<<nb, SCAN_THREADS, 0, c.stream>>>(d_in, n, bs);
     TC_KERNEL_CHECK();
-    TC_CUDA_TRY(launch_pdl(k_scan_blocks, 1, SCAN_THREADS, 0, c.stream, bs, nb, d_out + n));
+    TC_CUDA_TRY(launch_pdl(ovl, k_scan_blocks, 1, SCAN_THREADS, 0, c.stream, bs, nb, d_out + n));
     TC_KERNEL_CHECK();
-    TC_CUDA_TRY(launch_pdl(k_scan_apply, nb, SCAN_THREADS, 0, c.stream, d_in, n,
+    TC_CUDA_TRY(launch_pdl(ovl, k_scan_apply, nb, SCAN_THREADS, 0, c.stream, d_in, n,
                            (const int *)bs, d_out));
     TC_KERNEL_CHECK();
     return TC_OK;
@@ -906,6 +909,7 @@ int exclusive_scan(Context &c, const int *d_in, int *d_out, int n) {
 // ---------------------------------------------------------------------------- drivers
 int sort_sources(Context &c, const double *x, const double *y, const double *v, int n,
                  cudaEvent_t values_ready) {
+    const bool ovl = c.launch_overlap;   // launch_pdl chains (tc_set_launch_overlap)
     int rc;
     c.late_ready = nullptr;   // a late-value sort of an earlier call that failed midway
     double *xs, *ys, *vs;
@@ -959,13 +963,14 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     // in finish_sources
     const bool bucketed = values_ready == nullptr;
     if (bucketed)
-        TC_CUDA_TRY(launch_pdl(k_key_hist, grid_for(n, 256, 8), 256, 0, c.stream, x, y, n,
+        TC_CUDA_TRY(launch_pdl(ovl, k_key_hist, grid_for(n, 256, 8), 256, 0, c.stream, x, y, n,
                                (const Frame *)frame, npasses, hist));
     else
-        TC_CUDA_TRY(launch_pdl(k_keys_pack, grid_for(n, 256, 8), 256, 0, c.stream, x, y, n,
+        TC_CUDA_TRY(launch_pdl(ovl, k_keys_pack, grid_for(n, 256, 8), 256, 0, c.stream, x, y, n,
                                (const Frame *)frame, items_a, npasses, hist));
     TC_KERNEL_CHECK();
-    TC_CUDA_TRY(launch_pdl(k_hist_scan, NHIST, RS_RADIX, 0, c.stream, (const int *)hist, offsets));
+    TC_CUDA_TRY(launch_pdl(ovl, k_hist_scan, NHIST, RS_RADIX, 0, c.stream, (const int *)hist,
+                           offsets));
     TC_KERNEL_CHECK();
     unsigned *err = slot_ptr<unsigned>(c, S_ERR);
     const FirstPass fp = {x, y, v, frame, rec, offsets + RS_MAX_PASSES * RS_RADIX, bucket_fill};
@@ -978,7 +983,7 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
                                        : (stall >= 0 ? k_onesweep_items<false, true>
                                                      : k_onesweep_items<false, false>))
                            : k_onesweep_items<false, false>;
-        TC_CUDA_TRY(launch_pdl(pass, ntiles, PS_THREADS, 0, c.stream,
+        TC_CUDA_TRY(launch_pdl(ovl, pass, ntiles, PS_THREADS, 0, c.stream,
                                (const unsigned long long *)(odd ? items_b : items_a),
                                odd ? items_a : items_b, n, 32 + 8 * p,
                                (const int *)(offsets + p * RS_RADIX),
@@ -991,7 +996,7 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     if (c.test_stall == TC_STALL_SORT && (rc = check_device_errors(c, "source sort"))) return rc;
     if (values_ready) {
         // the keys now (the tree needs nothing else); x, y, v in finish_sources
-        TC_CUDA_TRY(launch_pdl(k_items_split, grid_for(n, 256, 8), 256, 0, c.stream,
+        TC_CUDA_TRY(launch_pdl(ovl, k_items_split, grid_for(n, 256, 8), 256, 0, c.stream,
                                (const unsigned long long *)items_a, n, keys, perm));
         TC_KERNEL_CHECK();
         c.late_x = x;
@@ -1002,9 +1007,9 @@ int sort_sources(Context &c, const double *x, const double *y, const double *v, 
     }
     // a window of the sorted order in flight at a time (4 CTAs per SM): its records come from
     // a compact range of buckets, which stays in L2
-    TC_CUDA_TRY(launch_pdl(k_gather_sources, grid_for(n, GS_THREADS * GS_ITEMS, 4), GS_THREADS, 0,
-                           c.stream, (const unsigned long long *)items_a, (const double2 *)rec, n,
-                           keys, perm, xs, ys, vs, err));
+    TC_CUDA_TRY(launch_pdl(ovl, k_gather_sources, grid_for(n, GS_THREADS * GS_ITEMS, 4),
+                           GS_THREADS, 0, c.stream, (const unsigned long long *)items_a,
+                           (const double2 *)rec, n, keys, perm, xs, ys, vs, err));
     TC_KERNEL_CHECK();
     return TC_OK;
 }

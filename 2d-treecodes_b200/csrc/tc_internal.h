@@ -120,6 +120,9 @@ struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // kernel chains launched with programmatic dependent launch (launch_pdl); the request
+    // server turns it off for its contexts (tc_set_launch_overlap)
+    bool launch_overlap = true;
     // auxiliary stream: interaction lists are built on it while the expansions are formed on
     // `stream`; ordered against `stream` with the events below
     cudaStream_t aux = nullptr;
@@ -208,12 +211,17 @@ T *slot_ptr(Context &c, Slot s) { return static_cast<T *>(c.buf[s].p); }
 // Streaming multiprocessors of the current device (queried once; thread-safe).
 int device_sm_count();
 
-// Launches `kernel` on `s` with programmatic stream serialization: its blocks may be scheduled
-// while the previous kernel of `s` drains, and wait in pdl_begin() (the kernel's first
-// statement) until that kernel has completed.  Follow with TC_KERNEL_CHECK().
+// Launches `kernel` on `s` with programmatic stream serialization when `overlap` is set (the
+// context's launch_overlap): its blocks may be scheduled while the previous kernel of `s`
+// drains, and wait in pdl_begin() (the kernel's first statement) until that kernel has
+// completed.  Otherwise an ordinary launch.  Follow with TC_KERNEL_CHECK().
 template <class... P, class... A>
-cudaError_t launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                       A &&...args) {
+cudaError_t launch_pdl(bool overlap, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, A &&...args) {
+    if (!overlap) {
+        kernel<<<grid, block, smem, s>>>(std::forward<A>(args)...);
+        return cudaSuccess;   // (TC_KERNEL_CHECK reads the launch error)
+    }
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr.val.programmaticStreamSerializationAllowed = 1;

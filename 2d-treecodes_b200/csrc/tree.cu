@@ -359,6 +359,7 @@ static int grid_for_tree(int n, int threads) {
 }
 
 int build_topology(Context &c, int leafcap) {
+    const bool ovl = c.launch_overlap;   // launch_pdl chains (tc_set_launch_overlap)
     const int n = c.nsrc;
     int rc;
     const int *keys = slot_ptr<int>(c, S_KEYS);
@@ -392,12 +393,12 @@ int build_topology(Context &c, int leafcap) {
     // a test stall leaves the list offsets wrong: report it before anything reads them
     if (c.test_stall == TC_STALL_TREE && (rc = check_device_errors(c, "tree build"))) return rc;
     // the rank kernels follow k_tree_list directly (launch_pdl)
-    TC_CUDA_TRY(launch_pdl(k_rank_count, nblk, RANK_THREADS, 0, c.stream,
+    TC_CUDA_TRY(launch_pdl(ovl, k_rank_count, nblk, RANK_THREADS, 0, c.stream,
                            (const unsigned short *)lmask, (const int *)d_nlist, blkc, nblk));
     TC_KERNEL_CHECK();
-    TC_CUDA_TRY(launch_pdl(k_rank_scan, LMAX, 1024, 0, c.stream, blkc, nblk, totals));
+    TC_CUDA_TRY(launch_pdl(ovl, k_rank_scan, LMAX, 1024, 0, c.stream, blkc, nblk, totals));
     TC_KERNEL_CHECK();
-    TC_CUDA_TRY(launch_pdl(k_rank_apply, nblk, RANK_THREADS, 0, c.stream,
+    TC_CUDA_TRY(launch_pdl(ovl, k_rank_apply, nblk, RANK_THREADS, 0, c.stream,
                            (const unsigned short *)lmask, (const int *)d_nlist, (const int *)blkc,
                            nblk, rank, rinv, cap));
     TC_KERNEL_CHECK();
@@ -444,7 +445,7 @@ int build_topology(Context &c, int leafcap) {
     k_tree_root<<<1, 1, 0, c.stream>>>(n, leafcap, tnode, range, cell);
     TC_KERNEL_CHECK();
     if (ninner > 0) {
-        TC_CUDA_TRY(launch_pdl(k_tree_children, grid_for_tree(4 * (int)ninner, 128), 128, 0,
+        TC_CUDA_TRY(launch_pdl(ovl, k_tree_children, grid_for_tree(4 * (int)ninner, 128), 128, 0,
                                c.stream, keys, n, leafcap, (const int *)lpos,
                                (const unsigned short *)lmask, (const int *)rank,
                                (const int *)rinv, cap, (int)ninner, lo, c.nnodes, tnode, range,

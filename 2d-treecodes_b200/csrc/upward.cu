@@ -677,6 +677,7 @@ static LevelOffsets level_offsets(const Context &c) {
 constexpr int MOM_TOP_MAX = 1024;   // levels with at most this many inner nodes: one block
 
 int upward_moments(Context &c) {
+    const bool ovl = c.launch_overlap;   // launch_pdl chains (tc_set_launch_overlap)
     const int nn = c.nnodes;
     const int2 *range = slot_ptr<int2>(c, S_RANGE);
     const int4 *cell = slot_ptr<int4>(c, S_CELL);
@@ -704,7 +705,7 @@ int upward_moments(Context &c) {
         const int ninner = (c.level_off[l + 2] - c.level_off[l + 1]) / 4;
         if (ninner <= 0) continue;
         if (after_kernel)
-            TC_CUDA_TRY(launch_pdl(k_moments_level, (ninner + 255) / 256, 256, 0, c.stream, l,
+            TC_CUDA_TRY(launch_pdl(ovl, k_moments_level, (ninner + 255) / 256, 256, 0, c.stream, l,
                                    offs, nn, cell, tnode, mass, w, wx, wy, frame, err));
         else
             k_moments_level<<<(ninner + 255) / 256, 256, 0, c.stream>>>(l, offs, nn, cell, tnode,
@@ -715,8 +716,8 @@ int upward_moments(Context &c) {
     }
     if (ltop >= 0) {
         if (after_kernel)
-            TC_CUDA_TRY(launch_pdl(k_moments_top, 1, MOM_TOP_MAX, 0, c.stream, ltop, offs, nn, cell,
-                                   tnode, mass, w, wx, wy, frame, err));
+            TC_CUDA_TRY(launch_pdl(ovl, k_moments_top, 1, MOM_TOP_MAX, 0, c.stream, ltop, offs, nn,
+                                   cell, tnode, mass, w, wx, wy, frame, err));
         else
             k_moments_top<<<1, MOM_TOP_MAX, 0, c.stream>>>(ltop, offs, nn, cell, tnode, mass, w,
                                                            wx, wy, frame, err);
@@ -728,6 +729,7 @@ int upward_moments(Context &c) {
 
 template <int P>
 static int run_expansions(Context &c) {
+    const bool ovl = c.launch_overlap;   // launch_pdl chains (tc_set_launch_overlap)
     const int nn = c.nnodes;
     const double *xs = slot_ptr<double>(c, S_XS), *ys = slot_ptr<double>(c, S_YS),
                  *vs = slot_ptr<double>(c, S_VS);
@@ -771,7 +773,7 @@ static int run_expansions(Context &c) {
             const int g = (int)std::min<long long>((ninner + 7) / 8,
                                                    (long long)sms * UP_WIDE_MIN_BLOCKS);
             if (after_kernel)
-                TC_CUDA_TRY(launch_pdl(k_upward_wide<P>, g, 32, 0, c.stream, l, offs, nn, cell,
+                TC_CUDA_TRY(launch_pdl(ovl, k_upward_wide<P>, g, 32, 0, c.stream, l, offs, nn, cell,
                                        (const TNode *)tnode, mass, w, exps, err));
             else
                 k_upward_wide<P><<<g, 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass, w, exps,
@@ -779,8 +781,8 @@ static int run_expansions(Context &c) {
         } else {
             const int g = (int)std::min<long long>((ninner + UP_WARPS - 1) / UP_WARPS, (long long)sms * 8);
             if (after_kernel)
-                TC_CUDA_TRY(launch_pdl(k_upward_level<P>, g, UP_WARPS * 32, 0, c.stream, l, offs,
-                                       nn, cell, (const TNode *)tnode, mass, w, exps, err));
+                TC_CUDA_TRY(launch_pdl(ovl, k_upward_level<P>, g, UP_WARPS * 32, 0, c.stream, l,
+                                       offs, nn, cell, (const TNode *)tnode, mass, w, exps, err));
             else
                 k_upward_level<P><<<g, UP_WARPS * 32, 0, c.stream>>>(l, offs, nn, cell, tnode, mass,
                                                                      w, exps, err);
@@ -790,8 +792,8 @@ static int run_expansions(Context &c) {
     }
     if (ltop >= 0) {
         if (after_kernel)
-            TC_CUDA_TRY(launch_pdl(k_upward_top<P>, 1, UP_TOP_WARPS * 32, 0, c.stream, ltop, offs,
-                                   nn, cell, (const TNode *)tnode, mass, w, exps, err));
+            TC_CUDA_TRY(launch_pdl(ovl, k_upward_top<P>, 1, UP_TOP_WARPS * 32, 0, c.stream, ltop,
+                                   offs, nn, cell, (const TNode *)tnode, mass, w, exps, err));
         else
             k_upward_top<P><<<1, UP_TOP_WARPS * 32, 0, c.stream>>>(ltop, offs, nn, cell, tnode,
                                                                    mass, w, exps, err);

@@ -41,6 +41,7 @@ SIGNATURES = {
     "tc_context_destroy": (None, [_vp]),
     "tc_set_precision": (_i, [_vp, _i]),
     "tc_set_host_waits": (_i, [_vp, _i]),
+    "tc_set_launch_overlap": (_i, [_vp, _i]),
     "tc_set_wait_test": (_i, [_vp, _i, _i, _i]),
     "tc_release_cached_memory": (_i, [_i]),
     "tc_reserve_cached_memory": (_i, [_i, ctypes.c_size_t]),
@@ -260,6 +261,11 @@ class Context:
         """0: the solving thread spins while the device works (lowest latency); 1: it polls
         and sleeps, leaving the host core to other threads."""
         _check(self.lib.tc_set_host_waits(self.h, int(sleeping)))
+
+    def set_launch_overlap(self, on=True):
+        """True (the default): the solve's kernel chains use programmatic dependent launch, each
+        kernel scheduled while the one before it drains; False: plain launches."""
+        _check(self.lib.tc_set_launch_overlap(self.h, int(bool(on))))
 
     def set_wait_test(self, stall=0, spin_limit=0, stack_limit=0):
         """Test settings: `stall` 1 (source sort) or 2 (tree build) makes one look-back tile

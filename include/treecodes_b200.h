@@ -108,6 +108,13 @@ TC_API int tc_set_precision(tc_context *ctx, int precision);
  * call, the lowest latency; 1 polls every 20 us and sleeps in between, which leaves the host core
  * to other threads (the request server's slots wait this way). */
 TC_API int tc_set_host_waits(tc_context *ctx, int sleeping);
+/* Programmatic dependent launch of the solve's kernel chains (the source and target sorts, the
+ * tree build, the upward pass): 1 (the default) lets each kernel of a chain be scheduled while
+ * the one before it drains, and it waits on the device until that one has completed; 0 launches
+ * them one after another.  It saves about 2.5 us per launch on a lone solve.  The request
+ * server turns it off on its contexts: with four solving at once it caused occasional stalls of
+ * tens of milliseconds. */
+TC_API int tc_set_launch_overlap(tc_context *ctx, int on);
 /* Test settings that make the library's bounded device waits and capacities run out on
  * purpose, so that their error paths can be exercised without faulting or hanging a GPU (no
  * counterpart in the reference, whose overflows are silent, drivers/upward.cpp:253).

@@ -36,6 +36,7 @@ void tc_context_destroy(tc_context *c) {
     g_live--;
 }
 int tc_set_host_waits(tc_context *, int) { return 0; }
+int tc_set_launch_overlap(tc_context *, int) { return 0; }
 int tc_set_precision(tc_context *c, int p) {
     c->precision = p;
     return 0;
