@@ -89,6 +89,10 @@ struct tc_server {
     std::unordered_map<long long, Client> clients;
     std::list<long long> lru;          // idle clients, least recently used first
     std::vector<tc_context *> pool;    // one pooled context per slot (one-off requests)
+    // evicted client contexts, destroyed by whoever evicted them once the lock is released:
+    // destroying a context synchronises its streams and frees its buffers, which must not hold
+    // up admission and submission (one release under the lock stalled both for 86 ms)
+    std::vector<tc_context *> graveyard;
     std::vector<size_t> pool_bytes;
     std::vector<char> slot_busy;
     std::vector<std::thread> workers;
@@ -104,6 +108,11 @@ struct tc_server {
     Job *pick(int slot, size_t *reserve, tc_context **ctx);
     bool make_room(int slot, size_t need, long long keep_client);
     void evict_client_locked(long long id);
+    std::vector<tc_context *> take_graveyard_locked() {
+        std::vector<tc_context *> dead;
+        dead.swap(graveyard);
+        return dead;
+    }
 };
 
 namespace {
@@ -178,7 +187,7 @@ void tc_server::evict_client_locked(long long id) {
     if (cl.ctx) {
         lru.erase(cl.lru);
         charged -= cl.bytes;
-        tc_context_destroy(cl.ctx);
+        graveyard.push_back(cl.ctx);   // destroyed outside the lock (take_graveyard_locked)
         cl.ctx = nullptr;
         cl.bytes = 0;
     }
@@ -305,7 +314,9 @@ void tc_server::worker(int slot) {
         slot_busy[slot] = 1;
         ++in_service;
         max_in_service = std::max(max_in_service, in_service);
+        std::vector<tc_context *> dead = take_graveyard_locked();   // evicted while admitting
         lock.unlock();
+        for (tc_context *d : dead) tc_context_destroy(d);
 
         const int rc = run_request(ctx, j->req);
         const size_t bytes = tc_context_device_bytes(ctx);
@@ -345,6 +356,12 @@ void tc_server::worker(int slot) {
         if (rc) ++failed;
         cv_done.notify_all();
         cv_work.notify_all();
+        dead = take_graveyard_locked();   // a client released after its last step
+        if (!dead.empty()) {
+            lock.unlock();
+            for (tc_context *d : dead) tc_context_destroy(d);
+            lock.lock();
+        }
     }
 }
 
@@ -395,6 +412,7 @@ TC_API void tc_server_destroy(tc_server *srv) {
     for (auto &t : srv->workers) t.join();
     for (auto *c : srv->pool) tc_context_destroy(c);
     for (auto &kv : srv->clients) tc_context_destroy(kv.second.ctx);
+    for (auto *c : srv->graveyard) tc_context_destroy(c);
     for (auto &kv : srv->jobs) delete kv.second;
     delete srv;
 }
@@ -484,15 +502,20 @@ TC_API int tc_server_wait_any(tc_server *srv, long long *ticket, tc_request_resu
 
 TC_API int tc_server_release_client(tc_server *srv, long long client) {
     if (!srv || client <= 0) return TC_ERR_INVALID;
-    std::lock_guard<std::mutex> lock(srv->mu);
-    auto it = srv->clients.find(client);
-    if (it == srv->clients.end()) return TC_OK;
-    Client &cl = it->second;
-    if (cl.busy || cl.queued > 0)
-        cl.release_pending = true;
-    else
-        srv->evict_client_locked(client);
-    srv->cv_work.notify_all();
+    std::vector<tc_context *> dead;
+    {
+        std::lock_guard<std::mutex> lock(srv->mu);
+        auto it = srv->clients.find(client);
+        if (it == srv->clients.end()) return TC_OK;
+        Client &cl = it->second;
+        if (cl.busy || cl.queued > 0)
+            cl.release_pending = true;
+        else
+            srv->evict_client_locked(client);
+        dead = srv->take_graveyard_locked();
+        srv->cv_work.notify_all();
+    }
+    for (tc_context *d : dead) tc_context_destroy(d);
     return TC_OK;
 }
 
