@@ -309,3 +309,30 @@ def test_timing_modes_give_the_same_results(gpu_ctx):
         finally:
             gpu_ctx.set_timing(0)
             gpu_ctx.set_precision(0)
+
+
+def test_launch_overlap_changes_nothing(gpu_ctx):
+    """Programmatic dependent launch of the sort, tree and upward kernel chains (the default) and
+    plain launches give the same outputs, bit for bit, for both entry points (device and host
+    pointers) and both forms; the sizes cover several radix tiles, tree levels and E2E
+    launches."""
+    wp = W.gaussian_mixture_potential(n=200000)
+    wf = W.lamb_oseen_force(n=300000, blocks_per_side=16, h=1.0 / 512)
+    try:
+        for precision in (0, 1):
+            gpu_ctx.set_precision(precision)
+            outs = []
+            for overlap in (True, False):
+                gpu_ctx.set_launch_overlap(overlap)
+                p = gpu_potential(gpu_ctx, wp, 0.5)
+                xo, yo = gpu_force(gpu_ctx, wf, 0.5)
+                # the host entry points sort with the values arriving late (another chain)
+                hp = gpu_ctx.potential_host(0.5, wp["xs"], wp["ys"], wp["vs"], wp["xt"], wp["yt"])
+                hx, hy = gpu_ctx.force_mrag_host(0.5, wf["xs"], wf["ys"], wf["vs"], wf["x0s"],
+                                                 wf["y0s"], wf["hs"])
+                outs.append((p, xo, yo, hp, hx, hy))
+            for a, b in zip(*outs):
+                assert np.array_equal(a, b)
+    finally:
+        gpu_ctx.set_launch_overlap(True)
+        gpu_ctx.set_precision(0)
